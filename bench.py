@@ -1,0 +1,340 @@
+"""Benchmark: the G = J - K/2 build of the 64-atom L<=3 cluster on B200.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl fjb|reference]
+                    [--precision fp64|routed]
+
+One step = one fused J/K/G build of the 64-atom cluster (512 shells, s x3,
+p x2, d x2, f x1 per atom, 1984 Cartesian AO, tau = 1e-12) for the step's
+density D_k = D + 1e-3 sym(N(0,1)) (the SCF-like sequence, seeded per
+iteration), every D_k resident in HBM before the timed region.  The plan is
+built once (it depends on (basis, tau) and orders pairs by the first D);
+each build screens with its own D_k.  The working set (D_k, J', K', J, K, G:
+6 x 31.5 MB plus the staged pairs) exceeds the 126 MB L2, so no flush is
+needed between steps.
+
+Prints ONE JSON line (rank 0).  With N > 1 (torchrun), every rank builds its
+own replica (the path is one molecule per GPU: "replicas only"), timed with
+CUDA events, max over ranks.
+
+--impl reference times the reference's CPU path, restated as the oracle
+(oracle/oracle.c), on a bounded sample of the same workload's quartets with
+every host core, and extrapolates to the whole build.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "G=J−K/2 build ms/iter: routed mixed vs plain FP64, same B200, |ΔG|≤1e-8"
+WORKLOAD = ("64-atom cluster (seed 1, 0.1 atoms/A^3, >=0.95 A), per atom s x3 p x2 d x2 f x1 "
+            "even-tempered Cartesian shells: 512 shells, 1984 AO; tau 1e-12, 4 eq.29 "
+            "magnitudes; 20 SCF-like densities D_k = D + 1e-3 sym(N(0,1))")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fjb", choices=["fjb", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "routed"])
+    ap.add_argument("--workload", default="c1")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# --- clocks -----------------------------------------------------------------
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --- CPU baseline: the oracle on a bounded sample ---------------------------
+
+def _time_quartets(args):
+    """Worker (spawned): oracle eri_block + digest-free timing of quartets."""
+    flat, quartets = args
+    sys.path.insert(0, HERE)
+    from oracle import oracle as O
+    ob = O.OracleBasis(*flat)
+    out = []
+    for q in quartets:
+        t = time.perf_counter()
+        O.eri_block(ob, *q)
+        out.append(time.perf_counter() - t)
+    return out
+
+
+def cpu_sample(w, lstats, plan, cores: int, budget_s: float = 20.0, seed: int = 0):
+    """Estimated ms of the whole build on the oracle: per (class, K_AB, K_CD)
+    launch key, time the oracle's ERI block on sampled computed-class
+    quartets of that key; weight by the computed counts of the last GPU
+    build.  Returns (ms_estimate, description, cpu_seconds_spent)."""
+    import multiprocessing as mp
+    rng = np.random.default_rng(seed)
+    keys = {}
+    for li, s in enumerate(lstats):
+        if s["computed"] == 0:
+            continue
+        k = (s["la"], s["lb"], s["lc"], s["ld"], s["kab"], s["kcd"])
+        keys.setdefault(k, []).append(li)
+    batches = plan.batches
+    samples, owners = [], []
+    for k, lis in sorted(keys.items()):
+        L = plan.launches[lis[int(rng.integers(len(lis)))]]
+        for _ in range(2):
+            bp = batches[L.bra].pairs[int(rng.integers(len(batches[L.bra].pairs)))]
+            kp = batches[L.ket].pairs[int(rng.integers(len(batches[L.ket].pairs)))]
+            samples.append((bp.a, bp.b, kp.a, kp.b))
+            owners.append(k)
+    f = w.basis.flat()
+    flat = (f["l"], f["centre"], f["prim0"], f["nprim"], f["exps"], f["coefs"])
+    chunks = [samples[i::cores] for i in range(cores)]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_time_quartets, [(flat, c) for c in chunks])
+    wall = time.perf_counter() - t0
+    times = {}
+    for i in range(cores):
+        for q, t in zip(chunks[i], res[i]):
+            pass
+    per = {}
+    flat_times = []
+    for i in range(cores):
+        flat_times.extend(zip(range(i, len(samples), cores), res[i]))
+    for idx, t in flat_times:
+        per.setdefault(owners[idx], []).append(t)
+    total_cpu_s = 0.0
+    for k, lis in keys.items():
+        # the oracle sums every primitive pair; a launch key's K_AB, K_CD are
+        # the kept degrees -- scale the sampled block time by the ratio
+        cnt = sum(lstats[li]["computed"] for li in lis)
+        total_cpu_s += cnt * float(np.median(per[k]))
+    ms = 1e3 * total_cpu_s / cores
+    spent = float(sum(t for _, t in flat_times))
+    desc = (f"oracle eri_block (MMD, FP64) on {len(samples)} sampled quartets, 2 per "
+            f"(class, K_AB, K_CD) key of the build's computed launches, median time per key "
+            f"x computed quartets, summed, / {cores} core(s); digest not timed")
+    return ms, desc, spent, wall
+
+
+# --- the GPU arm --------------------------------------------------------------
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return reference_arm(a, rank, world)
+
+    import torch
+    from felizjueves_b200 import _lib, configs, cost
+    from felizjueves_b200.fock import FockEngine
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    w = getattr(configs, a.workload)()
+    eng = FockEngine(w.basis, device=local)
+    P = eng.plan(w.D, w.tau, w.n_mag)
+    n = w.n_ao
+    n_d = 20
+    Ds = [torch.tensor(configs.perturbed_density(w.D, i), device=f"cuda:{local}")
+          for i in range(n_d)]
+    J = torch.empty((n, n), dtype=torch.float64, device=f"cuda:{local}")
+    K = torch.empty_like(J)
+    G = torch.empty_like(J)
+    prec = _lib.FJB_FP64 if a.precision == "fp64" else _lib.FJB_ROUTED
+    stream = torch.cuda.current_stream()
+    for i in range(a.warmup):
+        eng.build(Ds[i % n_d], J=J, K=K, G=G, precision=prec)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    launches = 0
+    for i in range(a.steps):
+        eng.build(Ds[i % n_d], J=J, K=K, G=G, precision=prec)
+        launches += eng.last_build_stats()[1] if i == 0 else 0
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    total_ms = e0.elapsed_time(e1)
+    ck = clocks.stop()
+    _, nl = eng.last_build_stats()
+    gpu_launches = nl * a.steps
+    ms = total_ms / a.steps
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # roofline of the dominant class kernel (last timed build)
+    cs = eng.class_stats()
+    ls = eng.launch_stats()
+    flops = cost.build_flops(ls)
+    top = max(cs, key=lambda r: r["ms"])
+    tcls = (top["la"], top["lb"], top["lc"], top["ld"])
+    peak64 = ctypes_probe(_lib, 0)
+    ach = flops.get(tcls, 0.0) / (top["ms"] * 1e-3) / 1e12
+    build_tf = sum(flops.values()) / (sum(r["ms"] for r in cs) * 1e-3) / 1e12
+    computed = sum(s["computed"] for s in ls)
+    launched = sum(s["launched"] for s in ls)
+
+    e2e = None
+    if not a.no_e2e and rank == 0:
+        Dh = [configs.perturbed_density(w.D, i) for i in range(3)]
+        eng.build_host(Dh[0], precision=prec)  # warm
+        k2 = min(a.steps, 3)
+        t0 = time.perf_counter()
+        for i in range(k2):
+            eng.build_host(Dh[i % 3], precision=prec)
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / k2
+        e2e = {"value": round(e2e_ms, 3), "unit": "ms/iter", "h2d_bytes_per_step": n * n * 8,
+               "d2h_bytes_per_step": 3 * n * n * 8,
+               "api": "fjb_fock_build_host (C ABI, host buffers; copies in the timed region)"}
+
+    cpu = None
+    if not a.no_cpu and rank == 0 and world == 1:
+        cores = 1
+        est, desc, spent, wall = cpu_sample(w, ls, P, cores)
+        cpu = {"value": round(est, 1), "unit": "ms/iter", "cores": cores, "kind": "port",
+               "sample": desc + f"; {spent:.1f} s of CPU sampled"}
+
+    out = {
+        "metric": METRIC, "value": round(ms, 3), "unit": "ms/iter", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if a.precision == "fp64" else "f64+f32",
+        "data": "synthetic (seeded cluster, random symmetric densities)",
+        "precision": a.precision,
+        "config": {"workload": WORKLOAD, "n_ao": n, "shells": len(w.basis.shells),
+                   "tau": w.tau, "quartets_launched": launched, "quartets_computed": computed,
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "working set > 126 MB L2 (6 x 31.5 MB matrices + pair records); no flush"},
+        "roofline": {"bound": "fp64", "kernel": "hgp_fock_kernel class (%d%d|%d%d)" % tcls,
+                     "achieved": round(ach, 3), "peak": round(peak64, 3), "unit": "TFLOP/s",
+                     "frac": round(ach / peak64, 4) if peak64 else None, "traffic": None,
+                     "peak_source": "measured: fjb_fma_probe FP64 FMA chains on this GPU "
+                                    "(MEASURED_PEAKS.json has no FP64 figure)",
+                     "build_tflops": round(build_tf, 3), "kernel_ms": round(top["ms"], 3),
+                     "flop_model": "reference hgp/cost.py x K^4 + y K^2 + z + 12 n_eri"},
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches, "clocks": ck,
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    if dist:
+        dist.destroy_process_group()
+
+
+def ctypes_probe(_lib, fp32: int) -> float:
+    import ctypes as C
+    v = C.c_double()
+    _lib.check(_lib.load().fjb_fma_probe(fp32, 5, C.byref(v)))
+    return float(v.value)
+
+
+def reference_arm(a, rank, world):
+    if rank != 0:
+        return
+    from felizjueves_b200 import configs
+    from felizjueves_b200.fock import FockEngine
+    w = getattr(configs, a.workload)()
+    # the plan is host work (no GPU); its launch counts come from the plan
+    eng = FockEngine(w.basis, device=-1)
+    P = eng.plan(w.D, w.tau, w.n_mag)
+    ls = eng.launch_stats()
+    # without a GPU build, every launched quartet is counted as computed:
+    # the extrapolation is an upper bound on the CPU work of the screened
+    # build by the fraction the six-block screen skips
+    for s in ls:
+        s["computed"] = s["launched"]
+    cores = os.cpu_count() or 1
+    times = []
+    for i in range(max(1, a.warmup) + a.steps if a.steps <= 3 else 1 + min(a.steps, 3)):
+        est, desc, spent, wall = cpu_sample(w, ls, P, cores, seed=i)
+        times.append(est)
+    v = float(np.median(times[1:] if len(times) > 1 else times))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms/iter",
+        "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(v, 1),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD},
+        "cpu_baseline": {"value": round(v, 1), "unit": "ms/iter", "cores": cores, "kind": "port",
+                         "sample": desc + "; every launched quartet counted (no GPU screen)"},
+        "e2e": {"value": round(v, 1), "unit": "ms/iter", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,100 @@
+"""ctypes binding of libfjb.so (include/fjb.h).
+
+The library is built in-tree (felizjueves_b200/build.py) and loaded from
+felizjueves_b200/_lib/libfjb.so.  There is no fallback: a missing library
+or a failing call raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libfjb.so")
+
+FJB_FP64 = 0
+FJB_ROUTED = 1
+
+_ERRORS = {-1: ValueError, -2: RuntimeError, -3: RuntimeError, -4: ValueError,
+           -5: TimeoutError, -6: ValueError}
+
+
+class Basis_t(C.Structure):
+    _fields_ = [("n_shells", C.c_int32), ("l", C.c_void_p), ("centre", C.c_void_p),
+                ("prim0", C.c_void_p), ("nprim", C.c_void_p), ("exps", C.c_void_p),
+                ("coefs", C.c_void_p)]
+
+
+class PlanCounts_t(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in (
+        "pairs", "pairs_deleted", "primitive_pairs", "primitive_pairs_pruned",
+        "batches", "batch_pairs", "batch_pairs_screened", "launches",
+        "kept_pairs", "kept_prims", "units", "quartets_launched")]
+
+
+class PlanLists_t(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in (
+        "batch_key", "batch_npairs", "pair_ab", "pair_mag", "prims",
+        "pair_G", "pair_dmax", "pair_key", "prim_G",
+        "launches", "screened", "deleted", "magnitudes", "eps", "g_max")]
+
+
+_lib = None
+
+
+def load():
+    """The loaded library; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libfjb.so is not built ({LIB_PATH}); run "
+                           "`python -m felizjueves_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    L.fjb_last_error.restype = C.c_char_p
+    L.fjb_last_error.argtypes = [vp]
+    L.fjb_version.restype = C.c_char_p
+    L.fjb_create.argtypes = [C.POINTER(vp), C.POINTER(Basis_t), C.c_int]
+    L.fjb_destroy.argtypes = [vp]
+    L.fjb_destroy.restype = None
+    L.fjb_n_ao.argtypes = [vp]
+    L.fjb_plan.argtypes = [vp, vp, dbl, C.c_int]
+    L.fjb_plan_counts.argtypes = [vp, C.POINTER(PlanCounts_t)]
+    L.fjb_plan_export.argtypes = [vp, C.POINTER(PlanLists_t)]
+    L.fjb_screen_mask.argtypes = [vp, vp, vp, vp]
+    L.fjb_fock_build.argtypes = [vp, vp, vp, vp, vp, C.c_int, dbl, vp]
+    L.fjb_fock_build_host.argtypes = [vp, vp, vp, vp, vp, C.c_int, dbl]
+    L.fjb_eri_blocks.argtypes = [vp, vp, C.c_int, vp, vp]
+    L.fjb_boys.argtypes = [C.c_int, vp, C.c_int, vp]
+    L.fjb_last_build_stats.argtypes = [vp, C.POINTER(dbl), C.POINTER(C.c_int)]
+    L.fjb_launch_stats.argtypes = [vp, vp, i64]
+    L.fjb_class_stats.argtypes = [vp, vp, i64, C.POINTER(i64)]
+    L.fjb_fma_probe.argtypes = [C.c_int, C.c_int, C.POINTER(dbl)]
+    _lib = L
+    return L
+
+
+EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_ao",
+           "fjb_plan", "fjb_plan_counts", "fjb_plan_export", "fjb_screen_mask",
+           "fjb_fock_build", "fjb_fock_build_host", "fjb_eri_blocks", "fjb_boys",
+           "fjb_last_build_stats", "fjb_launch_stats", "fjb_class_stats",
+           "fjb_fma_probe")
+
+
+class LaunchStat_t(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("la", "lb", "lc", "ld", "kab", "kcd")] + \
+               [("launched", C.c_int64), ("computed", C.c_int64)]
+
+
+class ClassStat_t(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("la", "lb", "lc", "ld")] + \
+               [("ms", C.c_double), ("units", C.c_int64)]
+
+
+def check(rc: int, handle=None) -> None:
+    if rc == 0:
+        return
+    msg = load().fjb_last_error(handle).decode(errors="replace")
+    raise _ERRORS.get(rc, RuntimeError)(f"fjb error {rc}: {msg}")

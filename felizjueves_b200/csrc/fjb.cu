@@ -1,0 +1,1095 @@
+// fjb.cu -- kernels and the C ABI of libfjb.so (include/fjb.h).
+//
+// Host runtime: a handle owns the basis, the plan (plan.cpp, the reference's
+// f_launches), the per-class recurrence programs (hgp_tables.cpp) staged in
+// device memory, and the work units.  A build is a short stream-ordered
+// sequence: density blocks -> zero J', K' -> one HGP kernel per class present
+// -> close (J = J' + J'^T, K = K' + K'^T, G = J - K/2).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+#include "../../include/fjb.h"
+#include "fjb_internal.h"
+#include "fock_kernels.cuh"
+#include "hgp_tables.h"
+#include "plan.h"
+
+namespace fjb {
+std::vector<double> boys_table();
+}
+
+using namespace fjb;
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr double kTwoOverSqrtPi = 1.1283791670955126;
+
+__global__ void density_blocks_kernel(const double *__restrict__ D, int n_ao, int n_sh,
+                                      const int *__restrict__ off, const int *__restrict__ nc,
+                                      double *__restrict__ Dsh) {
+    int st = blockIdx.x * blockDim.x + threadIdx.x;
+    if (st >= n_sh * n_sh) return;
+    int s = st / n_sh, t = st % n_sh;
+    double m = 0.0;
+    for (int i = 0; i < nc[s]; ++i)
+        for (int j = 0; j < nc[t]; ++j) {
+            double v = fabs(D[(size_t)(off[s] + i) * n_ao + off[t] + j]);
+            if (v > m) m = v;
+        }
+    Dsh[st] = m;
+}
+
+__global__ void close_kernel(const double *__restrict__ Jp, const double *__restrict__ Kp, int n,
+                             double *J, double *K, double *G) {
+    size_t ij = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ij >= (size_t)n * n) return;
+    size_t i = ij / n, j = ij % n, ji = j * n + i;
+    double jv = Jp[ij] + Jp[ji];
+    double kv = Kp[ij] + Kp[ji];
+    if (J) J[ij] = jv;
+    if (K) K[ij] = kv;
+    if (G) G[ij] = jv - 0.5 * kv;
+}
+
+__global__ void boys_kernel(int M, const double *T, int n, double *F, const double *tab) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double f[kBoysMaxM + 1];
+    boys_eval(M, T[i], f, tab);
+    for (int m = 0; m <= M; ++m) F[(size_t)i * (M + 1) + m] = f[m];
+}
+
+__global__ void screen_mask_kernel(const Unit *units, int n_units, const LaunchRec *launches,
+                                   const PairRec *pairs, const double *Dsh, int n_sh, double tau,
+                                   uint8_t *mask) {
+    for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
+        const Unit U = units[u];
+        const LaunchRec L = launches[U.launch];
+        const PairRec bra = pairs[L.bra_pair0 + U.ib];
+        const int64_t n = L.n_ket, ib = U.ib;
+        const int64_t row = L.diag ? ib * n - ib * (ib - 1) / 2 - ib : ib * n;
+        for (int ik = U.k0 + threadIdx.x; ik < U.k1; ik += blockDim.x) {
+            const PairRec ket = pairs[L.ket_pair0 + ik];
+            mask[L.qbase + row + ik] =
+                skip6(Dsh, n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G, tau) ? 1 : 0;
+        }
+    }
+}
+
+// The HGP Fock kernel (file header of fock_kernels.cuh).  All floating-point
+// work is FP64.
+__global__ void __launch_bounds__(kThreads) hgp_fock_kernel(const KArgs A) {
+    extern __shared__ __align__(16) double sm[];
+    const ClassDev &C = A.C;
+    double *V = sm + C.sm_V;
+    double *bound = sm + C.sm_bound;
+    double *S = sm + C.sm_S;
+    double *braP = sm + C.sm_braP;
+    double *ketP = sm + C.sm_ketP;
+    double *cb = sm + C.sm_cb;
+    double *ck = sm + C.sm_ck;
+    double *Dab = sm + C.sm_D;
+    double *Dcd = Dab + C.nab;
+    double *Dac = Dcd + C.ncd;
+    double *Dad = Dac + C.na * C.nc;
+    double *Dbc = Dad + C.na * C.nd;
+    double *Dbd = Dbc + C.nb * C.nc;
+    double *Jab = sm + C.sm_Jab;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int slots = C.slots;
+    const int na = C.na, nb = C.nb, nc = C.nc, nd = C.nd, nab = C.nab, ncd = C.ncd;
+    const int nbe = C.nbe, nbf = C.nbf, L = C.L, n_ao = A.n_ao;
+    const bool tap = A.tap_out != nullptr;
+
+    for (int u = blockIdx.x; u < A.n_units; u += gridDim.x) {
+        const Unit U = A.units[u];
+        const LaunchRec LR = A.launches[U.launch];
+        const PairRec bra = A.pairs[LR.bra_pair0 + U.ib];
+        const int kab = bra.nprim;
+        {
+            const double *src = reinterpret_cast<const double *>(A.prims + bra.prim0);
+            for (int i = tid; i < kab * 8; i += nt) braP[i] = src[i];
+        }
+        for (int i = tid; i < C.n_cb; i += nt) {
+            const HCoef h = C.cb[i];
+            cb[i] = (double)h.binom * ipow(bra.AB[0], h.px) * ipow(bra.AB[1], h.py) *
+                    ipow(bra.AB[2], h.pz);
+        }
+        if (!tap)
+            for (int i = tid; i < nab; i += nt) {
+                Dab[i] = A.D[(size_t)(bra.ao_a + i / nb) * n_ao + bra.ao_b + i % nb];
+                Jab[i] = 0.0;
+            }
+        __syncthreads();
+        int n_computed = 0;
+        for (int ik = U.k0; ik < U.k1; ++ik) {
+            const PairRec ket = A.pairs[LR.ket_pair0 + ik];
+            if (!tap && skip6(A.Dsh, A.n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G, A.tau))
+                continue;
+            ++n_computed;
+            const double deg = (bra.a == bra.b ? 0.5 : 1.0) * (ket.a == ket.b ? 0.5 : 1.0) *
+                               ((LR.diag && ik == U.ib) ? 0.5 : 1.0);
+            const int kcd = ket.nprim;
+            {
+                const double *src = reinterpret_cast<const double *>(A.prims + ket.prim0);
+                for (int i = tid; i < kcd * 8; i += nt) ketP[i] = src[i];
+            }
+            for (int i = tid; i < C.n_ck; i += nt) {
+                const HCoef h = C.ck[i];
+                ck[i] = (double)h.binom * ipow(ket.AB[0], h.px) * ipow(ket.AB[1], h.py) *
+                        ipow(ket.AB[2], h.pz);
+            }
+            if (!tap) {
+                const int oa = bra.ao_a, ob = bra.ao_b, oc = ket.ao_a, od = ket.ao_b;
+                for (int i = tid; i < ncd; i += nt)
+                    Dcd[i] = A.D[(size_t)(oc + i / nd) * n_ao + od + i % nd];
+                for (int i = tid; i < na * nc; i += nt)
+                    Dac[i] = A.D[(size_t)(oa + i / nc) * n_ao + oc + i % nc];
+                for (int i = tid; i < na * nd; i += nt)
+                    Dad[i] = A.D[(size_t)(oa + i / nd) * n_ao + od + i % nd];
+                for (int i = tid; i < nb * nc; i += nt)
+                    Dbc[i] = A.D[(size_t)(ob + i / nc) * n_ao + oc + i % nc];
+                for (int i = tid; i < nb * nd; i += nt)
+                    Dbd[i] = A.D[(size_t)(ob + i / nd) * n_ao + od + i % nd];
+            }
+            for (int i = tid; i < nbe * nbf; i += nt) bound[i] = 0.0;
+            __syncthreads();
+
+            const int K = kab * kcd;
+            for (int c0 = 0; c0 < K; c0 += slots) {
+                const int ns = min(slots, K - c0);
+                for (int s = tid; s < ns; s += nt) {
+                    const int t = c0 + s, ikcd = t / kab, ikab = t - ikcd * kab;
+                    const double *pb = braP + 8 * ikab, *pk = ketP + 8 * ikcd;
+                    const double p = pb[6], q = pk[6];
+                    const double ppq = p + q, inv = 1.0 / ppq, rho = p * q * inv;
+                    const double PQx = pb[0] - pk[0], PQy = pb[1] - pk[1], PQz = pb[2] - pk[2];
+                    const double wp = -q * inv, wq = p * inv;
+                    const double inv2p = 0.5 / p, inv2q = 0.5 / q;
+                    double *Ss = S + s;
+                    Ss[0 * slots] = pb[3];
+                    Ss[1 * slots] = pb[4];
+                    Ss[2 * slots] = pb[5];
+                    Ss[3 * slots] = wp * PQx;
+                    Ss[4 * slots] = wp * PQy;
+                    Ss[5 * slots] = wp * PQz;
+                    Ss[6 * slots] = inv2p;
+                    Ss[7 * slots] = inv2p * rho / p;
+                    Ss[8 * slots] = pk[3];
+                    Ss[9 * slots] = pk[4];
+                    Ss[10 * slots] = pk[5];
+                    Ss[11 * slots] = wq * PQx;
+                    Ss[12 * slots] = wq * PQy;
+                    Ss[13 * slots] = wq * PQz;
+                    Ss[14 * slots] = inv2q;
+                    Ss[15 * slots] = inv2q * rho / q;
+                    Ss[16 * slots] = 0.5 * inv;
+                    const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+                    double F[kMaxLQuartet + 1];
+                    boys_eval(L, T, F, A.boys_tab);
+                    const double seed = pb[7] * pk[7] * kTwoOverSqrtPi * sqrt(rho);
+                    V[s] = 0.0;
+                    for (int m = 0; m <= L; ++m) V[(size_t)__ldg(C.leaf + m) * slots + s] = seed * F[m];
+                }
+                __syncthreads();
+                for (int lv = 0; lv < C.n_levels; ++lv) {
+                    const int o0 = __ldg(C.level_off + lv), o1 = __ldg(C.level_off + lv + 1);
+                    const int items = (o1 - o0) * ns;
+                    for (int it = tid; it < items; it += nt) {
+                        const int oi = o0 + it / ns, s = it - (it / ns) * ns;
+                        const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(C.ops) + oi);
+                        VOp op;
+                        memcpy(&op, &raw, sizeof(op));
+                        const double *Ss = S + s;
+                        const int base = op.kind * 8;
+                        const double a = Ss[(base + op.d) * slots];
+                        const double b = Ss[(base + 3 + op.d) * slots];
+                        const double c = Ss[(base + 6) * slots];
+                        const double dd = Ss[(base + 7) * slots];
+                        const double e = Ss[16 * slots];
+                        double v = a * V[(size_t)op.s0 * slots + s] + b * V[(size_t)op.s1 * slots + s];
+                        v += (double)op.c2 * (c * V[(size_t)op.s2 * slots + s] - dd * V[(size_t)op.s3 * slots + s]);
+                        v += (double)op.c4 * e * V[(size_t)op.s4 * slots + s];
+                        V[(size_t)op.dst * slots + s] = v;
+                    }
+                    __syncthreads();
+                }
+                for (int t = tid; t < nbe * nbf; t += nt) {
+                    const size_t node = __ldg(C.tgt + t);
+                    double acc = 0.0;
+                    for (int s = 0; s < ns; ++s) acc += V[node * slots + s];
+                    bound[t] += acc;
+                }
+                __syncthreads();
+            }
+            // HRR, bra side: X[ab][f] = sum_k coefB(b,k) (a+k, 0 | f)
+            double *X = V, *Y = V + (size_t)nab * nbf;
+            for (int i = tid; i < nab * nbf; i += nt) {
+                const int ab = i / nbf, jf = i - ab * nbf;
+                const int t0 = __ldg(C.bra_off + ab), t1 = __ldg(C.bra_off + ab + 1);
+                double acc = 0.0;
+                for (int t = t0; t < t1; ++t) {
+                    const HTerm h = C.bra_terms[t];
+                    acc += cb[h.cidx] * bound[h.src * nbf + jf];
+                }
+                X[i] = acc;
+            }
+            __syncthreads();
+            // HRR, ket side: Y[ab][cd] = sum_k coefK(d,k) X[ab][c+k]
+            for (int i = tid; i < nab * ncd; i += nt) {
+                const int ab = i / ncd, cd = i - ab * ncd;
+                const int t0 = __ldg(C.ket_off + cd), t1 = __ldg(C.ket_off + cd + 1);
+                double acc = 0.0;
+                for (int t = t0; t < t1; ++t) {
+                    const HTerm h = C.ket_terms[t];
+                    acc += ck[h.cidx] * X[ab * nbf + h.src];
+                }
+                Y[i] = acc;
+            }
+            __syncthreads();
+            if (tap) {
+                double *out = A.tap_out + A.tap_off[u];
+                for (int i = tid; i < nab * ncd; i += nt) out[i] = Y[i];
+                __syncthreads();
+                continue;
+            }
+            // the six-block digest
+            {
+                const int oa = bra.ao_a, ob = bra.ao_b, oc = ket.ao_a, od = ket.ao_b;
+                const int n1 = nab, n2 = n1 + ncd, n3 = n2 + na * nc, n4 = n3 + na * nd,
+                          n5 = n4 + nb * nc, n6 = n5 + nb * nd;
+                const double w2 = 2.0 * deg;
+                for (int o = tid; o < n6; o += nt) {
+                    double acc = 0.0;
+                    if (o < n1) {
+                        const double *y = Y + (size_t)o * ncd;
+                        for (int kl = 0; kl < ncd; ++kl) acc += Dcd[kl] * y[kl];
+                        Jab[o] += w2 * acc;
+                    } else if (o < n2) {
+                        const int kl = o - n1;
+                        for (int ij = 0; ij < nab; ++ij) acc += Dab[ij] * Y[(size_t)ij * ncd + kl];
+                        atomicAdd(A.Jp + (size_t)(oc + kl / nd) * n_ao + od + kl % nd, w2 * acc);
+                    } else if (o < n3) {
+                        const int r = o - n2, i = r / nc, k = r % nc;
+                        for (int j = 0; j < nb; ++j)
+                            for (int l = 0; l < nd; ++l)
+                                acc += Dbd[j * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                        atomicAdd(A.Kp + (size_t)(oa + i) * n_ao + oc + k, deg * acc);
+                    } else if (o < n4) {
+                        const int r = o - n3, i = r / nd, l = r % nd;
+                        for (int j = 0; j < nb; ++j)
+                            for (int k = 0; k < nc; ++k)
+                                acc += Dbc[j * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                        atomicAdd(A.Kp + (size_t)(oa + i) * n_ao + od + l, deg * acc);
+                    } else if (o < n5) {
+                        const int r = o - n4, j = r / nc, k = r % nc;
+                        for (int i = 0; i < na; ++i)
+                            for (int l = 0; l < nd; ++l)
+                                acc += Dad[i * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                        atomicAdd(A.Kp + (size_t)(ob + j) * n_ao + oc + k, deg * acc);
+                    } else {
+                        const int r = o - n5, j = r / nd, l = r % nd;
+                        for (int i = 0; i < na; ++i)
+                            for (int k = 0; k < nc; ++k)
+                                acc += Dac[i * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                        atomicAdd(A.Kp + (size_t)(ob + j) * n_ao + od + l, deg * acc);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (!tap)
+            for (int i = tid; i < nab; i += nt)
+                atomicAdd(A.Jp + (size_t)(bra.ao_a + i / nb) * n_ao + bra.ao_b + i % nb, Jab[i]);
+        if (A.computed && tid == 0 && n_computed)
+            atomicAdd(A.computed + U.launch, (unsigned long long)n_computed);
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host runtime
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr int kSmemBudgetDoubles = 27648;  // 216 KiB of the 227 KiB a CTA may hold
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { reset(); }
+    void reset() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        if (count == n && p) return;
+        reset();
+        if (count == 0) return;
+        if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
+            p = nullptr;
+            throw std::runtime_error("cudaMalloc failed");
+        }
+        n = count;
+    }
+    void upload(const std::vector<T> &v) {
+        alloc(v.size());
+        if (!v.empty() && cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+            throw std::runtime_error("cudaMemcpy to device failed");
+    }
+};
+
+struct ClassEntry {
+    ClassHost host;
+    DevBuf<int> level_off, bra_off, ket_off;
+    DevBuf<VOp> ops;
+    DevBuf<uint16_t> leaf, tgt;
+    DevBuf<HCoef> cb, ck;
+    DevBuf<HTerm> bra_terms, ket_terms;
+    void upload() {
+        level_off.upload(host.level_off);
+        ops.upload(host.ops);
+        leaf.upload(host.leaf);
+        tgt.upload(host.tgt);
+        cb.upload(host.cb);
+        bra_off.upload(host.bra_off);
+        bra_terms.upload(host.bra_terms);
+        ck.upload(host.ck);
+        ket_off.upload(host.ket_off);
+        ket_terms.upload(host.ket_terms);
+    }
+    ClassDev dev(int max_kab, int max_kcd) const {
+        ClassDev d;
+        if (!layout_class(host, max_kab, max_kcd, kSmemBudgetDoubles, &d))
+            throw std::length_error("class does not fit in shared memory");
+        d.level_off = level_off.p;
+        d.ops = ops.p;
+        d.leaf = leaf.p;
+        d.tgt = tgt.p;
+        d.cb = cb.p;
+        d.bra_off = bra_off.p;
+        d.bra_terms = bra_terms.p;
+        d.ck = ck.p;
+        d.ket_off = ket_off.p;
+        d.ket_terms = ket_terms.p;
+        return d;
+    }
+};
+
+struct ClassRun {
+    ClassDev dev;
+    int unit0 = 0, n_units = 0;
+    int grid = 0;
+};
+
+}  // namespace
+
+struct fjb_handle {
+    int device = 0;
+    HostBasis basis;
+    std::string err;
+    std::map<std::tuple<int, int, int, int>, std::unique_ptr<ClassEntry>> classes;
+    DevBuf<double> boys;
+    DevBuf<int> sh_off, sh_nc;
+    // plan
+    bool planned = false;
+    Plan plan;
+    DevBuf<PairRec> pairs;
+    DevBuf<PrimRec> prims;
+    DevBuf<LaunchRec> launches;
+    DevBuf<Unit> units;
+    std::vector<ClassRun> runs;
+    int64_t quartets_launched = 0;
+    int n_units = 0;
+    // build scratch
+    DevBuf<double> Dsh, Jp, Kp;
+    DevBuf<double> hD, hJ, hK, hG;  // fjb_fock_build_host staging
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int last_launches = 0;
+    // measurement
+    DevBuf<unsigned long long> computed;
+    std::vector<fjb_launch_stat> lstat;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> cev;
+    bool built = false;
+
+    void free_class_events() {
+        for (auto &e : cev) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        cev.clear();
+    }
+    ~fjb_handle() { free_class_events(); }
+
+    ClassEntry &cls(int la, int lb, int lc, int ld) {
+        auto key = std::make_tuple(la, lb, lc, ld);
+        auto it = classes.find(key);
+        if (it != classes.end()) return *it->second;
+        auto e = std::make_unique<ClassEntry>();
+        e->host = build_class(la, lb, lc, ld);
+        e->upload();
+        auto &ref = *e;
+        classes[key] = std::move(e);
+        return ref;
+    }
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(fjb_handle *h, int code, const std::string &msg) {
+    if (h) h->err = msg;
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_OK(h, x)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail((h), FJB_E_CUDA, std::string(#x ": ") + cudaGetErrorString(e_));     \
+    } while (0)
+
+PrimRec prim_record(const HostShell &sa, const HostShell &sb, int k) {
+    const int kb = (int)sb.exps.size();
+    const int i = k / kb, j = k % kb;
+    const double x = sa.exps[i], y = sb.exps[j];
+    const double p = x + y;
+    double ab2 = 0.0;
+    for (int d = 0; d < 3; ++d) ab2 += (sa.centre[d] - sb.centre[d]) * (sa.centre[d] - sb.centre[d]);
+    PrimRec r;
+    for (int d = 0; d < 3; ++d) {
+        r.P[d] = (x * sa.centre[d] + y * sb.centre[d]) / p;
+        r.X[d] = r.P[d] - sa.centre[d];
+    }
+    r.zeta = p;
+    r.U = sa.coefs[i] * sb.coefs[j] * std::pow(M_PI / p, 1.5) * std::exp(-x * y / p * ab2);
+    return r;
+}
+
+PairRec pair_record(const HostBasis &B, int a, int b, double G, int prim0, int nprim) {
+    PairRec r{};
+    r.a = a;
+    r.b = b;
+    r.ao_a = B.offsets[a];
+    r.ao_b = B.offsets[b];
+    r.prim0 = prim0;
+    r.nprim = nprim;
+    r.G = G;
+    for (int d = 0; d < 3; ++d) r.AB[d] = B.shells[a].centre[d] - B.shells[b].centre[d];
+    return r;
+}
+
+int grid_for(const ClassDev &d, int n_units) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hgp_fock_kernel, kThreads,
+                                                  (size_t)d.sm_total * sizeof(double));
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int g = std::max(1, per_sm) * sms;
+    return std::max(1, std::min(n_units, g));
+}
+
+int ensure_smem_attr(fjb_handle *h) {
+    static bool done = false;
+    if (done) return 0;
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kSmemBudgetDoubles * (int)sizeof(double)));
+    done = true;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fjb_last_error(const fjb_handle *h) { return h ? h->err.c_str() : g_err.c_str(); }
+
+const char *fjb_version(void) { return "fjb 0.1 sm_100a"; }
+
+int fjb_create(fjb_handle **out, const fjb_basis *b, int device) {
+    if (!out || !b || b->n_shells <= 0) return fail(nullptr, FJB_E_ARG, "no basis");
+    auto h = std::make_unique<fjb_handle>();
+    h->device = device;
+    int n = 0;
+    for (int s = 0; s < b->n_shells; ++s) {
+        HostShell sh;
+        sh.l = b->l[s];
+        if (sh.l < 0) return fail(nullptr, FJB_E_ARG, "angular momentum is not an int >= 0");
+        if (sh.l > FJB_MAX_L)
+            return fail(nullptr, FJB_E_LIMIT, "l = " + std::to_string(sh.l) + " above the compiled maximum " +
+                                                   std::to_string(FJB_MAX_L));
+        for (int d = 0; d < 3; ++d) {
+            sh.centre[d] = b->centre[3 * s + d];
+            if (!std::isfinite(sh.centre[d])) return fail(nullptr, FJB_E_ARG, "centre has a non-finite entry");
+        }
+        if (b->nprim[s] < 1) return fail(nullptr, FJB_E_ARG, "a shell needs at least one primitive");
+        for (int k = 0; k < b->nprim[s]; ++k) {
+            double e = b->exps[b->prim0[s] + k], c = b->coefs[b->prim0[s] + k];
+            if (!(std::isfinite(e) && e > 0)) return fail(nullptr, FJB_E_ARG, "exponents must all be finite and > 0");
+            if (!std::isfinite(c)) return fail(nullptr, FJB_E_ARG, "coefficients have a non-finite entry");
+            sh.exps.push_back(e);
+            sh.coefs.push_back(c);
+        }
+        h->basis.offsets.push_back(n);
+        n += (sh.l + 1) * (sh.l + 2) / 2;
+        h->basis.shells.push_back(std::move(sh));
+    }
+    h->basis.n_ao = n;
+    if (device < 0) {  // host-only handle: plans and exports, no builds
+        *out = h.release();
+        return FJB_OK;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return fail(nullptr, FJB_E_CUDA, "cudaSetDevice failed");
+    try {
+        h->boys.upload(boys_table());
+        std::vector<int> off(h->basis.offsets), nc;
+        for (auto &s : h->basis.shells) nc.push_back((s.l + 1) * (s.l + 2) / 2);
+        h->sh_off.upload(off);
+        h->sh_nc.upload(nc);
+    } catch (const std::exception &e) {
+        return fail(nullptr, FJB_E_CUDA, e.what());
+    }
+    if (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)
+        return fail(nullptr, FJB_E_CUDA, "cudaEventCreate failed");
+    *out = h.release();
+    return FJB_OK;
+}
+
+void fjb_destroy(fjb_handle *h) {
+    if (!h) return;
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    delete h;
+}
+
+int fjb_n_ao(const fjb_handle *h) { return h ? h->basis.n_ao : -1; }
+
+int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
+    if (!h || !D_host) return fail(h, FJB_E_ARG, "null argument");
+    if (h->device >= 0) cudaSetDevice(h->device);
+    h->planned = false;
+    h->lstat.clear();
+    try {
+        unsigned nt = std::max(1u, std::thread::hardware_concurrency());
+        h->plan = f_launches(h->basis, D_host, tau, n_mag, (int)nt);
+    } catch (const std::invalid_argument &e) {
+        return fail(h, FJB_E_ARG, e.what());
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_PLAN, e.what());
+    }
+    const Plan &P = h->plan;
+    // stage pairs and primitive records, batch by batch
+    std::vector<PairRec> pr;
+    std::vector<PrimRec> pm;
+    std::vector<int> batch_pair0;
+    int max_deg = 1;
+    for (auto &bt : P.batches) {
+        batch_pair0.push_back((int)pr.size());
+        if (bt.degree > FJB_MAX_PRIM_PAIRS)
+            return fail(h, FJB_E_LIMIT, "degree " + std::to_string(bt.degree) +
+                                            " exceeds MAX_PRIM_PAIRS = 128, the shared staging cap");
+        max_deg = std::max(max_deg, bt.degree);
+        for (auto &p : bt.pairs) {
+            pr.push_back(pair_record(h->basis, p.a, p.b, p.G, (int)pm.size(), (int)p.prims.size()));
+            for (int k : p.prims) pm.push_back(prim_record(h->basis.shells[p.a], h->basis.shells[p.b], k));
+        }
+    }
+    // launches and work units, grouped by class
+    std::vector<LaunchRec> lr;
+    std::map<std::tuple<int, int, int, int>, std::vector<Unit>> by_class;
+    std::map<std::tuple<int, int, int, int>, std::pair<int, int>> class_deg;
+    int64_t qbase = 0;
+    for (auto &L : P.launches) {
+        const PlanBatch &br = P.batches[L.first], &kt = P.batches[L.second];
+        LaunchRec r{};
+        r.bra_pair0 = batch_pair0[L.first];
+        r.n_bra = (int)br.pairs.size();
+        r.ket_pair0 = batch_pair0[L.second];
+        r.n_ket = (int)kt.pairs.size();
+        r.diag = L.first == L.second;
+        r.qbase = qbase;
+        const int64_t nq = r.diag ? (int64_t)r.n_bra * (r.n_bra + 1) / 2 : (int64_t)r.n_bra * r.n_ket;
+        qbase += nq;
+        auto key = std::make_tuple(br.la, br.lb, kt.la, kt.lb);
+        const int li = (int)lr.size();
+        lr.push_back(r);
+        h->lstat.push_back(fjb_launch_stat{br.la, br.lb, kt.la, kt.lb, br.degree, kt.degree, nq, 0});
+        auto &cd = class_deg[key];
+        cd.first = std::max(cd.first, br.degree);
+        cd.second = std::max(cd.second, kt.degree);
+        auto &us = by_class[key];
+        for (int ib = 0; ib < r.n_bra; ++ib) {
+            const int k_begin = r.diag ? ib : 0;
+            for (int k0 = k_begin; k0 < r.n_ket; k0 += kKetChunk)
+                us.push_back(Unit{li, ib, k0, std::min(r.n_ket, k0 + kKetChunk)});
+        }
+    }
+    std::vector<Unit> units;
+    h->runs.clear();
+    if (h->device < 0) {  // host-only: the lists are complete, nothing is staged
+        for (auto &kv : by_class) units.insert(units.end(), kv.second.begin(), kv.second.end());
+        h->quartets_launched = qbase;
+        h->n_units = (int)units.size();
+        h->planned = true;
+        return FJB_OK;
+    }
+    try {
+        for (auto &kv : by_class) {
+            auto [la, lb, lc, ld] = kv.first;
+            ClassEntry &ce = h->cls(la, lb, lc, ld);
+            ClassRun run;
+            auto deg = class_deg[kv.first];
+            run.dev = ce.dev(deg.first, deg.second);
+            run.unit0 = (int)units.size();
+            run.n_units = (int)kv.second.size();
+            units.insert(units.end(), kv.second.begin(), kv.second.end());
+            h->runs.push_back(run);
+        }
+        h->pairs.upload(pr);
+        h->prims.upload(pm);
+        h->launches.upload(lr);
+        h->units.upload(units);
+        const size_t nn = (size_t)h->basis.n_ao * h->basis.n_ao;
+        const size_t ns = h->basis.shells.size();
+        h->Dsh.alloc(ns * ns);
+        h->Jp.alloc(nn);
+        h->Kp.alloc(nn);
+    } catch (const std::length_error &e) {
+        return fail(h, FJB_E_LIMIT, e.what());
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, e.what());
+    }
+    if (int rc = ensure_smem_attr(h)) return rc;
+    for (auto &r : h->runs) r.grid = grid_for(r.dev, r.n_units);
+    h->free_class_events();
+    for (size_t i = 0; i < h->runs.size(); ++i) {
+        cudaEvent_t a, b;
+        CUDA_OK(h, cudaEventCreate(&a));
+        CUDA_OK(h, cudaEventCreate(&b));
+        h->cev.emplace_back(a, b);
+    }
+    try {
+        h->computed.alloc(std::max<size_t>(1, lr.size()));
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, e.what());
+    }
+    h->built = false;
+    h->quartets_launched = qbase;
+    h->n_units = (int)units.size();
+    h->planned = true;
+    return FJB_OK;
+}
+
+int fjb_plan_counts(const fjb_handle *hc, fjb_plan_counts_t *o) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h || !o) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
+    const Plan &P = h->plan;
+    *o = fjb_plan_counts_t{};
+    int64_t kept = 0, kprims = 0;
+    for (auto &b : P.batches) {
+        kept += (int64_t)b.pairs.size();
+        for (auto &p : b.pairs) kprims += (int64_t)p.prims.size();
+    }
+    o->pairs = kept + (int64_t)P.deleted.size();
+    o->pairs_deleted = (int64_t)P.deleted.size();
+    o->primitive_pairs = P.n_prim_total;
+    o->primitive_pairs_pruned = P.n_prim_total - kprims;
+    o->batches = (int64_t)P.batches.size();
+    o->batch_pairs = o->batches * (o->batches + 1) / 2;
+    o->batch_pairs_screened = (int64_t)P.screened.size();
+    o->launches = (int64_t)P.launches.size();
+    o->kept_pairs = kept;
+    o->kept_prims = kprims;
+    o->units = h->n_units;
+    o->quartets_launched = h->quartets_launched;
+    return FJB_OK;
+}
+
+int fjb_plan_export(const fjb_handle *hc, fjb_plan_lists *o) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h || !o) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
+    const Plan &P = h->plan;
+    size_t ip = 0, ik = 0;
+    for (size_t bi = 0; bi < P.batches.size(); ++bi) {
+        const PlanBatch &b = P.batches[bi];
+        if (o->batch_key) {
+            o->batch_key[4 * bi + 0] = b.la;
+            o->batch_key[4 * bi + 1] = b.lb;
+            o->batch_key[4 * bi + 2] = b.degree;
+            o->batch_key[4 * bi + 3] = b.mag;
+        }
+        if (o->batch_npairs) o->batch_npairs[bi] = (int)b.pairs.size();
+        for (auto &p : b.pairs) {
+            if (o->pair_ab) {
+                o->pair_ab[2 * ip] = p.a;
+                o->pair_ab[2 * ip + 1] = p.b;
+            }
+            if (o->pair_G) o->pair_G[ip] = p.G;
+            if (o->pair_dmax) o->pair_dmax[ip] = p.dmax;
+            if (o->pair_key) o->pair_key[ip] = p.key;
+            if (o->pair_mag) o->pair_mag[ip] = p.mag;
+            for (size_t k = 0; k < p.prims.size(); ++k, ++ik) {
+                if (o->prims) o->prims[ik] = p.prims[k];
+                if (o->prim_G) o->prim_G[ik] = p.prim_G[k];
+            }
+            ++ip;
+        }
+    }
+    for (size_t i = 0; i < P.launches.size(); ++i)
+        if (o->launches) {
+            o->launches[2 * i] = P.launches[i].first;
+            o->launches[2 * i + 1] = P.launches[i].second;
+        }
+    for (size_t i = 0; i < P.screened.size(); ++i)
+        if (o->screened) {
+            o->screened[2 * i] = P.screened[i].first;
+            o->screened[2 * i + 1] = P.screened[i].second;
+        }
+    for (size_t i = 0; i < P.deleted.size(); ++i)
+        if (o->deleted) {
+            o->deleted[2 * i] = P.deleted[i].first;
+            o->deleted[2 * i + 1] = P.deleted[i].second;
+        }
+    if (o->magnitudes)
+        for (size_t i = 0; i < P.mags.size(); ++i) o->magnitudes[i] = P.mags[i];
+    if (o->eps) *o->eps = P.eps;
+    if (o->g_max) *o->g_max = P.g_max;
+    return FJB_OK;
+}
+
+int fjb_screen_mask(fjb_handle *h, const double *D_dev, uint8_t *mask_dev, void *stream) {
+    if (!h || !D_dev || !mask_dev) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    cudaSetDevice(h->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nsh = (int)h->basis.shells.size();
+    density_blocks_kernel<<<(nsh * nsh + 255) / 256, 256, 0, st>>>(D_dev, h->basis.n_ao, nsh, h->sh_off.p,
+                                                                 h->sh_nc.p, h->Dsh.p);
+    if (h->n_units > 0)
+        screen_mask_kernel<<<std::min(h->n_units, 148 * 16), 64, 0, st>>>(
+            h->units.p, h->n_units, h->launches.p, h->pairs.p, h->Dsh.p, nsh, h->plan.tau, mask_dev);
+    CUDA_OK(h, cudaGetLastError());
+    return FJB_OK;
+}
+
+int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_dev, double *G_dev,
+                   int precision, double threshold, void *stream) {
+    if (!h || !D_dev) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
+    if (precision != FJB_FP64 && precision != FJB_ROUTED) return fail(h, FJB_E_ARG, "unknown precision mode");
+    (void)threshold;
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    cudaSetDevice(h->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nsh = (int)h->basis.shells.size(), nao = h->basis.n_ao;
+    const size_t nn = (size_t)nao * nao;
+    int launches = 0;
+    density_blocks_kernel<<<(nsh * nsh + 255) / 256, 256, 0, st>>>(D_dev, nao, nsh, h->sh_off.p, h->sh_nc.p,
+                                                                 h->Dsh.p);
+    ++launches;
+    CUDA_OK(h, cudaMemsetAsync(h->Jp.p, 0, nn * sizeof(double), st));
+    CUDA_OK(h, cudaMemsetAsync(h->Kp.p, 0, nn * sizeof(double), st));
+    CUDA_OK(h, cudaMemsetAsync(h->computed.p, 0, h->computed.n * sizeof(unsigned long long), st));
+    CUDA_OK(h, cudaEventRecord(h->ev0, st));
+    for (size_t ri = 0; ri < h->runs.size(); ++ri) {
+        const ClassRun &r = h->runs[ri];
+        CUDA_OK(h, cudaEventRecord(h->cev[ri].first, st));
+        KArgs a{};
+        a.computed = h->computed.p;
+        a.C = r.dev;
+        a.units = h->units.p + r.unit0;
+        a.n_units = r.n_units;
+        a.launches = h->launches.p;
+        a.pairs = h->pairs.p;
+        a.prims = h->prims.p;
+        a.D = D_dev;
+        a.Dsh = h->Dsh.p;
+        a.n_sh = nsh;
+        a.n_ao = nao;
+        a.tau = h->plan.tau;
+        a.Jp = h->Jp.p;
+        a.Kp = h->Kp.p;
+        a.boys_tab = h->boys.p;
+        hgp_fock_kernel<<<r.grid, kThreads, (size_t)r.dev.sm_total * sizeof(double), st>>>(a);
+        ++launches;
+        CUDA_OK(h, cudaEventRecord(h->cev[ri].second, st));
+    }
+    h->built = true;
+    CUDA_OK(h, cudaEventRecord(h->ev1, st));
+    close_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(h->Jp.p, h->Kp.p, nao, J_dev, K_dev, G_dev);
+    ++launches;
+    CUDA_OK(h, cudaGetLastError());
+    h->last_launches = launches;
+    return FJB_OK;
+}
+
+int fjb_fock_build_host(fjb_handle *h, const double *D_host, double *J_host, double *K_host,
+                        double *G_host, int precision, double threshold) {
+    if (!h || !D_host) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    cudaSetDevice(h->device);
+    const size_t nn = (size_t)h->basis.n_ao * h->basis.n_ao;
+    try {
+        h->hD.alloc(nn);
+        h->hJ.alloc(nn);
+        h->hK.alloc(nn);
+        h->hG.alloc(nn);
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, e.what());
+    }
+    CUDA_OK(h, cudaMemcpy(h->hD.p, D_host, nn * sizeof(double), cudaMemcpyHostToDevice));
+    int rc = fjb_fock_build(h, h->hD.p, J_host ? h->hJ.p : nullptr, K_host ? h->hK.p : nullptr,
+                            G_host ? h->hG.p : nullptr, precision, threshold, nullptr);
+    if (rc) return rc;
+    if (J_host) CUDA_OK(h, cudaMemcpy(J_host, h->hJ.p, nn * sizeof(double), cudaMemcpyDeviceToHost));
+    if (K_host) CUDA_OK(h, cudaMemcpy(K_host, h->hK.p, nn * sizeof(double), cudaMemcpyDeviceToHost));
+    if (G_host) CUDA_OK(h, cudaMemcpy(G_host, h->hG.p, nn * sizeof(double), cudaMemcpyDeviceToHost));
+    CUDA_OK(h, cudaDeviceSynchronize());
+    return FJB_OK;
+}
+
+int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_dev, int64_t *offsets) {
+    if (!h || !quartets || n < 0 || !offsets) return fail(h, FJB_E_ARG, "null argument");
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    cudaSetDevice(h->device);
+    const int nsh = (int)h->basis.shells.size();
+    struct Item {
+        int q;
+        std::tuple<int, int, int, int> key;
+    };
+    std::vector<PairRec> pr;
+    std::vector<PrimRec> pm;
+    std::vector<LaunchRec> lr;
+    std::map<std::tuple<int, int, int, int>, std::vector<int>> by_class;
+    std::map<std::tuple<int, int, int, int>, std::pair<int, int>> deg;
+    offsets[0] = 0;
+    auto add_pair = [&](int a, int b) {
+        const HostShell &sa = h->basis.shells[a], &sb = h->basis.shells[b];
+        int K = (int)(sa.exps.size() * sb.exps.size());
+        if (K > FJB_MAX_PRIM_PAIRS) throw std::length_error("degree exceeds MAX_PRIM_PAIRS = 128");
+        pr.push_back(pair_record(h->basis, a, b, 0.0, (int)pm.size(), K));
+        for (int k = 0; k < K; ++k) pm.push_back(prim_record(sa, sb, k));
+        return K;
+    };
+    try {
+        for (int i = 0; i < n; ++i) {
+            int q[4];
+            for (int k = 0; k < 4; ++k) {
+                q[k] = quartets[4 * i + k];
+                if (q[k] < 0 || q[k] >= nsh) return fail(h, FJB_E_ARG, "shell index out of range");
+            }
+            int nabcd = 1;
+            for (int k = 0; k < 4; ++k) nabcd *= ncart(h->basis.shells[q[k]].l);
+            offsets[i + 1] = offsets[i] + nabcd;
+            LaunchRec r{};
+            r.bra_pair0 = (int)pr.size();
+            r.n_bra = 1;
+            int kab = add_pair(q[0], q[1]);
+            r.ket_pair0 = (int)pr.size();
+            r.n_ket = 1;
+            int kcd = add_pair(q[2], q[3]);
+            lr.push_back(r);
+            auto key = std::make_tuple(h->basis.shells[q[0]].l, h->basis.shells[q[1]].l, h->basis.shells[q[2]].l,
+                                       h->basis.shells[q[3]].l);
+            by_class[key].push_back(i);
+            auto &d = deg[key];
+            d.first = std::max(d.first, kab);
+            d.second = std::max(d.second, kcd);
+        }
+        DevBuf<PairRec> dpr;
+        DevBuf<PrimRec> dpm;
+        DevBuf<LaunchRec> dlr;
+        dpr.upload(pr);
+        dpm.upload(pm);
+        dlr.upload(lr);
+        if (int rc = ensure_smem_attr(h)) return rc;
+        for (auto &kv : by_class) {
+            auto [la, lb, lc, ld] = kv.first;
+            ClassEntry &ce = h->cls(la, lb, lc, ld);
+            ClassDev dev = ce.dev(deg[kv.first].first, deg[kv.first].second);
+            std::vector<Unit> us;
+            std::vector<int64_t> toff;
+            for (int qi : kv.second) {
+                us.push_back(Unit{qi, 0, 0, 1});
+                toff.push_back(offsets[qi]);
+            }
+            DevBuf<Unit> du;
+            DevBuf<int64_t> dto;
+            du.upload(us);
+            dto.upload(toff);
+            KArgs a{};
+            a.C = dev;
+            a.units = du.p;
+            a.n_units = (int)us.size();
+            a.launches = dlr.p;
+            a.pairs = dpr.p;
+            a.prims = dpm.p;
+            a.n_sh = nsh;
+            a.n_ao = h->basis.n_ao;
+            a.tau = -1.0;
+            a.tap_out = out_dev;
+            a.tap_off = dto.p;
+            a.boys_tab = h->boys.p;
+            hgp_fock_kernel<<<grid_for(dev, a.n_units), kThreads, (size_t)dev.sm_total * sizeof(double)>>>(a);
+            CUDA_OK(h, cudaGetLastError());
+            CUDA_OK(h, cudaDeviceSynchronize());
+        }
+    } catch (const std::length_error &e) {
+        return fail(h, FJB_E_LIMIT, e.what());
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, e.what());
+    }
+    return FJB_OK;
+}
+
+int fjb_boys(int m, const double *T_dev, int n, double *F_dev) {
+    if (m < 0 || m > kBoysMaxM - kBoysTaylor + 1 || n < 0 || !T_dev || !F_dev)
+        return fail(nullptr, FJB_E_ARG, "boys: order out of range or null argument");
+    static DevBuf<double> *tab = nullptr;
+    if (!tab) {
+        tab = new DevBuf<double>();
+        try {
+            tab->upload(boys_table());
+        } catch (const std::exception &e) {
+            return fail(nullptr, FJB_E_CUDA, e.what());
+        }
+    }
+    if (n == 0) return FJB_OK;
+    boys_kernel<<<(n + 127) / 128, 128>>>(m, T_dev, n, F_dev, tab->p);
+    CUDA_OK(nullptr, cudaGetLastError());
+    CUDA_OK(nullptr, cudaDeviceSynchronize());
+    return FJB_OK;
+}
+
+int fjb_last_build_stats(const fjb_handle *hc, double *ms, int *n_launches) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h) return fail(nullptr, FJB_E_ARG, "null handle");
+    if (ms) {
+        float f = 0.f;
+        CUDA_OK(h, cudaEventSynchronize(h->ev1));
+        CUDA_OK(h, cudaEventElapsedTime(&f, h->ev0, h->ev1));
+        *ms = f;
+    }
+    if (n_launches) *n_launches = h->last_launches;
+    return FJB_OK;
+}
+
+int fjb_launch_stats(const fjb_handle *hc, fjb_launch_stat *out, int64_t n) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h || !out) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
+    if (n < (int64_t)h->lstat.size()) return fail(h, FJB_E_ARG, "output holds fewer entries than launches");
+    std::vector<unsigned long long> c(h->lstat.size(), 0);
+    if (h->device >= 0 && h->built && !c.empty()) {
+        CUDA_OK(h, cudaEventSynchronize(h->ev1));
+        CUDA_OK(h, cudaMemcpy(c.data(), h->computed.p, c.size() * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost));
+    }
+    for (size_t i = 0; i < h->lstat.size(); ++i) {
+        out[i] = h->lstat[i];
+        out[i].computed = (int64_t)c[i];
+    }
+    return FJB_OK;
+}
+
+int fjb_class_stats(const fjb_handle *hc, fjb_class_stat *out, int64_t n, int64_t *n_classes) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h) return fail(h, FJB_E_ARG, "null argument");
+    if (n_classes) *n_classes = (int64_t)h->runs.size();
+    if (!out) return FJB_OK;
+    if (!h->built) return fail(h, FJB_E_STATE, "no build yet");
+    for (size_t i = 0; i < h->runs.size() && (int64_t)i < n; ++i) {
+        const ClassDev &d = h->runs[i].dev;
+        float ms = 0.f;
+        CUDA_OK(h, cudaEventSynchronize(h->cev[i].second));
+        CUDA_OK(h, cudaEventElapsedTime(&ms, h->cev[i].first, h->cev[i].second));
+        out[i] = fjb_class_stat{d.la, d.lb, d.lc, d.ld, (double)ms, (int64_t)h->runs[i].n_units};
+    }
+    return FJB_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+__global__ void fma_probe_kernel(T *out, int iters, T a, T b) {
+    T x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = (T)(threadIdx.x + k) * (T)1e-3;
+    for (int i = 0; i < iters; ++i)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += x[k];
+    if (s == (T)12345.678) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+template <typename T>
+int run_probe(int reps, double *tflops) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int threads = 256, blocks = sms * 8, iters = 4096;
+    T *out = nullptr;
+    if (cudaMalloc(&out, sizeof(T) * threads * blocks) != cudaSuccess)
+        return fail(nullptr, FJB_E_CUDA, "cudaMalloc failed");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 1e30;
+    for (int r = 0; r < reps + 1; ++r) {
+        cudaEventRecord(e0);
+        fma_probe_kernel<T><<<blocks, threads>>>(out, iters, (T)0.999999, (T)1e-7);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (r > 0) best = std::min(best, (double)ms);  // the first launch warms up
+    }
+    cudaError_t err = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (err != cudaSuccess) return fail(nullptr, FJB_E_CUDA, cudaGetErrorString(err));
+    *tflops = 2.0 * 8.0 * iters * (double)threads * blocks / (best * 1e-3) / 1e12;
+    return FJB_OK;
+}
+
+}  // namespace
+
+extern "C" int fjb_fma_probe(int fp32, int reps, double *tflops) {
+    if (!tflops || reps < 1) return fail(nullptr, FJB_E_ARG, "bad argument");
+    return fp32 ? run_probe<float>(reps, tflops) : run_probe<double>(reps, tflops);
+}

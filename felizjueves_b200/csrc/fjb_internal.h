@@ -1,0 +1,93 @@
+// fjb_internal.h -- structures shared by the host runtime (C++) and the
+// sm_100a kernels.  Not part of the public ABI (include/fjb.h is).
+#pragma once
+#include <cstdint>
+
+namespace fjb {
+
+constexpr int kMaxL = 3;          // per shell in the Fock build
+constexpr int kMaxLQuartet = 4 * kMaxL;
+constexpr int kBoysMaxM = 24;     // orders held by the Taylor table
+constexpr int kBoysTaylor = 7;    // Taylor terms (orders m .. m+6)
+constexpr double kBoysDelta = 0.05;
+constexpr double kBoysTMax = 40.0;  // table covers [0, kBoysTMax]
+constexpr int kBoysNT = 801;        // kBoysTMax / kBoysDelta + 1
+constexpr int kThreads = 128;       // threads per CTA of the HGP kernel
+constexpr int kKetChunk = 64;       // ket pairs per work unit
+constexpr int kNumScalars = 17;     // per-primitive-quartet VRR scalars
+
+// One VRR node update, 16 bytes.  value(dst) =
+//   A_d V[s0] + B_d V[s1] + c2 (C V[s2] - Dc V[s3]) + c4 E V[s4]
+// with (A, B, C, Dc) the bra set (PA, WP, 1/2p, rho/(2p^2)) for kind 0 and
+// the ket set (QC, WQ, 1/2q, rho/(2q^2)) for kind 1; E = 1/(2(p+q)).
+// Absent terms point at node 0, which always holds 0.
+struct VOp {
+    uint16_t dst, s0, s1, s2, s3, s4;
+    uint8_t d, kind, c2, c4;
+};
+static_assert(sizeof(VOp) == 16, "VOp is 16 bytes");
+
+// One HRR transform term: out += coef[cidx] * in[src].
+struct HTerm {
+    uint16_t src, cidx;
+};
+
+// A binomial coefficient of the HRR: binom * sep_x^px sep_y^py sep_z^pz.
+struct HCoef {
+    float binom;
+    uint8_t px, py, pz, pad;
+};
+
+// A primitive pair as staged for the kernels: P, X = P - A (first centre),
+// zeta, U = c_a c_b (pi/zeta)^{3/2} exp(-alpha beta/zeta |AB|^2).
+struct PrimRec {
+    double P[3], X[3], zeta, U;
+};
+
+// A contracted shell pair (canonical: la <= lb, lower index first on a tie).
+struct PairRec {
+    int32_t a, b, ao_a, ao_b;
+    int32_t prim0, nprim, pad0, pad1;
+    double G;
+    double AB[3];
+};
+
+// One launch: a bra batch against a ket batch (bra <= ket).
+struct LaunchRec {
+    int32_t bra_pair0, n_bra, ket_pair0, n_ket;
+    int32_t diag, cls, pad0, pad1;
+    int64_t qbase;  // index of this launch's first quartet in screen order
+};
+
+// A work unit: bra pair ib of launch `launch`, ket pairs [k0, k1).
+struct Unit {
+    int32_t launch, ib, k0, k1;
+};
+
+// Device view of one class's tables (all pointers are device pointers).
+struct ClassDev {
+    int la, lb, lc, ld;
+    int na, nb, nc, nd, nab, ncd;
+    int L;
+    int n_nodes;      // including node 0 (zero) and node 1 (scratch)
+    int n_levels;
+    int nbe, nbf;     // boundary extents (e with la<=|e|<=la+lb, f likewise)
+    int n_cb, n_ck;   // HRR coefficient counts
+    int slots;        // primitive quartets per chunk
+    const int *level_off;   // [n_levels + 1] into ops
+    const VOp *ops;
+    const uint16_t *leaf;   // [L + 1] node of [0|0]^(m), 0 if unread
+    const uint16_t *tgt;    // [nbe * nbf] node of boundary (e, f)
+    const HCoef *cb;        // [n_cb]
+    const int *bra_off;     // [nab + 1]
+    const HTerm *bra_terms;
+    const HCoef *ck;        // [n_ck]
+    const int *ket_off;     // [ncd + 1]
+    const HTerm *ket_terms;
+    // shared-memory carve-up, in doubles
+    int sm_V, sm_bound, sm_S, sm_braP, sm_ketP, sm_cb, sm_ck, sm_D, sm_Jab;
+    int sm_total;
+    int vregion;      // doubles in the V region (also holds X and Y)
+};
+
+}  // namespace fjb

@@ -1,0 +1,94 @@
+// fock_kernels.cuh -- sm_100a device code of the Fock build.
+//
+//   boys_eval       F_0..F_M(T): tabulated Taylor (7 terms at the nearest
+//                   0.05 node) then downward recursion below T = 40; the
+//                   erf-free large-T start F_0 = sqrt(pi/T)/2 and upward
+//                   recursion above (stable there: (2m+1)/(2T) < 1).
+//   skip6           the six-block screen of a quartet, in the reference's
+//                   operation order (walk_f.py:344-351; kernel_f.py:152-163).
+//   hgp_fock_kernel one CTA per work unit (a bra shell pair and a chunk of
+//                   its kets); per computed quartet: staged primitive pairs,
+//                   per-primitive-quartet scalars and Boys leaves, the VRR
+//                   program level by level over (node x primitive quartet),
+//                   the boundary contraction, the two HRR transforms, and
+//                   the six-block digest into J and K (thread-private sums,
+//                   FP64 atomics for the five ket-dependent blocks, the bra
+//                   block F_ab accumulated in shared memory and flushed once
+//                   per unit, kernel_f.py:94-131).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fjb_internal.h"
+
+namespace fjb {
+
+struct KArgs {
+    ClassDev C;
+    const Unit *units;
+    int n_units;
+    const LaunchRec *launches;
+    const PairRec *pairs;
+    const PrimRec *prims;
+    const double *D;
+    const double *Dsh;
+    int n_sh, n_ao;
+    double tau;
+    double *Jp, *Kp;
+    double *tap_out;        // ERI tap mode when non-null
+    const int64_t *tap_off; // per unit
+    const double *boys_tab;
+    const uint8_t *route;   // per unit ket flags, routed mode (null: all FP64)
+    double route_thresh;
+    unsigned long long *computed;  // per launch: quartets computed (null: not counted)
+};
+
+__device__ __forceinline__ void boys_eval(int M, double T, double *F, const double *__restrict__ tab) {
+    if (T < kBoysTMax) {
+        const int i = __double2int_rn(T * (1.0 / kBoysDelta));
+        const double d = (double)i * kBoysDelta - T;
+        const double *row = tab + (size_t)i * (kBoysMaxM + 1) + M;
+        double f = __ldg(row + 6);
+        f = __ldg(row + 5) + f * d * (1.0 / 6.0);
+        f = __ldg(row + 4) + f * d * (1.0 / 5.0);
+        f = __ldg(row + 3) + f * d * (1.0 / 4.0);
+        f = __ldg(row + 2) + f * d * (1.0 / 3.0);
+        f = __ldg(row + 1) + f * d * (1.0 / 2.0);
+        f = __ldg(row + 0) + f * d;
+        F[M] = f;
+        if (M > 0) {
+            const double e = exp(-T), t2 = 2.0 * T;
+            for (int m = M - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) / (double)(2 * m + 1);
+        }
+    } else {
+        const double e = exp(-T), h = 0.5 / T;
+        F[0] = 0.5 * sqrt(3.141592653589793 / T);
+        for (int m = 0; m < M; ++m) F[m + 1] = ((double)(2 * m + 1) * F[m] - e) * h;
+    }
+}
+
+// The six-block screen: dmax over |w_b| Dsh_b in BLOCKS order (ab, cd, ac,
+// ad, bc, bd) with |w| = (2, 2, 1/2, 1/2, 1/2, 1/2), then
+// G_ab (G_cd dmax) < tau.  Multiplies and compares only: bit-exact.
+__device__ __forceinline__ bool skip6(const double *__restrict__ Dsh, int n_sh, int a, int b, int c,
+                                      int d, double Gb, double Gk, double tau) {
+    double dmax = 2.0 * __ldg(Dsh + (size_t)a * n_sh + b);
+    double t = 2.0 * __ldg(Dsh + (size_t)c * n_sh + d);
+    if (dmax < t) dmax = t;
+    t = 0.5 * __ldg(Dsh + (size_t)a * n_sh + c);
+    if (dmax < t) dmax = t;
+    t = 0.5 * __ldg(Dsh + (size_t)a * n_sh + d);
+    if (dmax < t) dmax = t;
+    t = 0.5 * __ldg(Dsh + (size_t)b * n_sh + c);
+    if (dmax < t) dmax = t;
+    t = 0.5 * __ldg(Dsh + (size_t)b * n_sh + d);
+    if (dmax < t) dmax = t;
+    return __dmul_rn(Gb, __dmul_rn(Gk, dmax)) < tau;
+}
+
+__device__ __forceinline__ double ipow(double x, int n) {
+    double r = 1.0;
+    for (int k = 0; k < n; ++k) r *= x;
+    return r;
+}
+
+}  // namespace fjb

@@ -1,0 +1,349 @@
+"""The Fock build's host surface: the reference's driver-level API over the
+C ABI of libfjb.so, with device memory and streams from PyTorch.
+
+Mirrors (paths within the reference project):
+
+* `f_launches(basis, D, *, tau, n)`  eri/fock/launch_f.py:390 -> FPlan,
+  the pair stream as data (FPair, FBatch, FLaunch, counts()).  The bound is
+  the reference's primitive_schwarz_bounds (ao/pairs.py:537), built in
+  C++; it is not injectable here.
+* `fock_two_electron(basis, D, *, tau, n)`  eri/fock/fock.py:166
+  fock_two_electron_reference -> G = J - K/2, and
+  `coulomb_exchange(basis, D, ...)`  eri/fock/fock.py:126 -> (J, K).
+* `eri_block(basis, a, b, c, d)`  eri/eri.py:145 -> the (ab|cd) block.
+* `FockEngine`  the reusable form: plan once per (basis, tau, n), then build
+  for any symmetric D, on device tensors (torch) or host arrays (numpy).
+
+Refusals are the reference's: an asymmetric or non-finite D, a bad tau, an
+l or a contraction degree above the compiled limits raise ValueError.  There
+is no CPU path: every number comes from the sm_100a kernels.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Iterator
+
+import numpy as np
+
+from . import _lib
+from .shell import Basis
+
+
+@dataclass(frozen=True)
+class FPair:
+    a: int
+    b: int
+    la: int
+    lb: int
+    n_prim: int
+    prims: tuple[int, ...]
+    prim_G: tuple[float, ...]
+    G: float
+    dmax: float
+    key: float
+    mag: int
+
+    @property
+    def degree(self) -> int:
+        return len(self.prims)
+
+
+@dataclass(frozen=True)
+class FBatch:
+    la: int
+    lb: int
+    degree: int
+    mag: int
+    magnitude: float
+    pairs: tuple[FPair, ...]
+
+    @property
+    def g_max(self) -> float:
+        return max(p.G for p in self.pairs)
+
+
+@dataclass(frozen=True)
+class FLaunch:
+    bra: int
+    ket: int
+    am: tuple[int, int, int, int]
+
+
+@dataclass(frozen=True)
+class FPlan:
+    tau: float
+    n: int
+    magnitudes: tuple[float, ...]
+    eps: float
+    g_max: float
+    batches: tuple[FBatch, ...]
+    launches: tuple[FLaunch, ...]
+    screened: tuple[tuple[int, int], ...]
+    deleted: tuple[tuple[int, int], ...]
+    n_prim_total: int
+    quartets_launched: int = 0
+    units: int = 0
+
+    def __iter__(self) -> Iterator[FLaunch]:
+        return iter(self.launches)
+
+    def __len__(self) -> int:
+        return len(self.launches)
+
+    @property
+    def pairs(self) -> tuple[FPair, ...]:
+        return tuple(p for b in self.batches for p in b.pairs)
+
+    @property
+    def n_prim_kept(self) -> int:
+        return sum(p.degree for p in self.pairs)
+
+    def counts(self) -> dict[str, int]:
+        nb = len(self.batches)
+        return {"pairs": len(self.pairs) + len(self.deleted),
+                "pairs_deleted": len(self.deleted),
+                "primitive_pairs": self.n_prim_total,
+                "primitive_pairs_pruned": self.n_prim_total - self.n_prim_kept,
+                "batches": nb, "batch_pairs": nb * (nb + 1) // 2,
+                "batch_pairs_screened": len(self.screened),
+                "launches": len(self.launches)}
+
+
+def _checked_density(basis: Basis, D) -> np.ndarray:
+    n = basis.n_ao
+    try:
+        A = np.asarray(D, dtype=np.float64)
+    except (TypeError, ValueError):
+        raise ValueError(f"D is not an {n} x {n} matrix") from None
+    if A.shape != (n, n):
+        raise ValueError(f"D is not an {n} x {n} matrix")
+    if not np.all(np.isfinite(A)):
+        raise ValueError("D has a non-finite entry")
+    if not np.array_equal(A, A.T):
+        i, j = map(int, np.argwhere(A != A.T)[0])
+        raise ValueError(f"D is not symmetric: D[{i}][{j}] = {A[i, j]!r} but "
+                         f"D[{j}][{i}] = {A[j, i]!r}. An asymmetric density is "
+                         "rejected, not symmetrised")
+    return np.ascontiguousarray(A)
+
+
+def _checked_tau(tau) -> float:
+    import math
+    if not (isinstance(tau, (int, float)) and not isinstance(tau, bool)
+            and math.isfinite(tau) and tau >= 0.0):
+        raise ValueError(f"tau = {tau!r} is not a finite float >= 0")
+    return float(tau)
+
+
+class FockEngine:
+    """One basis on one GPU.  `plan(D, tau, n)` builds and stages the pair
+    stream; `build(D)` runs the fused J/K/G build."""
+
+    def __init__(self, basis: Basis, device: int = 0):
+        if not isinstance(basis, Basis):
+            raise ValueError(f"{basis!r} is not a Basis")
+        self.basis = basis
+        self.device = int(device)
+        self._L = _lib.load()
+        f = basis.flat()
+        self._flat = f  # keep alive for the call
+        bt = _lib.Basis_t(len(basis.shells), f["l"].ctypes.data, f["centre"].ctypes.data,
+                          f["prim0"].ctypes.data, f["nprim"].ctypes.data,
+                          f["exps"].ctypes.data, f["coefs"].ctypes.data)
+        h = C.c_void_p()
+        _lib.check(self._L.fjb_create(C.byref(h), C.byref(bt), self.device))
+        self._h = h
+        self._plan = None
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.fjb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def n_ao(self) -> int:
+        return self.basis.n_ao
+
+    # -- the plan ----------------------------------------------------------
+    def plan(self, D, tau: float = 1e-12, n: int = 4) -> FPlan:
+        A = _checked_density(self.basis, D)
+        tau = _checked_tau(tau)
+        if type(n) is not int or n < 1:
+            raise ValueError(f"n = {n!r} is not an int >= 1 (the number of eq. 29 magnitudes)")
+        _lib.check(self._L.fjb_plan(self._h, A.ctypes.data, tau, n), self._h)
+        self._tau = tau
+        self._plan = self._export(n)
+        return self._plan
+
+    def counts_raw(self) -> dict[str, int]:
+        c = _lib.PlanCounts_t()
+        _lib.check(self._L.fjb_plan_counts(self._h, C.byref(c)), self._h)
+        return {k: int(getattr(c, k)) for k, _ in c._fields_}
+
+    def _export(self, n: int) -> FPlan:
+        c = self.counts_raw()
+        nb, nk, npr = c["batches"], c["kept_pairs"], c["kept_prims"]
+        arr = {
+            "batch_key": np.zeros(4 * nb, np.int32), "batch_npairs": np.zeros(nb, np.int32),
+            "pair_ab": np.zeros(2 * nk, np.int32), "pair_mag": np.zeros(nk, np.int32),
+            "prims": np.zeros(npr, np.int32), "pair_G": np.zeros(nk), "pair_dmax": np.zeros(nk),
+            "pair_key": np.zeros(nk), "prim_G": np.zeros(npr),
+            "launches": np.zeros(2 * c["launches"], np.int32),
+            "screened": np.zeros(2 * c["batch_pairs_screened"], np.int32),
+            "deleted": np.zeros(2 * c["pairs_deleted"], np.int32),
+            "magnitudes": np.zeros(n), "eps": np.zeros(1), "g_max": np.zeros(1)}
+        lists = _lib.PlanLists_t(**{k: v.ctypes.data for k, v in arr.items()})
+        _lib.check(self._L.fjb_plan_export(self._h, C.byref(lists)), self._h)
+        shells = self.basis.shells
+        bk = arr["batch_key"].reshape(-1, 4)
+        pab = arr["pair_ab"].reshape(-1, 2)
+        batches, ip, ik = [], 0, 0
+        mags = tuple(float(x) for x in arr["magnitudes"])
+        for bi in range(nb):
+            la, lb, deg, mag = map(int, bk[bi])
+            pairs = []
+            for _ in range(int(arr["batch_npairs"][bi])):
+                a, b = map(int, pab[ip])
+                pairs.append(FPair(a, b, la, lb, shells[a].n_prim * shells[b].n_prim,
+                                   tuple(int(x) for x in arr["prims"][ik:ik + deg]),
+                                   tuple(float(x) for x in arr["prim_G"][ik:ik + deg]),
+                                   float(arr["pair_G"][ip]), float(arr["pair_dmax"][ip]),
+                                   float(arr["pair_key"][ip]), int(arr["pair_mag"][ip])))
+                ip += 1
+                ik += deg
+            batches.append(FBatch(la, lb, deg, mag, mags[mag], tuple(pairs)))
+        L = arr["launches"].reshape(-1, 2)
+        launches = tuple(FLaunch(int(i), int(j), (batches[i].la, batches[i].lb,
+                                                  batches[j].la, batches[j].lb))
+                         for i, j in L)
+        return FPlan(self._tau, n, mags, float(arr["eps"][0]),
+                     float(arr["g_max"][0]), tuple(batches), launches,
+                     tuple(map(tuple, arr["screened"].reshape(-1, 2).tolist())),
+                     tuple(map(tuple, arr["deleted"].reshape(-1, 2).tolist())),
+                     c["primitive_pairs"], c["quartets_launched"], c["units"])
+
+    # -- builds --------------------------------------------------------------
+    def _require_plan(self):
+        if self._plan is None:
+            raise RuntimeError("no plan: call plan(D, tau, n) first")
+
+    def build(self, D, *, J=None, K=None, G=None, precision: int = _lib.FJB_FP64,
+              threshold: float = 0.0, stream=None):
+        """Device build: D (torch, cuda, float64, n x n, symmetric) in; J, K,
+        G (allocated if not given) out.  Stream-ordered, not synchronised."""
+        import torch
+        self._require_plan()
+        n = self.n_ao
+        if not (isinstance(D, torch.Tensor) and D.is_cuda and D.dtype == torch.float64
+                and tuple(D.shape) == (n, n) and D.is_contiguous()):
+            raise ValueError(f"D must be a contiguous cuda float64 tensor of shape ({n}, {n})")
+        out = []
+        for M in (J, K, G):
+            if M is None:
+                M = torch.empty((n, n), dtype=torch.float64, device=D.device)
+            out.append(M)
+        st = stream if stream is not None else torch.cuda.current_stream(D.device)
+        _lib.check(self._L.fjb_fock_build(self._h, D.data_ptr(), out[0].data_ptr(),
+                                          out[1].data_ptr(), out[2].data_ptr(),
+                                          int(precision), float(threshold),
+                                          C.c_void_p(st.cuda_stream)), self._h)
+        return tuple(out)
+
+    def build_host(self, D, *, precision: int = _lib.FJB_FP64, threshold: float = 0.0):
+        """Host build through the C ABI's host-buffer entry point: numpy in,
+        (J, K, G) numpy out."""
+        self._require_plan()
+        A = _checked_density(self.basis, D)
+        n = self.n_ao
+        J, K, G = (np.empty((n, n)) for _ in range(3))
+        _lib.check(self._L.fjb_fock_build_host(self._h, A.ctypes.data, J.ctypes.data,
+                                               K.ctypes.data, G.ctypes.data,
+                                               int(precision), float(threshold)), self._h)
+        return J, K, G
+
+    def last_build_stats(self) -> tuple[float, int]:
+        ms, nl = C.c_double(), C.c_int()
+        _lib.check(self._L.fjb_last_build_stats(self._h, C.byref(ms), C.byref(nl)), self._h)
+        return float(ms.value), int(nl.value)
+
+    def launch_stats(self) -> list[dict]:
+        """Per launch: class, degrees, quartets met and computed by the last
+        build."""
+        n = self.counts_raw()["launches"]
+        arr = (_lib.LaunchStat_t * max(n, 1))()
+        _lib.check(self._L.fjb_launch_stats(self._h, C.cast(arr, C.c_void_p), n), self._h)
+        return [{k: getattr(arr[i], k) for k, _ in _lib.LaunchStat_t._fields_} for i in range(n)]
+
+    def class_stats(self) -> list[dict]:
+        """Per class kernel of the last build: class, ms, work units."""
+        nc = C.c_int64()
+        _lib.check(self._L.fjb_class_stats(self._h, None, 0, C.byref(nc)), self._h)
+        arr = (_lib.ClassStat_t * max(nc.value, 1))()
+        _lib.check(self._L.fjb_class_stats(self._h, C.cast(arr, C.c_void_p), nc.value,
+                                           C.byref(nc)), self._h)
+        return [{k: getattr(arr[i], k) for k, _ in _lib.ClassStat_t._fields_}
+                for i in range(nc.value)]
+
+    def screen_mask(self, D) -> np.ndarray:
+        """Per launched quartet (launch, bra pair, ket pair order), 1 when
+        the six-block screen skips it (walk_f.py:344-380)."""
+        import torch
+        self._require_plan()
+        Dt = torch.as_tensor(_checked_density(self.basis, D if not hasattr(D, "cpu") else D.cpu().numpy()),
+                             device=f"cuda:{self.device}")
+        m = torch.zeros(self._plan.quartets_launched, dtype=torch.uint8, device=Dt.device)
+        _lib.check(self._L.fjb_screen_mask(self._h, Dt.data_ptr(), m.data_ptr(),
+                                           C.c_void_p(torch.cuda.current_stream(Dt.device).cuda_stream)),
+                   self._h)
+        torch.cuda.synchronize(Dt.device)
+        return m.cpu().numpy()
+
+    def eri_blocks(self, quartets) -> list[np.ndarray]:
+        """(ab|cd) of ordered shell quartets, each a (n_a n_b, n_c n_d) array
+        in the reference's eri_block layout."""
+        import torch
+        q = np.ascontiguousarray(np.asarray(quartets, np.int32).reshape(-1, 4))
+        off = np.zeros(len(q) + 1, np.int64)
+        sizes = [np.prod([self.basis.shells[s].n_cart for s in row]) for row in q]
+        total = int(np.sum(sizes)) if len(q) else 0
+        out = torch.zeros(max(total, 1), dtype=torch.float64, device=f"cuda:{self.device}")
+        _lib.check(self._L.fjb_eri_blocks(self._h, q.ctypes.data, len(q), out.data_ptr(),
+                                          off.ctypes.data), self._h)
+        flat = out.cpu().numpy()
+        res = []
+        for i, row in enumerate(q):
+            na, nb, nc, nd = (self.basis.shells[s].n_cart for s in row)
+            res.append(flat[off[i]:off[i + 1]].reshape(na * nb, nc * nd))
+        return res
+
+
+def f_launches(basis: Basis, D, *, tau: float, n: int, device: int = 0) -> FPlan:
+    eng = FockEngine(basis, device)
+    return eng.plan(D, tau, n)
+
+
+def coulomb_exchange(basis: Basis, D, *, tau: float = 0.0, n: int = 4, device: int = 0):
+    """(J, K) of the total density D (numpy arrays), on the GPU."""
+    eng = FockEngine(basis, device)
+    eng.plan(D, tau, n)
+    J, K, _ = eng.build_host(D)
+    return J, K
+
+
+def fock_two_electron(basis: Basis, D, *, tau: float = 0.0, n: int = 4, device: int = 0):
+    """G = J - K/2 of the total closed-shell density D, on the GPU."""
+    eng = FockEngine(basis, device)
+    eng.plan(D, tau, n)
+    return eng.build_host(D)[2]
+
+
+def eri_block(basis: Basis, a: int, b: int, c: int, d: int, device: int = 0) -> np.ndarray:
+    return FockEngine(basis, device).eri_blocks([(a, b, c, d)])[0]

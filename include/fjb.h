@@ -1,0 +1,185 @@
+/*
+ * fjb.h -- the C ABI of libfjb.so, a B200 (sm_100a) Fock-build engine.
+ *
+ * Plain C: pointers, sizes, status codes.  No torch or CUDA types in the
+ * signatures (a stream is passed as `void*`, a cudaStream_t; NULL is the
+ * legacy default stream).  Every function returns 0 on success or a negative
+ * FJB_E* code; fjb_last_error() then holds a one-line message.
+ *
+ * Each entry point names the reference interface it replaces (paths within
+ * the reference project, whatDiracIsCooking/FelizJueves):
+ *
+ *   fjb_create        ao/shell.py:110-165   Shell / Basis (l, centre,
+ *                                            exponents, coefficients; AO
+ *                                            offsets in Basis order)
+ *   fjb_plan          eri/fock/launch_f.py:390-466  f_launches(basis, D, *,
+ *                                            bound, tau, n) with the bound
+ *                                            ao/pairs.py:528-541
+ *                                            primitive_schwarz_bounds
+ *   fjb_plan_counts,
+ *   fjb_plan_export   launch_f.py:312-345   FPlan.counts() and the lists
+ *                                            (batches, pairs, prims,
+ *                                            launches, screened, deleted)
+ *   fjb_screen_mask   eri/fock/walk_f.py:344-380  the six-block in-kernel
+ *                                            screen, per launched quartet
+ *   fjb_fock_build    eri/fock/walk_f.py:306-415 + kernel_f.py:655 +
+ *                                            kernel_f.py:621 close: the fused
+ *                                            G = J - K/2 build, and J and K
+ *                                            (eri/fock/fock.py:126-176 define
+ *                                            them; j.py:436, k.py:482)
+ *   fjb_eri_blocks    eri/eri.py:133-145 eri_block and
+ *                     eri/hgp_drive.py:206 (the per-quartet ERI tap)
+ *   fjb_boys          emit/_c.py:144-210 fj_boys<M> (device Boys)
+ *   fjb_last_error,
+ *   fjb_destroy       the reference raises ValueError with a message
+ *
+ * Units and conventions are the reference's: Bohr, Cartesian AOs in
+ * cartesians(l) order (i desc, then j desc), coefficients multiplying
+ * UNNORMALISED primitives; D is n_ao x n_ao row-major, finite and EXACTLY
+ * symmetric (refused otherwise, never symmetrised).
+ */
+#ifndef FJB_H
+#define FJB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FJB_OK 0
+#define FJB_E_ARG (-1)      /* a refused argument (the reference's ValueError) */
+#define FJB_E_CUDA (-2)     /* a CUDA runtime error */
+#define FJB_E_STATE (-3)    /* called out of order (e.g. build before plan) */
+#define FJB_E_LIMIT (-4)    /* above a compiled limit (L, degree) */
+#define FJB_E_TIMEOUT (-5)  /* a bounded device wait ran out */
+#define FJB_E_PLAN (-6)     /* the plan's soundness check failed */
+
+#define FJB_MAX_L 3            /* per shell, Fock build */
+#define FJB_MAX_PRIM_PAIRS 128 /* kernel_f.py:196-203 MAX_PRIM_PAIRS */
+
+/* precision modes of fjb_fock_build */
+#define FJB_FP64 0   /* every quartet in FP64 */
+#define FJB_ROUTED 1 /* quartets under the magnitude threshold run E/R/VRR in FP32 */
+
+typedef struct fjb_handle fjb_handle;
+
+/* A basis: per shell its l, centre (3 doubles), first primitive index and
+ * primitive count into exps/coefs. */
+typedef struct fjb_basis {
+    int32_t n_shells;
+    const int32_t *l;
+    const double *centre;
+    const int32_t *prim0;
+    const int32_t *nprim;
+    const double *exps;
+    const double *coefs;
+} fjb_basis;
+
+typedef struct fjb_plan_counts_t {
+    int64_t pairs, pairs_deleted, primitive_pairs, primitive_pairs_pruned;
+    int64_t batches, batch_pairs, batch_pairs_screened, launches;
+    int64_t kept_pairs, kept_prims, units, quartets_launched;
+} fjb_plan_counts_t;
+
+/* The plan's lists, written into caller-owned host arrays sized from
+ * fjb_plan_counts (any pointer may be NULL to skip that list):
+ *   batch_key[4*batches]   (la, lb, degree, mag), batches in plan order
+ *   batch_npairs[batches]
+ *   pair_ab[2*kept_pairs]  (a, b) of each kept pair, batch by batch, each
+ *                          batch's pairs in their sorted order
+ *   pair_G, pair_dmax, pair_key [kept_pairs]; pair_mag [kept_pairs]
+ *   prims[kept_prims]      kept primitive-pair indices (i*K_b + j), per pair
+ *   prim_G[kept_prims]
+ *   launches[2*launches], screened[2*batch_pairs_screened],
+ *   deleted[2*pairs_deleted]                                               */
+typedef struct fjb_plan_lists {
+    int32_t *batch_key, *batch_npairs, *pair_ab, *pair_mag, *prims;
+    double *pair_G, *pair_dmax, *pair_key, *prim_G;
+    int32_t *launches, *screened, *deleted;
+    double *magnitudes; /* [n_mag] */
+    double *eps, *g_max; /* scalars */
+} fjb_plan_lists;
+
+const char *fjb_last_error(const fjb_handle *h);
+const char *fjb_version(void);
+
+int fjb_create(fjb_handle **out, const fjb_basis *basis, int device);
+void fjb_destroy(fjb_handle *h);
+
+/* Build the pair stream for density D (HOST pointer, n_ao^2) at threshold
+ * tau with n_mag eq.29 magnitudes, and stage it on the device.  The plan's
+ * sort inside a batch reads D; the builds that follow take any symmetric D
+ * (the in-kernel six-block screen reads the density each build is given). */
+int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag);
+int fjb_plan_counts(const fjb_handle *h, fjb_plan_counts_t *out);
+int fjb_plan_export(const fjb_handle *h, fjb_plan_lists *out);
+int fjb_n_ao(const fjb_handle *h);
+
+/* The six-block screen decision of every launched quartet, in (launch, bra
+ * pair, ket pair >= bra on the diagonal) order: mask_dev[q] = 1 when the
+ * quartet is skipped.  D_dev and mask_dev are DEVICE pointers
+ * (quartets_launched bytes). */
+int fjb_screen_mask(fjb_handle *h, const double *D_dev, uint8_t *mask_dev,
+                    void *stream);
+
+/* The fused build.  D_dev, J_dev, K_dev, G_dev are DEVICE pointers to
+ * n_ao^2 doubles (any of J/K/G may be NULL).  precision: FJB_FP64 or
+ * FJB_ROUTED (then `threshold` is the Schwarz x |D| bound under which a
+ * quartet runs its recurrences in FP32; <= 0 means the default 1e-9).
+ * Stream-ordered; nothing is synchronised. */
+int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_dev,
+                   double *G_dev, int precision, double threshold, void *stream);
+
+/* The same build through host buffers: D_host in, J/K/G_host out (any of
+ * the outputs may be NULL).  Copies in, builds, copies out, synchronises. */
+int fjb_fock_build_host(fjb_handle *h, const double *D_host, double *J_host,
+                        double *K_host, double *G_host, int precision, double threshold);
+
+/* ERI blocks (ab|cd) of n ordered shell quartets quartets[4*n], every
+ * primitive, by the same HGP recurrences as the build.  out_dev (DEVICE)
+ * receives the blocks back to back, each n_a n_b x n_c n_d row-major in the
+ * reference's eri_block layout; offsets[n+1] (HOST, filled) gives where.
+ * Synchronises. */
+int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_dev,
+                   int64_t *offsets);
+
+/* Device Boys F_0..F_m(T[i]) for n arguments into F_dev[i*(m+1) + k]
+ * (DEVICE pointers).  Synchronises. */
+int fjb_boys(int m, const double *T_dev, int n, double *F_dev);
+
+/* Elapsed device milliseconds of the last fjb_fock_build's class kernels
+ * (events recorded on the build's stream); and the number of kernel
+ * launches that build issued. */
+int fjb_last_build_stats(const fjb_handle *h, double *ms_kernels, int *n_launches);
+
+/* Per launch of the plan (launch_f.py FLaunch order): its class, the two
+ * sides' contraction degrees, the quartets it meets and the quartets the
+ * last build computed (not skipped by the six-block screen).  n = launches
+ * of fjb_plan_counts.  Synchronises on the last build. */
+typedef struct fjb_launch_stat {
+    int32_t la, lb, lc, ld, kab, kcd;
+    int64_t launched, computed;
+} fjb_launch_stat;
+int fjb_launch_stats(const fjb_handle *h, fjb_launch_stat *out, int64_t n);
+
+/* Per class kernel of the last build: its class, device milliseconds
+ * (events around the launch on the build's stream) and work units. */
+typedef struct fjb_class_stat {
+    int32_t la, lb, lc, ld;
+    double ms;
+    int64_t units;
+} fjb_class_stat;
+int fjb_class_stats(const fjb_handle *h, fjb_class_stat *out, int64_t n, int64_t *n_classes);
+
+/* Achievable CUDA-core FMA throughput (TFLOP/s, 2 flops per FMA) by
+ * independent FMA chains on every SM, best of `reps` timed launches
+ * (the method of the reference's performance/ceilings.py:17-40).
+ * fp32 = 0: FP64, 1: FP32. */
+int fjb_fma_probe(int fp32, int reps, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,383 @@
+"""Generate the golden fixtures under tests/golden/ from the reference.
+
+This script is test infrastructure. It imports the reference's own Python
+(`src/felizjueves`, pure Python + numpy) from a reference checkout and
+records its outputs on this repository's seeded workloads, plus the
+libcint/PySCF fixtures the reference tracks (`test/oracle/fixtures/*.json`).
+Nothing at test time reads the reference: the tests read only the .npz/.json
+files this script writes.
+
+    python tests/golden/make_golden.py --ref /path/to/reference [parts...]
+
+parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost (default: all
+but plan_c1 and jk_small, which take minutes).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import sys
+import time
+from functools import partial
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+REF = os.environ.get("FJB_REF")  # set in main; inherited by spawned workers
+if REF:
+    sys.path.insert(0, os.path.join(REF, "src"))
+
+
+def _ref_imports():
+    p = os.path.join(os.environ["FJB_REF"], "src")
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def ref_basis(basis):
+    from felizjueves.ao.shell import Basis, Shell
+    return Basis(tuple(Shell(s.l, s.centre, s.exponents, s.coefficients)
+                       for s in basis.shells))
+
+
+def flat_shells(shells_l, centres, exps, coefs):
+    n = len(shells_l)
+    p0, npr, ex, co = [], [], [], []
+    for e, c in zip(exps, coefs):
+        p0.append(len(ex))
+        npr.append(len(e))
+        ex.extend(e)
+        co.extend(c)
+    return dict(l=np.asarray(shells_l, np.int32),
+                centre=np.asarray(centres, np.float64).reshape(n, 3),
+                prim0=np.asarray(p0, np.int32), nprim=np.asarray(npr, np.int32),
+                exps=np.asarray(ex, np.float64),
+                coefs=np.asarray(co, np.float64))
+
+
+# --- libcint fixtures ---------------------------------------------------------
+
+LIBCINT = ["h2_sto3g", "h2o_sto3g", "h2o_631g", "h2o_ccpvdz", "h10_chain_ccpvdz",
+           "co_ccpvtz"]
+
+
+def part_libcint():
+    fx = os.path.join(REF, "test", "oracle", "fixtures")
+    for name in LIBCINT:
+        dj = json.load(open(os.path.join(fx, name + "_j.json")))
+        dk = json.load(open(os.path.join(fx, name + "_k.json")))
+        assert dj["provenance"]["cart"] is True
+        conv = dj["converted"]["shells"]
+        assert conv == dk["converted"]["shells"]
+        n = dj["nao"]
+        D = np.asarray(dj["arrays"]["density"]["values"]).reshape(n, n)
+        Dk = np.asarray(dk["arrays"]["density"]["values"]).reshape(n, n)
+        assert np.array_equal(D, Dk)
+        vj = np.asarray(dj["arrays"]["vj"]["values"]).reshape(n, n)
+        vk = np.asarray(dk["arrays"]["vk"]["values"]).reshape(n, n)
+        sh = flat_shells([s["l"] for s in conv], [s["centre"] for s in conv],
+                         [s["exponents"] for s in conv],
+                         [s["coefficients"] for s in conv])
+        np.savez_compressed(os.path.join(HERE, f"libcint_{name}.npz"),
+                            D=D, vj=vj, vk=vk, **sh,
+                            source=np.asarray(f"test/oracle/fixtures/{name}_j.json "
+                                              f"+ _k.json (PySCF "
+                                              f"{dj['provenance']['pyscf']}, libcint "
+                                              f"{dj['provenance']['libcint']})"))
+        print("libcint", name, n)
+
+
+# --- Boys -------------------------------------------------------------------
+
+
+def part_boys():
+    _ref_imports()
+    from felizjueves.reference.boys import boys
+    rng = np.random.default_rng(7)
+    T = np.concatenate([
+        [0.0, 1e-12, 1e-8, 1e-5, 1e-3, 0.01, 0.1, 0.5, 1.0, 2.0, 5.0, 10.0,
+         15.0, 20.0, 25.0, 30.0, 35.0, 36.0, 40.0, 50.0, 75.0, 100.0, 124.9,
+         125.0, 150.0, 300.0, 1e3, 1e4, 1e5, 1e6],
+        rng.uniform(0, 40, 200), 10 ** rng.uniform(-6, 6, 100)])
+    M = np.arange(0, 25)
+    F = np.array([[boys(int(m), float(t)) for t in T] for m in M])
+    np.savez_compressed(os.path.join(HERE, "boys_ref.npz"), T=T, M=M, F=F)
+    print("boys", F.shape)
+
+
+# --- ERI blocks on sampled quartets -----------------------------------------
+
+
+def _eri_one(args):
+    basis_flat, q = args
+    _ref_imports()
+    from functools import partial as _p
+    from felizjueves.eri.eri import eri_block_and_scale
+    from felizjueves.reference.pq import pq
+    shells = basis_flat
+    a, b, c, d = q
+    blk, scale = eri_block_and_scale((shells[a], shells[b]), (shells[c], shells[d]),
+                                     pq=pq)
+    return (np.asarray(blk, np.float64).ravel(), np.asarray(scale, np.float64).ravel())
+
+
+def sample_quartets(basis, rng, per_class, max_l_sum=None):
+    """Ordered quartets (a,b,c,d) sampled per class (la,lb,lc,ld), shells
+    chosen at random among those of each l."""
+    by_l = {}
+    for i, s in enumerate(basis.shells):
+        by_l.setdefault(s.l, []).append(i)
+    ls = sorted(by_l)
+    out = []
+    for la in ls:
+        for lb in ls:
+            for lc in ls:
+                for ld in ls:
+                    if max_l_sum is not None and la + lb + lc + ld > max_l_sum:
+                        continue
+                    for _ in range(per_class):
+                        out.append(tuple(int(rng.choice(by_l[x]))
+                                         for x in (la, lb, lc, ld)))
+    return out
+
+
+def part_eri():
+    _ref_imports()
+    from felizjueves_b200 import configs
+    rng = np.random.default_rng(11)
+    for wname, w, per in (("c0", configs.c0(), 3), ("c1", configs.c1(), 1)):
+        rb = ref_basis(w.basis)
+        qs = sample_quartets(w.basis, rng, per)
+        t = time.time()
+        with mp.get_context("spawn").Pool(8) as pool:
+            res = pool.map(_eri_one, [(rb.shells, q) for q in qs], chunksize=1)
+        vals = np.concatenate([r[0] for r in res])
+        scl = np.concatenate([r[1] for r in res])
+        offs = np.cumsum([0] + [len(r[0]) for r in res]).astype(np.int64)
+        np.savez_compressed(os.path.join(HERE, f"eri_{wname}.npz"),
+                            quartets=np.asarray(qs, np.int32), values=vals,
+                            scale=scl, offsets=offs)
+        print("eri", wname, len(qs), "quartets", round(time.time() - t, 1), "s")
+
+
+# --- f_launches plan lists --------------------------------------------------
+
+
+def _bounds_one(args):
+    shells, pairs = args
+    _ref_imports()
+    from felizjueves.ao.pairs import primitive_schwarz_bounds
+    from felizjueves.reference.pq import one_centre
+    return [tuple(primitive_schwarz_bounds(shells[a], shells[b],
+                                           one_centre=one_centre))
+            for a, b in pairs]
+
+
+def _plan(w, parallel_bounds):
+    _ref_imports()
+    from felizjueves.ao.pairs import primitive_schwarz_bounds
+    from felizjueves.eri.fock.launch_f import f_launches
+    from felizjueves.reference.pq import one_centre
+    rb = ref_basis(w.basis)
+    sh = rb.shells
+    t = time.time()
+    if parallel_bounds:
+        pairs = [(i, j) for i in range(len(sh)) for j in range(i, len(sh))]
+        pairs = [(i, j) if (sh[i].l, i) <= (sh[j].l, j) else (j, i) for i, j in pairs]
+        chunks = [pairs[k:k + 512] for k in range(0, len(pairs), 512)]
+        with mp.get_context("spawn").Pool(8) as pool:
+            res = pool.map(_bounds_one, [(sh, c) for c in chunks])
+        table = {}
+        for c, r in zip(chunks, res):
+            for p, g in zip(c, r):
+                table[p] = g
+        idx = {id(s): i for i, s in enumerate(sh)}
+
+        def bound(sa, sb):
+            return table[(idx[id(sa)], idx[id(sb)])]
+    else:
+        bound = partial(primitive_schwarz_bounds, one_centre=one_centre)
+    print("bounds", round(time.time() - t, 1), "s", flush=True)
+    P = f_launches(rb, w.D.tolist(), bound=bound, tau=w.tau, n=w.n_mag)
+    print("plan", P.counts(), round(time.time() - t, 1), "s", flush=True)
+    return P
+
+
+def save_plan(P, path):
+    pairs = P.pairs
+    batch_of = []
+    for bi, b in enumerate(P.batches):
+        batch_of.extend([bi] * len(b.pairs))
+    prim_off = np.cumsum([0] + [len(p.prims) for p in pairs]).astype(np.int64)
+    np.savez_compressed(
+        path,
+        tau=P.tau, n=P.n, magnitudes=np.asarray(P.magnitudes), eps=P.eps,
+        g_max=P.g_max,
+        batch_key=np.asarray([(b.la, b.lb, b.degree, b.mag) for b in P.batches],
+                             np.int32),
+        batch_npairs=np.asarray([len(b.pairs) for b in P.batches], np.int32),
+        pair_ab=np.asarray([(p.a, p.b) for p in pairs], np.int32),
+        pair_batch=np.asarray(batch_of, np.int32),
+        pair_nprim=np.asarray([p.n_prim for p in pairs], np.int32),
+        pair_G=np.asarray([p.G for p in pairs], np.float64),
+        pair_dmax=np.asarray([p.dmax for p in pairs], np.float64),
+        pair_key=np.asarray([p.key for p in pairs], np.float64),
+        pair_mag=np.asarray([p.mag for p in pairs], np.int32),
+        prims=np.asarray([k for p in pairs for k in p.prims], np.int32),
+        prim_G=np.asarray([g for p in pairs for g in p.prim_G], np.float64),
+        prim_off=prim_off,
+        launches=np.asarray([(L.bra, L.ket) for L in P.launches], np.int32).reshape(-1, 2),
+        screened=np.asarray(P.screened, np.int32).reshape(-1, 2),
+        deleted=np.asarray(P.deleted, np.int32).reshape(-1, 2),
+        n_prim_total=P.n_prim_total,
+        counts=json.dumps(P.counts()))
+
+
+def part_plan_c0():
+    from felizjueves_b200 import configs
+    w = configs.c0()
+    P = _plan(w, parallel_bounds=False)
+    save_plan(P, os.path.join(HERE, "plan_c0.npz"))
+    return P
+
+
+def part_plan_c1():
+    from felizjueves_b200 import configs
+    w = configs.c1()
+    P = _plan(w, parallel_bounds=True)
+    save_plan(P, os.path.join(HERE, "plan_c1.npz"))
+
+
+# --- six-block screen of the c0 plan (walk_f's prediction) -------------------
+
+
+def part_screen_c0():
+    _ref_imports()
+    from felizjueves.eri.fock import kernel_f as KF
+    from felizjueves_b200 import configs
+    w = configs.c0()
+    P = _plan(w, parallel_bounds=False)
+    rb = ref_basis(w.basis)
+    n_sh = len(rb.shells)
+    Dsh = KF.density_blocks(w.D.tolist(), rb.offsets, [s.n_cart for s in rb.shells])
+    wabs = [abs(KF.WEIGHTS.of(b)) for b in KF.BLOCKS]
+    tau = P.tau
+    # walk_f.py:344-351, in the kernel's operation order, per launched quartet
+    # in the launch's orientation (bra batch's pair first).
+    rows = []
+    for li, L in enumerate(P.launches):
+        diag = L.bra == L.ket
+        bras, kets = P.batches[L.bra].pairs, P.batches[L.ket].pairs
+        for ib, br in enumerate(bras):
+            for ik, kt in enumerate(kets):
+                if diag and ik < ib:
+                    continue
+                s = (br.a, br.b, kt.a, kt.b)
+                dmax = wabs[0] * Dsh[s[0] * n_sh + s[1]]
+                for wv, (u, v) in zip(wabs[1:], KF.BLOCKS[1:]):
+                    t = wv * Dsh[s[u] * n_sh + s[v]]
+                    if dmax < t:
+                        dmax = t
+                skip = br.G * (kt.G * dmax) < tau
+                rows.append((li, ib, ik, int(skip)))
+    rows = np.asarray(rows, np.int32)
+    np.savez_compressed(os.path.join(HERE, "screen_c0.npz"), rows=rows,
+                        Dsh=np.asarray(Dsh))
+    print("screen_c0", len(rows), "quartets launched,", int(rows[:, 3].sum()), "skipped")
+
+
+# --- J and K on small nested systems (reference host path) ------------------
+
+
+def _jk(args):
+    which, w = args
+    _ref_imports()
+    from felizjueves.eri.j_coulomb.j import coulomb_matrix
+    from felizjueves.eri.k_exchange.k import exchange_matrix
+    from felizjueves.reference.pq import pq
+    rb = ref_basis(w.basis)
+    t = time.time()
+    if which == "J":
+        M = coulomb_matrix(rb, w.D.tolist(), pq=pq)
+    else:
+        M = exchange_matrix(rb, w.D.tolist(), pq=pq)
+    return which, np.asarray(M, np.float64), time.time() - t
+
+
+def part_jk_small():
+    from felizjueves_b200 import configs
+    cases = [("c0_1at", configs.sub_workload(configs.c0(), 1)),
+             ("c0_2at", configs.sub_workload(configs.c0(), 2)),
+             ("c1_1at", configs.sub_workload(configs.c1(), 1))]
+    jobs = [(k, w) for _, w in cases for k in ("J", "K")]
+    with mp.get_context("spawn").Pool(6) as pool:
+        res = pool.map(_jk, jobs, chunksize=1)
+    for i, (name, w) in enumerate(cases):
+        (_, J, tj), (_, K, tk) = res[2 * i], res[2 * i + 1]
+        np.savez_compressed(os.path.join(HERE, f"jk_{name}.npz"), J=J, K=K,
+                            D=w.D, t_J=tj, t_K=tk)
+        print("jk", name, w.n_ao, "J", round(tj, 1), "s K", round(tk, 1), "s")
+
+
+# --- the reference's FLOP model (hgp/cost.py) for every class to L=3 ---------
+
+
+def part_cost():
+    _ref_imports()
+    from felizjueves.hgp.cost import cost
+    from felizjueves.hgp import hrr, vrr
+    rows = []
+    pc = [(a, b) for a in range(4) for b in range(a, 4)]
+    for i, bra in enumerate(pc):
+        for ket in pc[i:]:
+            for cls in ((*bra, *ket),):
+                c = cost(cls)
+                v, h = vrr.build(cls), hrr.build(cls)
+                rows.append({"class": list(cls), "x": c.x,
+                             "y_bra": c.k2["bra"], "y_ket": c.k2["ket"],
+                             "z": c.z, "vrr_nodes": v.n_nodes,
+                             "boundary": h.n_boundary,
+                             "hrr_statements": h.n_statements,
+                             "n_eri": h.n_eri,
+                             "boys_max_order": c.boys_max_order})
+    out = {"source": "reference src/felizjueves/hgp/cost.py:245 cost(cls), "
+                     "pruned VRR DAG + bra-first HRR DAG; one + - * / = 1 flop, "
+                     "no FMA; Boys/exp/rsqrt named separately",
+           "digest_flops_per_eri": 12, "classes": rows}
+    path = os.path.join(REPO, "felizjueves_b200", "data", "hgp_cost.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+    print("cost", len(rows), "classes")
+
+
+PARTS = {"libcint": part_libcint, "boys": part_boys, "eri": part_eri,
+         "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
+         "screen_c0": part_screen_c0, "jk_small": part_jk_small,
+         "cost": part_cost}
+DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri"]
+
+
+def main():
+    global REF
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", required=True)
+    ap.add_argument("parts", nargs="*")
+    a = ap.parse_args()
+    REF = os.path.abspath(a.ref)
+    os.environ["FJB_REF"] = REF
+    _ref_imports()
+    for p in a.parts or DEFAULT:
+        t = time.time()
+        PARTS[p]()
+        print(f"[{p}] {time.time() - t:.1f} s", flush=True)
+
+
+if __name__ == "__main__":
+    main()

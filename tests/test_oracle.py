@@ -1,0 +1,78 @@
+"""The CPU oracle (oracle/oracle.c) pinned to the reference's own outputs
+(tests/golden/, written by tests/golden/make_golden.py from the reference's
+Python) and to the libcint/PySCF vj/vk fixtures the reference tracks."""
+
+import numpy as np
+import pytest
+
+from conftest import golden
+from felizjueves_b200 import configs
+
+
+def test_boys_matches_reference_quadrature(oracle_lib):
+    z = golden("boys_ref.npz")
+    F = np.array([[oracle_lib.boys(int(m), float(t)) for t in z["T"]] for m in z["M"]])
+    rel = np.abs(F - z["F"]) / np.abs(z["F"])
+    assert rel.max() < 1e-14
+
+
+@pytest.mark.parametrize("wname", ["c0", "c1"])
+def test_eri_blocks_match_reference(oracle_lib, wname):
+    w = getattr(configs, wname)()
+    z = golden(f"eri_{wname}.npz")
+    ob = oracle_lib.OracleBasis.of(w.basis)
+    for i, q in enumerate(z["quartets"]):
+        lo, hi = z["offsets"][i], z["offsets"][i + 1]
+        got = oracle_lib.eri_block(ob, *map(int, q))
+        err = np.abs(got - z["values"][lo:hi])
+        assert np.all(err <= 1e-14 * z["scale"][lo:hi] + 1e-300), (q, err.max())
+
+
+LIBCINT = ["h2_sto3g", "h2o_sto3g", "h2o_631g", "h2o_ccpvdz", "h10_chain_ccpvdz", "co_ccpvtz"]
+
+
+@pytest.mark.parametrize("name", LIBCINT)
+def test_jk_matches_libcint(oracle_lib, name):
+    g = golden(f"libcint_{name}.npz")
+    ob = oracle_lib.OracleBasis.from_npz(g)
+    J, K = oracle_lib.jk(ob, g["D"])
+    assert np.abs(J - g["vj"]).max() <= 1e-12 * np.abs(g["vj"]).max()
+    assert np.abs(K - g["vk"]).max() <= 1e-12 * np.abs(g["vk"]).max()
+
+
+@pytest.mark.parametrize("name,atoms,wfn", [("c0_1at", 1, "c0"), ("c0_2at", 2, "c0"),
+                                            ("c1_1at", 1, "c1")])
+def test_jk_matches_reference_host_path(oracle_lib, name, atoms, wfn):
+    """J and K of the reference's coulomb_matrix / exchange_matrix
+    (eri/j_coulomb/j.py:436, eri/k_exchange/k.py:482) on nested systems."""
+    w = configs.sub_workload(getattr(configs, wfn)(), atoms)
+    g = golden(f"jk_{name}.npz")
+    assert np.array_equal(g["D"], w.D)
+    ob = oracle_lib.OracleBasis.of(w.basis)
+    for ordered in (False, True):
+        J, K = oracle_lib.jk(ob, w.D, ordered=ordered)
+        scale = max(np.abs(g["J"]).max(), np.abs(g["K"]).max())
+        assert np.abs(J - g["J"]).max() <= 1e-14 * scale * 10
+        assert np.abs(K - g["K"]).max() <= 1e-14 * scale * 10
+
+
+def test_ordered_and_unique_sweeps_agree(oracle_lib):
+    w = configs.cluster(2, 3)
+    ob = oracle_lib.OracleBasis.of(w.basis)
+    J1, K1 = oracle_lib.jk(ob, w.D)
+    J2, K2 = oracle_lib.jk(ob, w.D, ordered=True)
+    s = max(np.abs(J1).max(), np.abs(K1).max())
+    assert np.abs(J1 - J2).max() <= 1e-13 * s
+    assert np.abs(K1 - K2).max() <= 1e-13 * s
+
+
+def test_wrong_weight_fails(oracle_lib):
+    """A planted mistake (the Coulomb blocks at weight 1, the predecessor's
+    bug the reference documents at kernel_f.py:98-101) misses by far more than
+    the tolerance: the check can fail."""
+    w = configs.cluster(1, 3)
+    ob = oracle_lib.OracleBasis.of(w.basis)
+    J, K = oracle_lib.jk(ob, w.D)
+    J2, _ = oracle_lib.jk(ob, w.D, ordered=True)
+    wrong = 0.5 * J  # what weight 1 on the Coulomb blocks would give
+    assert np.abs(wrong - J2).max() > 1e3 * 1e-13 * np.abs(J2).max()
