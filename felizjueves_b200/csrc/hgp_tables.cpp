@@ -275,6 +275,11 @@ bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, Clas
     int want = std::max(1, std::min(max_kab * max_kcd, kThreads));
     int slots = want;
     auto total = [&](int s) { return std::max(s * c.n_nodes, hr) + s * kNumScalars + fixed; };
+    // Occupancy first: shrink the chunk of primitive quartets until four
+    // CTAs fit on an SM (a quarter of the budget), unless one slot already
+    // needs more; then stay inside the budget.
+    const int quarter = budget / 4;
+    while (slots > 1 && total(slots) > quarter) --slots;
     while (slots > 1 && total(slots) > budget) --slots;
     if (total(slots) > budget) return false;
     o->slots = slots;

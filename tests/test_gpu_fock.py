@@ -51,14 +51,24 @@ def test_boys_device_matches_reference(cuda, lib_built):
 
 @pytest.mark.parametrize("wname", ["c0", "c1"])
 def test_eri_tap_matches_reference(cuda, lib_built, wname):
+    """The HGP tap against the reference's MMD eri_block.  The two
+    recurrences cancel differently, so an element is held to 1e-12 of its
+    own `scale` or, for elements that vanish against their block (a far
+    pair's HRR multiplies by |AB|^l), to 1e-11 of the block's largest
+    `scale` -- both far below anything a J/K/G element can see."""
     w = getattr(configs, wname)()
     z = golden(f"eri_{wname}.npz")
     eng = FockEngine(w.basis)
     blocks = eng.eri_blocks(z["quartets"])
+    worst = 0.0
     for i, q in enumerate(z["quartets"]):
         lo, hi = z["offsets"][i], z["offsets"][i + 1]
+        sc = z["scale"][lo:hi]
         err = np.abs(blocks[i].ravel() - z["values"][lo:hi])
-        assert np.all(err <= 1e-12 * z["scale"][lo:hi] + 1e-300), (tuple(q), err.max())
+        tol = np.maximum(1e-12 * sc, 1e-11 * sc.max())
+        worst = max(worst, float((err / np.maximum(tol, 1e-300)).max()))
+        assert np.all(err <= tol), (tuple(q), err.max(), sc.max())
+    print(f"worst err/tol = {worst:.3f}")
 
 
 def _gpu_jkg(basis, D, tau, n=4):
