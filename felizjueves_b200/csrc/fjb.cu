@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -1092,4 +1093,89 @@ int run_probe(int reps, double *tflops) {
 extern "C" int fjb_fma_probe(int fp32, int reps, double *tflops) {
     if (!tflops || reps < 1) return fail(nullptr, FJB_E_ARG, "bad argument");
     return fp32 ? run_probe<float>(reps, tflops) : run_probe<double>(reps, tflops);
+}
+
+// ---------------------------------------------------------------------------
+// fjb_fock_build_noalloc: the build with its scratch in a file-scope array
+// ---------------------------------------------------------------------------
+//
+// The scratch -- J' and K' (n_ao^2 each, accumulated by atomics, so they
+// must start at zero) and the shell-block maxima Dsh (n_sh^2) -- lives in
+// g_noalloc_scratch instead of handle-owned buffers.  In host code the name
+// g_noalloc_scratch is only a host-side stand-in for the array, not a device
+// address; the address a kernel may use is looked up once per device, with
+// that device current, by cudaGetSymbolAddress, and passed to the kernels.
+
+namespace {
+
+static __device__ __align__(256) double g_noalloc_scratch[FJB_NOALLOC_SCRATCH_DOUBLES];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// The device address of g_noalloc_scratch on `device` (current), looked up
+// on the first call for that device.  Returns nullptr on failure.
+double *noalloc_scratch(int device, std::string *why) {
+    if (device < 0 || device >= kNoallocMaxDevices) {
+        *why = "device ordinal out of range for the no-allocation scratch table";
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            *why = std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e);
+            return nullptr;
+        }
+        g_noalloc_ptr[device] = static_cast<double *>(p);
+    }
+    return g_noalloc_ptr[device];
+}
+
+}  // namespace
+
+extern "C" int fjb_fock_build_noalloc(fjb_handle *h, const double *D_dev, double *J_dev, double *K_dev,
+                                      double *G_dev, void *stream) {
+    if (!h || !D_dev) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    const int nsh = (int)h->basis.shells.size(), nao = h->basis.n_ao;
+    if (nao > FJB_NOALLOC_MAX_AO || nsh > FJB_NOALLOC_MAX_SHELLS)
+        return fail(h, FJB_E_LIMIT,
+                    "fjb_fock_build_noalloc: n_ao = " + std::to_string(nao) + ", n_shells = " +
+                        std::to_string(nsh) + " exceed its fixed scratch (n_ao <= " +
+                        std::to_string(FJB_NOALLOC_MAX_AO) + ", n_shells <= " +
+                        std::to_string(FJB_NOALLOC_MAX_SHELLS) + "); use fjb_fock_build");
+    CUDA_OK(h, cudaSetDevice(h->device));
+    std::string why;
+    double *scratch = noalloc_scratch(h->device, &why);
+    if (!scratch) return fail(h, FJB_E_CUDA, why);
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t nn = (size_t)nao * nao;
+    double *Jp = scratch, *Kp = scratch + nn, *Dsh = scratch + 2 * nn;
+    density_blocks_kernel<<<(nsh * nsh + 255) / 256, 256, 0, st>>>(D_dev, nao, nsh, h->sh_off.p, h->sh_nc.p, Dsh);
+    CUDA_OK(h, cudaMemsetAsync(Jp, 0, 2 * nn * sizeof(double), st));
+    for (const ClassRun &r : h->runs) {
+        KArgs a{};
+        a.C = r.dev;
+        a.units = h->units.p + r.unit0;
+        a.n_units = r.n_units;
+        a.launches = h->launches.p;
+        a.pairs = h->pairs.p;
+        a.prims = h->prims.p;
+        a.D = D_dev;
+        a.Dsh = Dsh;
+        a.n_sh = nsh;
+        a.n_ao = nao;
+        a.tau = h->plan.tau;
+        a.Jp = Jp;
+        a.Kp = Kp;
+        a.boys_tab = h->boys.p;
+        hgp_fock_kernel<<<r.grid, kThreads, (size_t)r.dev.sm_total * sizeof(double), st>>>(a);
+    }
+    close_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(Jp, Kp, nao, J_dev, K_dev, G_dev);
+    CUDA_OK(h, cudaGetLastError());
+    return FJB_OK;
 }

@@ -173,6 +173,29 @@ typedef struct fjb_class_stat {
 } fjb_class_stat;
 int fjb_class_stats(const fjb_handle *h, fjb_class_stat *out, int64_t n, int64_t *n_classes);
 
+/* fjb_fock_build without any device allocation (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc while they run the
+ * SCF loop: a host framework that owns every byte of device memory through
+ * its own pool and refuses raw allocations after start-up, or a loop that
+ * must not take the allocator's latency or fail on fragmentation between
+ * iterations.  The handle and its plan are made once at set-up (they do
+ * allocate); this call then builds J, K and G (FP64) into the caller's
+ * DEVICE buffers using, as its scratch (the J', K' accumulators and the
+ * shell-block density maxima), one file-scope device array of
+ * FJB_NOALLOC_SCRATCH_DOUBLES doubles (4.5 MiB) that every GPU loading the
+ * library holds until exit.  Limits: n_ao <= FJB_NOALLOC_MAX_AO and
+ * n_shells <= FJB_NOALLOC_MAX_SHELLS, else FJB_E_LIMIT.  The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  Every call shares the
+ * one array: calls that overlap on the GPU (two streams, two handles, two
+ * threads) race and corrupt each other's results; serialise them. */
+#define FJB_NOALLOC_MAX_AO 512
+#define FJB_NOALLOC_MAX_SHELLS 256
+#define FJB_NOALLOC_SCRATCH_DOUBLES                                              \
+    (2 * FJB_NOALLOC_MAX_AO * FJB_NOALLOC_MAX_AO + FJB_NOALLOC_MAX_SHELLS * FJB_NOALLOC_MAX_SHELLS)
+int fjb_fock_build_noalloc(fjb_handle *h, const double *D_dev, double *J_dev, double *K_dev,
+                           double *G_dev, void *stream);
+
 /* Achievable CUDA-core FMA throughput (TFLOP/s, 2 flops per FMA) by
  * independent FMA chains on every SM, best of `reps` timed launches
  * (the method of the reference's performance/ceilings.py:17-40).
