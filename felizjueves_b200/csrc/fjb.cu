@@ -28,6 +28,10 @@
 
 namespace fjb {
 std::vector<double> boys_table();
+// fock_compiled.cu: the class-templated register kernels
+bool compiled_available(int la, int lb, int lc, int ld);
+int compiled_blocks_per_sm(int la, int lb, int lc, int ld);
+cudaError_t launch_compiled(int la, int lb, int lc, int ld, int grid, cudaStream_t st, const KArgs &a);
 }
 
 using namespace fjb;
@@ -94,7 +98,8 @@ __global__ void screen_mask_kernel(const Unit *units, int n_units, const LaunchR
 
 // The HGP Fock kernel (file header of fock_kernels.cuh).  All floating-point
 // work is FP64.
-__global__ void __launch_bounds__(kThreads) hgp_fock_kernel(const KArgs A) {
+template <int NT>
+__global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
     extern __shared__ __align__(16) double sm[];
     const ClassDev &C = A.C;
     double *V = sm + C.sm_V;
@@ -382,9 +387,16 @@ struct ClassEntry {
         ket_off.upload(host.ket_off);
         ket_terms.upload(host.ket_terms);
     }
-    ClassDev dev(int max_kab, int max_kcd) const {
+    // threads/slots <= 0: the class's default configuration
+    ClassDev dev(int max_kab, int max_kcd, int threads = 0, int slots = 0) const {
         ClassDev d;
-        if (!layout_class(host, max_kab, max_kcd, kSmemBudgetDoubles, &d))
+        int th = 0, target = 0;
+        default_config(host, kSmemBudgetDoubles, &th, &target);
+        if (threads > 0) {
+            th = threads;
+            target = kSmemBudgetDoubles * threads / (16 * 32);
+        }
+        if (!layout_class(host, max_kab, max_kcd, kSmemBudgetDoubles, th, target, slots, &d))
             throw std::length_error("class does not fit in shared memory");
         d.level_off = level_off.p;
         d.ops = ops.p;
@@ -401,10 +413,49 @@ struct ClassEntry {
 };
 
 struct ClassRun {
-    ClassDev dev;
+    ClassDev dev;  // the interpreter kernel's layout (kept valid for every class)
     int unit0 = 0, n_units = 0;
     int grid = 0;
+    int max_kab = 1, max_kcd = 1;
+    bool compiled = false;  // run on the class-templated register kernel
 };
+
+template <int NT>
+int occupancy(const ClassDev &d) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hgp_fock_kernel<NT>, NT,
+                                                  (size_t)d.sm_total * sizeof(double));
+    return per_sm;
+}
+
+// Launch the HGP kernel instantiated for the class's CTA width.
+cudaError_t launch_hgp(const ClassDev &d, int grid, cudaStream_t st, const KArgs &a) {
+    const size_t smem = (size_t)d.sm_total * sizeof(double);
+    switch (d.threads) {
+        case 32: hgp_fock_kernel<32><<<grid, 32, smem, st>>>(a); break;
+        case 64: hgp_fock_kernel<64><<<grid, 64, smem, st>>>(a); break;
+        case 128: hgp_fock_kernel<128><<<grid, 128, smem, st>>>(a); break;
+        case 256: hgp_fock_kernel<256><<<grid, 256, smem, st>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+int sm_count() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+// Grid of a class run: the register kernel puts one warp on a unit, four
+// warps to a CTA; the interpreter one CTA on a unit.
+int run_grid(const ClassRun &r);
+
+cudaError_t launch_run(const ClassRun &r, cudaStream_t st, const KArgs &a) {
+    if (r.compiled) return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, r.grid, st, a);
+    return launch_hgp(r.dev, r.grid, st, a);
+}
 
 }  // namespace
 
@@ -413,6 +464,7 @@ struct fjb_handle {
     HostBasis basis;
     std::string err;
     std::map<std::tuple<int, int, int, int>, std::unique_ptr<ClassEntry>> classes;
+    std::map<std::tuple<int, int, int, int>, std::pair<int, int>> cfg;  // (threads, slots) overrides
     DevBuf<double> boys;
     DevBuf<int> sh_off, sh_nc;
     // plan
@@ -507,8 +559,12 @@ PairRec pair_record(const HostBasis &B, int a, int b, double G, int prim0, int n
 
 int grid_for(const ClassDev &d, int n_units) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hgp_fock_kernel, kThreads,
-                                                  (size_t)d.sm_total * sizeof(double));
+    switch (d.threads) {
+        case 32: per_sm = occupancy<32>(d); break;
+        case 64: per_sm = occupancy<64>(d); break;
+        case 128: per_sm = occupancy<128>(d); break;
+        default: per_sm = occupancy<256>(d); break;
+    }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -516,11 +572,21 @@ int grid_for(const ClassDev &d, int n_units) {
     return std::max(1, std::min(n_units, g));
 }
 
+int run_grid(const ClassRun &r) {
+    if (!r.compiled) return grid_for(r.dev, r.n_units);
+    const int per_sm = std::max(1, compiled_blocks_per_sm(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld));
+    const int warps_needed = (r.n_units + 3) / 4;
+    return std::max(1, std::min(warps_needed, per_sm * sm_count()));
+}
+
 int ensure_smem_attr(fjb_handle *h) {
     static bool done = false;
     if (done) return 0;
-    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    kSmemBudgetDoubles * (int)sizeof(double)));
+    const int bytes = kSmemBudgetDoubles * (int)sizeof(double);
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     done = true;
     return 0;
 }
@@ -666,7 +732,13 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
             ClassEntry &ce = h->cls(la, lb, lc, ld);
             ClassRun run;
             auto deg = class_deg[kv.first];
-            run.dev = ce.dev(deg.first, deg.second);
+            auto ov = h->cfg.find(kv.first);
+            run.max_kab = deg.first;
+            run.max_kcd = deg.second;
+            const int th = ov == h->cfg.end() ? 0 : ov->second.first;
+            run.dev = ov == h->cfg.end() || th == 1 ? ce.dev(deg.first, deg.second)
+                                                     : ce.dev(deg.first, deg.second, th, ov->second.second);
+            run.compiled = compiled_available(la, lb, lc, ld) && (th == 0 || th == 1);
             run.unit0 = (int)units.size();
             run.n_units = (int)kv.second.size();
             units.insert(units.end(), kv.second.begin(), kv.second.end());
@@ -687,7 +759,7 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
         return fail(h, FJB_E_CUDA, e.what());
     }
     if (int rc = ensure_smem_attr(h)) return rc;
-    for (auto &r : h->runs) r.grid = grid_for(r.dev, r.n_units);
+    for (auto &r : h->runs) r.grid = run_grid(r);
     h->free_class_events();
     for (size_t i = 0; i < h->runs.size(); ++i) {
         cudaEvent_t a, b;
@@ -807,7 +879,7 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
     if (!h || !D_dev) return fail(h, FJB_E_ARG, "null argument");
     if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
     if (precision != FJB_FP64 && precision != FJB_ROUTED) return fail(h, FJB_E_ARG, "unknown precision mode");
-    (void)threshold;
+    const double route = precision == FJB_ROUTED ? (threshold > 0.0 ? threshold : 1e-9) : 0.0;
     if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
     cudaSetDevice(h->device);
     cudaStream_t st = (cudaStream_t)stream;
@@ -840,7 +912,8 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
         a.Jp = h->Jp.p;
         a.Kp = h->Kp.p;
         a.boys_tab = h->boys.p;
-        hgp_fock_kernel<<<r.grid, kThreads, (size_t)r.dev.sm_total * sizeof(double), st>>>(a);
+        a.route_thresh = route;
+        CUDA_OK(h, launch_run(r, st, a));
         ++launches;
         CUDA_OK(h, cudaEventRecord(h->cev[ri].second, st));
     }
@@ -961,8 +1034,7 @@ int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_de
             a.tap_out = out_dev;
             a.tap_off = dto.p;
             a.boys_tab = h->boys.p;
-            hgp_fock_kernel<<<grid_for(dev, a.n_units), kThreads, (size_t)dev.sm_total * sizeof(double)>>>(a);
-            CUDA_OK(h, cudaGetLastError());
+            CUDA_OK(h, launch_hgp(dev, grid_for(dev, a.n_units), nullptr, a));
             CUDA_OK(h, cudaDeviceSynchronize());
         }
     } catch (const std::length_error &e) {
@@ -1019,6 +1091,34 @@ int fjb_launch_stats(const fjb_handle *hc, fjb_launch_stat *out, int64_t n) {
     for (size_t i = 0; i < h->lstat.size(); ++i) {
         out[i] = h->lstat[i];
         out[i].computed = (int64_t)c[i];
+    }
+    return FJB_OK;
+}
+
+int fjb_set_class_config(fjb_handle *h, int la, int lb, int lc, int ld, int threads, int slots) {
+    if (!h) return fail(h, FJB_E_ARG, "null handle");
+    if (threads != 0 && threads != 1 && threads != 32 && threads != 64 && threads != 128 && threads != 256)
+        return fail(h, FJB_E_ARG, "threads must be 0, 1 (register kernel), 32, 64, 128 or 256");
+    if (slots < 0 || slots > kMaxThreads) return fail(h, FJB_E_ARG, "slots out of range");
+    auto key = std::make_tuple(la, lb, lc, ld);
+    if (threads == 0 && slots == 0)
+        h->cfg.erase(key);
+    else
+        h->cfg[key] = {threads, slots};
+    if (h->device < 0 || !h->planned) return FJB_OK;
+    for (auto &r : h->runs) {
+        if (std::make_tuple(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld) != key) continue;
+        try {
+            if (threads == 1 && !compiled_available(la, lb, lc, ld))
+                return fail(h, FJB_E_LIMIT, "this class has no compiled register kernel");
+            ClassDev d = threads == 1 ? h->cls(la, lb, lc, ld).dev(r.max_kab, r.max_kcd)
+                                      : h->cls(la, lb, lc, ld).dev(r.max_kab, r.max_kcd, threads, slots);
+            r.dev = d;
+            r.compiled = compiled_available(la, lb, lc, ld) && (threads == 0 || threads == 1);
+            r.grid = run_grid(r);
+        } catch (const std::length_error &e) {
+            return fail(h, FJB_E_LIMIT, e.what());
+        }
     }
     return FJB_OK;
 }
@@ -1173,7 +1273,7 @@ extern "C" int fjb_fock_build_noalloc(fjb_handle *h, const double *D_dev, double
         a.Jp = Jp;
         a.Kp = Kp;
         a.boys_tab = h->boys.p;
-        hgp_fock_kernel<<<r.grid, kThreads, (size_t)r.dev.sm_total * sizeof(double), st>>>(a);
+        CUDA_OK(h, launch_run(r, st, a));
     }
     close_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(Jp, Kp, nao, J_dev, K_dev, G_dev);
     CUDA_OK(h, cudaGetLastError());

@@ -12,8 +12,9 @@ constexpr int kBoysTaylor = 7;    // Taylor terms (orders m .. m+6)
 constexpr double kBoysDelta = 0.05;
 constexpr double kBoysTMax = 40.0;  // table covers [0, kBoysTMax]
 constexpr int kBoysNT = 801;        // kBoysTMax / kBoysDelta + 1
-constexpr int kThreads = 128;       // threads per CTA of the HGP kernel
-constexpr int kKetChunk = 64;       // ket pairs per work unit
+constexpr int kThreads = 128;       // widest CTA of the HGP kernel's default choice
+constexpr int kMaxThreads = 256;    // widest CTA the kernel is instantiated for
+constexpr int kKetChunk = 32;       // ket pairs per work unit (one per lane of a warp)
 constexpr int kNumScalars = 17;     // per-primitive-quartet VRR scalars
 
 // One VRR node update, 16 bytes.  value(dst) =
@@ -74,6 +75,7 @@ struct ClassDev {
     int nbe, nbf;     // boundary extents (e with la<=|e|<=la+lb, f likewise)
     int n_cb, n_ck;   // HRR coefficient counts
     int slots;        // primitive quartets per chunk
+    int threads;      // CTA width: 32, 64, 128 or 256
     const int *level_off;   // [n_levels + 1] into ops
     const VOp *ops;
     const uint16_t *leaf;   // [L + 1] node of [0|0]^(m), 0 if unread

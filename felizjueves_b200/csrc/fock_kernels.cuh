@@ -85,6 +85,24 @@ __device__ __forceinline__ bool skip6(const double *__restrict__ Dsh, int n_sh, 
     return __dmul_rn(Gb, __dmul_rn(Gk, dmax)) < tau;
 }
 
+// G_ab G_cd dmax itself (skip6's left-hand side): the bound on every term
+// the quartet deposits, read by the precision router.
+__device__ __forceinline__ double six_block_bound(const double *__restrict__ Dsh, int n_sh, int a, int b,
+                                                 int c, int d, double Gb, double Gk) {
+    double dmax = 2.0 * __ldg(Dsh + (size_t)a * n_sh + b);
+    double t = 2.0 * __ldg(Dsh + (size_t)c * n_sh + d);
+    if (dmax < t) dmax = t;
+    t = 0.5 * __ldg(Dsh + (size_t)a * n_sh + c);
+    if (dmax < t) dmax = t;
+    t = 0.5 * __ldg(Dsh + (size_t)a * n_sh + d);
+    if (dmax < t) dmax = t;
+    t = 0.5 * __ldg(Dsh + (size_t)b * n_sh + c);
+    if (dmax < t) dmax = t;
+    t = 0.5 * __ldg(Dsh + (size_t)b * n_sh + d);
+    if (dmax < t) dmax = t;
+    return __dmul_rn(Gb, __dmul_rn(Gk, dmax));
+}
+
 __device__ __forceinline__ double ipow(double x, int n) {
     double r = 1.0;
     for (int k = 0; k < n; ++k) r *= x;

@@ -249,7 +249,21 @@ ClassHost build_class(int la, int lb, int lc, int ld) {
     return c;
 }
 
-bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, ClassDev *o) {
+void default_config(const ClassHost &c, int budget, int *threads, int *target) {
+    if (c.n_nodes <= 1200) {
+        *threads = 32;
+        *target = budget / 16;
+    } else if (c.n_nodes <= 4000) {
+        *threads = 64;
+        *target = budget / 8;
+    } else {
+        *threads = 128;
+        *target = budget / 2;
+    }
+}
+
+bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, int threads, int target,
+                  int force_slots, ClassDev *o) {
     *o = ClassDev{};
     o->la = c.la;
     o->lb = c.lb;
@@ -272,15 +286,16 @@ bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, Clas
     const int dblk = c.nab + c.ncd + c.na * c.nc + c.na * c.nd + c.nb * c.nc + c.nb * c.nd;
     const int fixed = c.nbe * c.nbf + 8 * max_kab + 8 * max_kcd + o->n_cb + o->n_ck + dblk +
                       c.nab + 16;
-    int want = std::max(1, std::min(max_kab * max_kcd, kThreads));
-    int slots = want;
+    int want = std::max(1, std::min(max_kab * max_kcd, threads));
+    int slots = force_slots > 0 ? std::min(force_slots, threads) : want;
     auto total = [&](int s) { return std::max(s * c.n_nodes, hr) + s * kNumScalars + fixed; };
-    // Occupancy first: shrink the chunk of primitive quartets until four
-    // CTAs fit on an SM (a quarter of the budget), unless one slot already
-    // needs more; then stay inside the budget.
-    const int quarter = budget / 4;
-    while (slots > 1 && total(slots) > quarter) --slots;
+    // Occupancy first: shrink the chunk of primitive quartets until the CTA
+    // fits its target, unless one slot already needs more; then stay inside
+    // the hard budget.
+    if (force_slots <= 0)
+        while (slots > 1 && total(slots) > target) --slots;
     while (slots > 1 && total(slots) > budget) --slots;
+    o->threads = threads;
     if (total(slots) > budget) return false;
     o->slots = slots;
     o->vregion = std::max(slots * c.n_nodes, hr);

@@ -274,6 +274,11 @@ class FockEngine:
         _lib.check(self._L.fjb_last_build_stats(self._h, C.byref(ms), C.byref(nl)), self._h)
         return float(ms.value), int(nl.value)
 
+    def set_class_config(self, cls, threads: int = 0, slots: int = 0) -> None:
+        """CTA width and primitive-quartet chunk of one class (0 = default)."""
+        _lib.check(self._L.fjb_set_class_config(self._h, *map(int, cls), int(threads),
+                                                int(slots)), self._h)
+
     def launch_stats(self) -> list[dict]:
         """Per launch: class, degrees, quartets met and computed by the last
         build."""

@@ -173,6 +173,14 @@ typedef struct fjb_class_stat {
 } fjb_class_stat;
 int fjb_class_stats(const fjb_handle *h, fjb_class_stat *out, int64_t n, int64_t *n_classes);
 
+/* Per-class launch configuration: the CTA width (32, 64, 128, 256; 0 =
+ * the class's default) and the chunk of primitive quartets one CTA pass
+ * holds (0 = sized for occupancy).  Applies to the current plan and to later
+ * ones.  This is what the autotuner sets after timing candidates, as the
+ * reference's performance/dispatch.py:1-45 picks a batch count from measured
+ * medians.  FJB_E_LIMIT if the class does not fit that configuration. */
+int fjb_set_class_config(fjb_handle *h, int la, int lb, int lc, int ld, int threads, int slots);
+
 /* fjb_fock_build without any device allocation (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc while they run the
  * SCF loop: a host framework that owns every byte of device memory through
