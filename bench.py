@@ -198,7 +198,7 @@ def main():
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    w = getattr(configs, a.workload)()
+    w = configs.by_name(a.workload)
     eng = FockEngine(w.basis, device=local)
     P = eng.plan(w.D, w.tau, w.n_mag)
     n = w.n_ao
@@ -309,7 +309,7 @@ def reference_arm(a, rank, world):
         return
     from felizjueves_b200 import configs
     from felizjueves_b200.fock import FockEngine
-    w = getattr(configs, a.workload)()
+    w = configs.by_name(a.workload)
     # the plan is host work (no GPU); its launch counts come from the plan
     eng = FockEngine(w.basis, device=-1)
     P = eng.plan(w.D, w.tau, w.n_mag)

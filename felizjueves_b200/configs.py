@@ -160,3 +160,12 @@ def sub_workload(w: Workload, atoms: int) -> Workload:
 
 
 WORKLOADS = {"c0": c0, "c1": c1}
+
+
+def by_name(name: str) -> Workload:
+    """`c0`, `c1`, or `clusterN` (N atoms of the c1 recipe, seed 5)."""
+    if name in WORKLOADS:
+        return WORKLOADS[name]()
+    if name.startswith("cluster") and name[7:].isdigit():
+        return cluster(int(name[7:]), 5)
+    raise ValueError(f"unknown workload {name!r}")

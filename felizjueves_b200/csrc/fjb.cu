@@ -177,7 +177,62 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
             __syncthreads();
 
             const int K = kab * kcd;
-            for (int c0 = 0; c0 < K; c0 += slots) {
+            if (slots == 1) {
+                // One primitive quartet at a time: every thread holds its
+                // scalars in registers; one thread evaluates the Boys leaves.
+                for (int t = 0; t < K; ++t) {
+                    const int ikcd = t / kab, ikab = t - ikcd * kab;
+                    const double *pb = braP + 8 * ikab, *pk = ketP + 8 * ikcd;
+                    const double p = pb[6], q = pk[6];
+                    const double ppq = p + q, inv = 1.0 / ppq, rho = p * q * inv;
+                    const double PQx = pb[0] - pk[0], PQy = pb[1] - pk[1], PQz = pb[2] - pk[2];
+                    const double wp = -q * inv, wq = p * inv;
+                    const double i2p = 0.5 / p, i2q = 0.5 / q;
+                    const double rp = i2p * rho / p, rq = i2q * rho / q, e2 = 0.5 * inv;
+                    const double pa0 = pb[3], pa1 = pb[4], pa2 = pb[5];
+                    const double qc0 = pk[3], qc1 = pk[4], qc2 = pk[5];
+                    const double wp0 = wp * PQx, wp1 = wp * PQy, wp2 = wp * PQz;
+                    const double wq0 = wq * PQx, wq1 = wq * PQy, wq2 = wq * PQz;
+                    if (tid == 0) {
+                        const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+                        double F[kMaxLQuartet + 1];
+                        boys_eval(L, T, F, A.boys_tab);
+                        const double seed = pb[7] * pk[7] * kTwoOverSqrtPi * sqrt(rho);
+                        V[0] = 0.0;
+                        for (int m = 0; m <= L; ++m) V[__ldg(C.leaf + m)] = seed * F[m];
+                    }
+                    __syncthreads();
+                    for (int lv = 0; lv < C.n_levels; ++lv) {
+                        const int o0 = __ldg(C.level_off + lv), o1 = __ldg(C.level_off + lv + 1);
+                        for (int oi = o0 + tid; oi < o1; oi += nt) {
+                            const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(C.ops) + oi);
+                            VOp op;
+                            memcpy(&op, &raw, sizeof(op));
+                            const int d = op.d;
+                            double a, b, c, dd;
+                            if (op.kind) {
+                                a = d == 0 ? qc0 : (d == 1 ? qc1 : qc2);
+                                b = d == 0 ? wq0 : (d == 1 ? wq1 : wq2);
+                                c = i2q;
+                                dd = rq;
+                            } else {
+                                a = d == 0 ? pa0 : (d == 1 ? pa1 : pa2);
+                                b = d == 0 ? wp0 : (d == 1 ? wp1 : wp2);
+                                c = i2p;
+                                dd = rp;
+                            }
+                            double v = a * V[op.s0] + b * V[op.s1];
+                            v += (double)op.c2 * (c * V[op.s2] - dd * V[op.s3]);
+                            v += (double)op.c4 * e2 * V[op.s4];
+                            V[op.dst] = v;
+                        }
+                        __syncthreads();
+                    }
+                    for (int i = tid; i < nbe * nbf; i += nt) bound[i] += V[__ldg(C.tgt + i)];
+                    __syncthreads();
+                }
+            }
+            for (int c0 = 0; slots > 1 && c0 < K; c0 += slots) {
                 const int ns = min(slots, K - c0);
                 for (int s = tid; s < ns; s += nt) {
                     const int t = c0 + s, ikcd = t / kab, ikab = t - ikcd * kab;
