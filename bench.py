@@ -46,10 +46,10 @@ WORKLOAD = ("64-atom cluster (seed 1, 0.1 atoms/A^3, >=0.95 A), per atom s x3 p 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fjb", choices=["fjb", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "routed"])
+    ap.add_argument("--precision", default="routed", choices=["fp64", "routed"])
     ap.add_argument("--workload", default="c1")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -154,10 +154,6 @@ def cpu_sample(w, lstats, plan, cores: int, budget_s: float = 20.0, seed: int = 
     with mp.get_context("spawn").Pool(cores) as pool:
         res = pool.map(_time_quartets, [(flat, c) for c in chunks])
     wall = time.perf_counter() - t0
-    times = {}
-    for i in range(cores):
-        for q, t in zip(chunks[i], res[i]):
-            pass
     per = {}
     flat_times = []
     for i in range(cores):
@@ -166,8 +162,8 @@ def cpu_sample(w, lstats, plan, cores: int, budget_s: float = 20.0, seed: int = 
         per.setdefault(owners[idx], []).append(t)
     total_cpu_s = 0.0
     for k, lis in keys.items():
-        # the oracle sums every primitive pair; a launch key's K_AB, K_CD are
-        # the kept degrees -- scale the sampled block time by the ratio
+        # the oracle sums every primitive pair of the sampled shells (no
+        # pruning), so the estimate is an upper bound on the pruned work
         cnt = sum(lstats[li]["computed"] for li in lis)
         total_cpu_s += cnt * float(np.median(per[k]))
     ms = 1e3 * total_cpu_s / cores
@@ -208,40 +204,50 @@ def main():
     J = torch.empty((n, n), dtype=torch.float64, device=f"cuda:{local}")
     K = torch.empty_like(J)
     G = torch.empty_like(J)
-    prec = _lib.FJB_FP64 if a.precision == "fp64" else _lib.FJB_ROUTED
     stream = torch.cuda.current_stream()
-    for i in range(a.warmup):
-        eng.build(Ds[i % n_d], J=J, K=K, G=G, precision=prec)
-    torch.cuda.synchronize()
-    clocks = Clocks(local)
-    clocks.start()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    launches = 0
-    for i in range(a.steps):
-        eng.build(Ds[i % n_d], J=J, K=K, G=G, precision=prec)
-        launches += eng.last_build_stats()[1] if i == 0 else 0
-    e1.record(stream)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    total_ms = e0.elapsed_time(e1)
-    ck = clocks.stop()
-    _, nl = eng.last_build_stats()
-    gpu_launches = nl * a.steps
-    ms = total_ms / a.steps
-    if dist:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
 
-    # roofline of the dominant class kernel (last timed build)
-    cs = eng.class_stats()
-    ls = eng.launch_stats()
+    def timed(prec):
+        """W untimed builds, then K builds between two events on the build
+        stream, bracketed by barrier + synchronize; nvidia-smi sampled over
+        the timed region.  Returns ms/build (max over ranks), clocks, the
+        kernel launches per build, the class and launch statistics of the
+        last build and a copy of its G."""
+        for i in range(a.warmup):
+            eng.build(Ds[i % n_d], J=J, K=K, G=G, precision=prec)
+        torch.cuda.synchronize()
+        clocks = Clocks(local)
+        clocks.start()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(a.steps):
+            eng.build(Ds[i % n_d], J=J, K=K, G=G, precision=prec)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms_ = e0.elapsed_time(e1) / a.steps
+        ck_ = clocks.stop()
+        if dist:
+            t = torch.tensor([ms_], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_ = float(t.item())
+        return ms_, ck_, eng.last_build_stats()[1], eng.class_stats(), eng.launch_stats(), G.clone()
+
+    ms64, ck64, nl64, cs, ls, G64 = timed(_lib.FJB_FP64)
+    if a.precision == "routed":
+        ms, ck, nl, cs_r, ls_r, Gr = timed(_lib.FJB_ROUTED)
+        dG = float((Gr - G64).abs().max())
+        prec = _lib.FJB_ROUTED
+    else:
+        ms, ck, nl, cs_r, ls_r, dG = ms64, ck64, nl64, cs, ls, 0.0
+        prec = _lib.FJB_FP64
+    gpu_launches = nl * a.steps
+
+    # roofline of the dominant class kernel of the plain FP64 build
     flops = cost.build_flops(ls)
     top = max(cs, key=lambda r: r["ms"])
     tcls = (top["la"], top["lb"], top["lc"], top["ld"])
@@ -278,6 +284,10 @@ def main():
         "dtype": "f64" if a.precision == "fp64" else "f64+f32",
         "data": "synthetic (seeded cluster, random symmetric densities)",
         "precision": a.precision,
+        "fp64": {"ms_per_step": round(ms64, 3), "clocks": ck64},
+        "speedup_routed_vs_fp64": round(ms64 / ms, 4) if a.precision == "routed" else None,
+        "max_abs_dG_vs_fp64": dG if a.precision == "routed" else None,
+        "route_threshold": 1e-9 if a.precision == "routed" else None,
         "config": {"workload": WORKLOAD, "n_ao": n, "shells": len(w.basis.shells),
                    "tau": w.tau, "quartets_launched": launched, "quartets_computed": computed,
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",

@@ -29,9 +29,10 @@
 namespace fjb {
 std::vector<double> boys_table();
 // fock_compiled.cu: the class-templated register kernels
-bool compiled_available(int la, int lb, int lc, int ld);
-int compiled_blocks_per_sm(int la, int lb, int lc, int ld);
-cudaError_t launch_compiled(int la, int lb, int lc, int ld, int grid, cudaStream_t st, const KArgs &a);
+bool compiled_available(int la, int lb, int lc, int ld, bool fp32);
+int compiled_blocks_per_sm(int la, int lb, int lc, int ld, bool fp32);
+cudaError_t launch_compiled(int la, int lb, int lc, int ld, bool fp32, int grid, cudaStream_t st,
+                            const KArgs &a);
 }
 
 using namespace fjb;
@@ -96,6 +97,39 @@ __global__ void screen_mask_kernel(const Unit *units, int n_units, const LaunchR
     }
 }
 
+// The precision router: one warp per work unit (a lane per ket).  A unit
+// whose every computed quartet has G_ab G_cd dmax under `thresh` goes to the
+// FP32 queue, one with any quartet at or above it to the FP64 queue, one with
+// no computed quartet to neither.  Skipping stays the six-block screen's.
+__global__ void route_units_kernel(const Unit *units, int unit0, int n_units, const LaunchRec *launches,
+                                   const PairRec *pairs, const double *Dsh, int n_sh, double tau,
+                                   double thresh, int *list32, int *list64, int *counts) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int i = warp; i < n_units; i += nwarps) {
+        const Unit U = units[unit0 + i];
+        const LaunchRec L = launches[U.launch];
+        const PairRec bra = pairs[L.bra_pair0 + U.ib];
+        const int ik = U.k0 + lane;
+        bool active = false, low = true;
+        if (ik < U.k1) {
+            const PairRec ket = pairs[L.ket_pair0 + ik];
+            const double b = six_block_bound(Dsh, n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G);
+            active = !(b < tau);
+            low = !active || b < thresh;
+        }
+        const bool any = __any_sync(0xffffffffu, active);
+        const bool all_low = __all_sync(0xffffffffu, low);
+        if (lane == 0 && any) {
+            if (all_low)
+                list32[atomicAdd(counts + 0, 1)] = i;
+            else
+                list64[atomicAdd(counts + 1, 1)] = i;
+        }
+    }
+}
+
 // The HGP Fock kernel (file header of fock_kernels.cuh).  All floating-point
 // work is FP64.
 template <int NT>
@@ -122,7 +156,9 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
     const int nbe = C.nbe, nbf = C.nbf, L = C.L, n_ao = A.n_ao;
     const bool tap = A.tap_out != nullptr;
 
-    for (int u = blockIdx.x; u < A.n_units; u += gridDim.x) {
+    const int n_todo = A.unit_list ? *A.unit_count : A.n_units;
+    for (int ui = blockIdx.x; ui < n_todo; ui += gridDim.x) {
+        const int u = A.unit_list ? A.unit_list[ui] : ui;
         const Unit U = A.units[u];
         const LaunchRec LR = A.launches[U.launch];
         const PairRec bra = A.pairs[LR.bra_pair0 + U.ib];
@@ -472,7 +508,9 @@ struct ClassRun {
     int unit0 = 0, n_units = 0;
     int grid = 0;
     int max_kab = 1, max_kcd = 1;
-    bool compiled = false;  // run on the class-templated register kernel
+    bool compiled = false;  // FP64 units run on the class-templated register kernel
+    bool has32 = false;     // the class has an FP32 register body (routed builds)
+    int grid32 = 0;         // grid of the FP32 register kernel
 };
 
 template <int NT>
@@ -507,9 +545,15 @@ int sm_count() {
 // warps to a CTA; the interpreter one CTA on a unit.
 int run_grid(const ClassRun &r);
 
+// The FP64 path of a class run (its register kernel, else the interpreter).
 cudaError_t launch_run(const ClassRun &r, cudaStream_t st, const KArgs &a) {
-    if (r.compiled) return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, r.grid, st, a);
+    if (r.compiled) return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, false, r.grid, st, a);
     return launch_hgp(r.dev, r.grid, st, a);
+}
+
+// The FP32 register kernel of a class run (routed builds).
+cudaError_t launch_run32(const ClassRun &r, cudaStream_t st, const KArgs &a) {
+    return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, true, r.grid32, st, a);
 }
 
 }  // namespace
@@ -539,6 +583,7 @@ struct fjb_handle {
     int last_launches = 0;
     // measurement
     DevBuf<unsigned long long> computed;
+    DevBuf<int> route_list, route_counts;  // the router's per-class FP32 / FP64 queues
     std::vector<fjb_launch_stat> lstat;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> cev;
     bool built = false;
@@ -629,7 +674,14 @@ int grid_for(const ClassDev &d, int n_units) {
 
 int run_grid(const ClassRun &r) {
     if (!r.compiled) return grid_for(r.dev, r.n_units);
-    const int per_sm = std::max(1, compiled_blocks_per_sm(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld));
+    const int per_sm = std::max(1, compiled_blocks_per_sm(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, false));
+    const int warps_needed = (r.n_units + 3) / 4;
+    return std::max(1, std::min(warps_needed, per_sm * sm_count()));
+}
+
+int run_grid32(const ClassRun &r) {
+    if (!r.has32) return 0;
+    const int per_sm = std::max(1, compiled_blocks_per_sm(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, true));
     const int warps_needed = (r.n_units + 3) / 4;
     return std::max(1, std::min(warps_needed, per_sm * sm_count()));
 }
@@ -793,7 +845,8 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
             const int th = ov == h->cfg.end() ? 0 : ov->second.first;
             run.dev = ov == h->cfg.end() || th == 1 ? ce.dev(deg.first, deg.second)
                                                      : ce.dev(deg.first, deg.second, th, ov->second.second);
-            run.compiled = compiled_available(la, lb, lc, ld) && (th == 0 || th == 1);
+            run.compiled = compiled_available(la, lb, lc, ld, false) && (th == 0 || th == 1);
+            run.has32 = compiled_available(la, lb, lc, ld, true);
             run.unit0 = (int)units.size();
             run.n_units = (int)kv.second.size();
             units.insert(units.end(), kv.second.begin(), kv.second.end());
@@ -814,7 +867,10 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
         return fail(h, FJB_E_CUDA, e.what());
     }
     if (int rc = ensure_smem_attr(h)) return rc;
-    for (auto &r : h->runs) r.grid = run_grid(r);
+    for (auto &r : h->runs) {
+        r.grid = run_grid(r);
+        r.grid32 = run_grid32(r);
+    }
     h->free_class_events();
     for (size_t i = 0; i < h->runs.size(); ++i) {
         cudaEvent_t a, b;
@@ -824,6 +880,8 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     }
     try {
         h->computed.alloc(std::max<size_t>(1, lr.size()));
+        h->route_list.alloc(std::max<size_t>(1, 2 * units.size()));
+        h->route_counts.alloc(std::max<size_t>(1, 2 * h->runs.size()));
     } catch (const std::exception &e) {
         return fail(h, FJB_E_CUDA, e.what());
     }
@@ -947,6 +1005,8 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
     CUDA_OK(h, cudaMemsetAsync(h->Jp.p, 0, nn * sizeof(double), st));
     CUDA_OK(h, cudaMemsetAsync(h->Kp.p, 0, nn * sizeof(double), st));
     CUDA_OK(h, cudaMemsetAsync(h->computed.p, 0, h->computed.n * sizeof(unsigned long long), st));
+    const bool routed = route > 0.0;
+    if (routed) CUDA_OK(h, cudaMemsetAsync(h->route_counts.p, 0, h->route_counts.n * sizeof(int), st));
     CUDA_OK(h, cudaEventRecord(h->ev0, st));
     for (size_t ri = 0; ri < h->runs.size(); ++ri) {
         const ClassRun &r = h->runs[ri];
@@ -968,8 +1028,28 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
         a.Kp = h->Kp.p;
         a.boys_tab = h->boys.p;
         a.route_thresh = route;
-        CUDA_OK(h, launch_run(r, st, a));
-        ++launches;
+        if (routed && r.has32) {
+            // the precision router splits the class's units into an FP32 and
+            // an FP64 queue; each queue has its own kernel
+            int *l32 = h->route_list.p + r.unit0;
+            int *l64 = h->route_list.p + h->n_units + r.unit0;
+            int *cnt = h->route_counts.p + 2 * ri;
+            const int rgrid = std::max(1, std::min((r.n_units + 3) / 4, 16 * sm_count()));
+            route_units_kernel<<<rgrid, 128, 0, st>>>(h->units.p, r.unit0, r.n_units, h->launches.p,
+                                                      h->pairs.p, h->Dsh.p, nsh, h->plan.tau, route, l32,
+                                                      l64, cnt);
+            KArgs a32 = a, a64 = a;
+            a32.unit_list = l32;
+            a32.unit_count = cnt;
+            a64.unit_list = l64;
+            a64.unit_count = cnt + 1;
+            CUDA_OK(h, launch_run32(r, st, a32));
+            CUDA_OK(h, launch_run(r, st, a64));
+            launches += 3;
+        } else {
+            CUDA_OK(h, launch_run(r, st, a));
+            ++launches;
+        }
         CUDA_OK(h, cudaEventRecord(h->cev[ri].second, st));
     }
     h->built = true;
@@ -1164,12 +1244,12 @@ int fjb_set_class_config(fjb_handle *h, int la, int lb, int lc, int ld, int thre
     for (auto &r : h->runs) {
         if (std::make_tuple(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld) != key) continue;
         try {
-            if (threads == 1 && !compiled_available(la, lb, lc, ld))
+            if (threads == 1 && !compiled_available(la, lb, lc, ld, false))
                 return fail(h, FJB_E_LIMIT, "this class has no compiled register kernel");
             ClassDev d = threads == 1 ? h->cls(la, lb, lc, ld).dev(r.max_kab, r.max_kcd)
                                       : h->cls(la, lb, lc, ld).dev(r.max_kab, r.max_kcd, threads, slots);
             r.dev = d;
-            r.compiled = compiled_available(la, lb, lc, ld) && (threads == 0 || threads == 1);
+            r.compiled = compiled_available(la, lb, lc, ld, false) && (threads == 0 || threads == 1);
             r.grid = run_grid(r);
         } catch (const std::length_error &e) {
             return fail(h, FJB_E_LIMIT, e.what());

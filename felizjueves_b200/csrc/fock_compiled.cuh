@@ -15,9 +15,10 @@
 //
 // R = double is the plain FP64 path.  R = float is the routed path's
 // recurrence type: the quartet's scalars, Boys values, density blocks and
-// every J/K/G accumulation stay FP64; a warp takes it only when every
-// computed quartet of the warp is under the routing threshold
-// (G_ab G_cd dmax < threshold, the same bound the six-block screen uses).
+// every J/K/G accumulation stay FP64.  The router (route_units_kernel) hands
+// the FP32 instantiation only units whose every computed quartet is under
+// the routing threshold (G_ab G_cd dmax < threshold, the bound the six-block
+// screen uses).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -209,40 +210,42 @@ __device__ __forceinline__ void quartet_compiled(const KArgs &A, const PairRec &
     }
 }
 
-template <int LA, int LB, int LC, int LD>
+// The units a kernel takes: all of them, or the device-side queue the
+// precision router filled (A.unit_list, *A.unit_count entries).
+__device__ __forceinline__ int units_to_do(const KArgs &A) {
+    return A.unit_list ? *A.unit_count : A.n_units;
+}
+__device__ __forceinline__ int unit_at(const KArgs &A, int i) { return A.unit_list ? A.unit_list[i] : i; }
+
+template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128) hgp_compiled_kernel(const KArgs A) {
     constexpr int NA = cnc(LA), NB = cnc(LB), NAB = NA * NB;
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-    for (int u = warp; u < A.n_units; u += nwarps) {
+    const int n = units_to_do(A);
+    for (int ui = warp; ui < n; ui += nwarps) {
+        const int u = unit_at(A, ui);
         const Unit U = A.units[u];
         const LaunchRec LR = A.launches[U.launch];
         const PairRec bra = A.pairs[LR.bra_pair0 + U.ib];
         const int ik = U.k0 + lane;
         bool active = ik < U.k1;
         PairRec ket{};
-        double bound = 0.0;
         if (active) {
             ket = A.pairs[LR.ket_pair0 + ik];
             active = !skip6(A.Dsh, A.n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G, A.tau);
-            if (active && A.route_thresh > 0.0) bound = six_block_bound(A.Dsh, A.n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G);
         }
         const unsigned mask = __ballot_sync(0xffffffffu, active);
         if (!mask) continue;
         if (A.computed && lane == 0) atomicAdd(A.computed + U.launch, (unsigned long long)__popc(mask));
-        const bool low = A.route_thresh > 0.0 &&
-                         __all_sync(0xffffffffu, !active || bound < A.route_thresh);
         double jab[NAB];
 #pragma unroll
         for (int t = 0; t < NAB; ++t) jab[t] = 0.0;
         if (active) {
             const double deg = (bra.a == bra.b ? 0.5 : 1.0) * (ket.a == ket.b ? 0.5 : 1.0) *
                                ((LR.diag && ik == U.ib) ? 0.5 : 1.0);
-            if (low)
-                quartet_compiled<LA, LB, LC, LD, float>(A, bra, ket, deg, jab);
-            else
-                quartet_compiled<LA, LB, LC, LD, double>(A, bra, ket, deg, jab);
+            quartet_compiled<LA, LB, LC, LD, R>(A, bra, ket, deg, jab);
         }
 #pragma unroll
         for (int t = 0; t < NAB; ++t) {

@@ -40,6 +40,8 @@ struct KArgs {
     const uint8_t *route;   // per unit ket flags, routed mode (null: all FP64)
     double route_thresh;
     unsigned long long *computed;  // per launch: quartets computed (null: not counted)
+    const int *unit_list;   // device queue of unit indices (null: every unit)
+    const int *unit_count;  // its length, on the device
 };
 
 __device__ __forceinline__ void boys_eval(int M, double T, double *F, const double *__restrict__ tab) {

@@ -32,7 +32,11 @@ namespace {
 // (Measured with ptxas -v on sm_100a: up to ~500 nodes the FP64 bodies fit
 // the 255-register file with at most a few KiB of spill; from ~650 nodes
 // ptxas falls back to a 32-register allocation with 20-60 KiB of stack.)
-constexpr int kMaxVrrNodes = 520;
+// The FP32 bodies (the routed path's recurrence type) hold twice as many
+// values in the same registers, so they are generated up to twice the size;
+// their FP64 twins only up to kMaxVrrNodes64.
+constexpr int kMaxVrrNodes64 = 500;
+constexpr int kMaxVrrNodes = 1100;
 constexpr int kMaxHrrTerms = 6000;
 
 std::string n(int i) { return "n" + std::to_string(i); }
@@ -126,6 +130,7 @@ int main(int argc, char **argv) {
     o << "// Generated by gen_hgp.cpp from hgp_tables.cpp's programs; do not edit.\n#pragma once\n\n"
       << "namespace fjb {\n\n";
     std::vector<std::string> names;
+    std::vector<int> has64;
     for (int la = 0; la <= kMaxL; ++la)
         for (int lb = la; lb <= kMaxL; ++lb)
             for (int lc = 0; lc <= kMaxL; ++lc)
@@ -137,9 +142,15 @@ int main(int argc, char **argv) {
                     emit_class(o, c);
                     names.push_back(std::to_string(la) + std::to_string(lb) + std::to_string(lc) +
                                     std::to_string(ld));
+                    has64.push_back(c.vrr_nodes() <= kMaxVrrNodes64);
                 }
+    // X(la, lb, lc, ld, fp64): every compiled class has an FP32 body; fp64
+    // says whether its FP64 twin is instantiated too.
     o << "}  // namespace fjb\n\n#define FJB_COMPILED_CLASSES(X)";
-    for (auto &s : names) o << " X(" << s[0] << ", " << s[1] << ", " << s[2] << ", " << s[3] << ")";
+    for (size_t i = 0; i < names.size(); ++i) {
+        const auto &s = names[i];
+        o << " X(" << s[0] << ", " << s[1] << ", " << s[2] << ", " << s[3] << ", " << has64[i] << ")";
+    }
     o << "\n";
     std::printf("%zu compiled classes\n", names.size());
     return 0;

@@ -141,6 +141,27 @@ def test_cluster_fp64_matches_oracle(cuda, lib_built, oracle_lib, atoms, seed):
     assert np.abs(G - (Jo - 0.5 * Ko)).max() <= FP64_ABS
 
 
+@pytest.mark.parametrize("atoms,seed", [(3, 5), (4, 7)])
+def test_routed_build_within_budget(cuda, lib_built, oracle_lib, atoms, seed):
+    """The routed build (FP32 recurrences for quartets under the 1e-9
+    Schwarz x |D| bound) stays within the metric's budget max|dG| <= 1e-8
+    against the FP64 build and against the oracle; the error is reported."""
+    import torch
+    from felizjueves_b200 import _lib
+    w = configs.cluster(atoms, seed)
+    eng = FockEngine(w.basis)
+    eng.plan(w.D, w.tau, w.n_mag)
+    D = torch.tensor(w.D, device=cuda)
+    G64 = eng.build(D)[2].clone()
+    G32 = eng.build(D, precision=_lib.FJB_ROUTED, threshold=1e-9)[2].clone()
+    torch.cuda.synchronize()
+    Jo, Ko = oracle_lib.jk(oracle_lib.OracleBasis.of(w.basis), w.D)
+    d64 = float((G32 - G64).abs().max())
+    dor = float(np.abs(G32.cpu().numpy() - (Jo - 0.5 * Ko)).max())
+    print(f"routed: max|dG| vs FP64 {d64:.3e}, vs oracle {dor:.3e}")
+    assert d64 <= 1e-8 and dor <= 1e-8
+
+
 def test_device_build_matches_host_build(cuda, lib_built):
     import torch
     w = configs.c0()
