@@ -12,10 +12,11 @@ compared class by class, and the winner is set.
 from __future__ import annotations
 
 import json
+import os
 
 import numpy as np
 
-CANDIDATES = ((32, 0), (64, 0), (128, 0), (256, 0))
+CANDIDATES = ((1, 0), (32, 0), (64, 0), (128, 0), (256, 0), (512, 0))  # (1, 0): register kernel
 
 
 def autotune(eng, D, candidates=CANDIDATES, reps: int = 1, precision: int = 0) -> dict:
@@ -77,3 +78,16 @@ def apply(eng, table: dict) -> None:
 def save(table: dict, path: str) -> None:
     with open(path, "w") as f:
         json.dump(table, f, indent=1)
+
+
+DEFAULT_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
+                             "class_config.json")
+
+
+def load_default() -> dict | None:
+    """The shipped per-class choice (made by `autotune` on the 64-atom
+    cluster on a B200), or None."""
+    if not os.path.exists(DEFAULT_TABLE):
+        return None
+    with open(DEFAULT_TABLE) as f:
+        return json.load(f)

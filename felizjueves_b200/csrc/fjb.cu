@@ -529,6 +529,7 @@ cudaError_t launch_hgp(const ClassDev &d, int grid, cudaStream_t st, const KArgs
         case 64: hgp_fock_kernel<64><<<grid, 64, smem, st>>>(a); break;
         case 128: hgp_fock_kernel<128><<<grid, 128, smem, st>>>(a); break;
         case 256: hgp_fock_kernel<256><<<grid, 256, smem, st>>>(a); break;
+        case 512: hgp_fock_kernel<512><<<grid, 512, smem, st>>>(a); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -663,7 +664,8 @@ int grid_for(const ClassDev &d, int n_units) {
         case 32: per_sm = occupancy<32>(d); break;
         case 64: per_sm = occupancy<64>(d); break;
         case 128: per_sm = occupancy<128>(d); break;
-        default: per_sm = occupancy<256>(d); break;
+        case 256: per_sm = occupancy<256>(d); break;
+        default: per_sm = occupancy<512>(d); break;
     }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -694,6 +696,7 @@ int ensure_smem_attr(fjb_handle *h) {
     CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     done = true;
     return 0;
 }
@@ -1232,8 +1235,9 @@ int fjb_launch_stats(const fjb_handle *hc, fjb_launch_stat *out, int64_t n) {
 
 int fjb_set_class_config(fjb_handle *h, int la, int lb, int lc, int ld, int threads, int slots) {
     if (!h) return fail(h, FJB_E_ARG, "null handle");
-    if (threads != 0 && threads != 1 && threads != 32 && threads != 64 && threads != 128 && threads != 256)
-        return fail(h, FJB_E_ARG, "threads must be 0, 1 (register kernel), 32, 64, 128 or 256");
+    if (threads != 0 && threads != 1 && threads != 32 && threads != 64 && threads != 128 && threads != 256 &&
+        threads != 512)
+        return fail(h, FJB_E_ARG, "threads must be 0, 1 (register kernel), 32, 64, 128, 256 or 512");
     if (slots < 0 || slots > kMaxThreads) return fail(h, FJB_E_ARG, "slots out of range");
     auto key = std::make_tuple(la, lb, lc, ld);
     if (threads == 0 && slots == 0)

@@ -13,7 +13,7 @@ constexpr double kBoysDelta = 0.05;
 constexpr double kBoysTMax = 40.0;  // table covers [0, kBoysTMax]
 constexpr int kBoysNT = 801;        // kBoysTMax / kBoysDelta + 1
 constexpr int kThreads = 128;       // widest CTA of the HGP kernel's default choice
-constexpr int kMaxThreads = 256;    // widest CTA the kernel is instantiated for
+constexpr int kMaxThreads = 512;    // widest CTA the kernel is instantiated for
 constexpr int kKetChunk = 32;       // ket pairs per work unit (one per lane of a warp)
 constexpr int kNumScalars = 17;     // per-primitive-quartet VRR scalars
 

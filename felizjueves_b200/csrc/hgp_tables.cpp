@@ -250,15 +250,18 @@ ClassHost build_class(int la, int lb, int lc, int ld) {
 }
 
 void default_config(const ClassHost &c, int budget, int *threads, int *target) {
+    // About 16 warps an SM in every regime: many one-warp CTAs for small
+    // programs, four 128-thread CTAs for mid-size ones, one 512-thread CTA
+    // for the largest (whose shared memory allows a single CTA an SM).
     if (c.n_nodes <= 1200) {
         *threads = 32;
         *target = budget / 16;
     } else if (c.n_nodes <= 4000) {
-        *threads = 64;
-        *target = budget / 8;
-    } else {
         *threads = 128;
-        *target = budget / 2;
+        *target = budget / 4;
+    } else {
+        *threads = 512;
+        *target = budget;
     }
 }
 

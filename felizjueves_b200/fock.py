@@ -141,11 +141,15 @@ class FockEngine:
     """One basis on one GPU.  `plan(D, tau, n)` builds and stages the pair
     stream; `build(D)` runs the fused J/K/G build."""
 
-    def __init__(self, basis: Basis, device: int = 0):
+    def __init__(self, basis: Basis, device: int = 0, tuned: bool = True):
+        """`device` -1 makes a host-only handle (plans and lists, no builds);
+        `tuned` applies the autotuner's shipped per-class configuration
+        (felizjueves_b200/data/class_config.json) after each plan."""
         if not isinstance(basis, Basis):
             raise ValueError(f"{basis!r} is not a Basis")
         self.basis = basis
         self.device = int(device)
+        self.tuned = bool(tuned)
         self._L = _lib.load()
         f = basis.flat()
         self._flat = f  # keep alive for the call
@@ -181,6 +185,11 @@ class FockEngine:
         _lib.check(self._L.fjb_plan(self._h, A.ctypes.data, tau, n), self._h)
         self._tau = tau
         self._plan = self._export(n)
+        if self.tuned and self.device >= 0:
+            from . import autotune
+            table = autotune.load_default()
+            if table:
+                autotune.apply(self, table)
         return self._plan
 
     def counts_raw(self) -> dict[str, int]:
