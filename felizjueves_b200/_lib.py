@@ -74,6 +74,7 @@ def load():
     L.fjb_fma_probe.argtypes = [C.c_int, C.c_int, C.POINTER(dbl)]
     L.fjb_fock_build_noalloc.argtypes = [vp, vp, vp, vp, vp, vp]
     L.fjb_set_class_config.argtypes = [vp] + [C.c_int] * 6
+    L.fjb_fock_build_graph.argtypes = [vp, vp, vp, vp, vp, C.c_int, dbl, vp]
     _lib = L
     return L
 
@@ -82,7 +83,8 @@ EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_
            "fjb_plan", "fjb_plan_counts", "fjb_plan_export", "fjb_screen_mask",
            "fjb_fock_build", "fjb_fock_build_host", "fjb_eri_blocks", "fjb_boys",
            "fjb_last_build_stats", "fjb_launch_stats", "fjb_class_stats",
-           "fjb_fma_probe", "fjb_fock_build_noalloc", "fjb_set_class_config")
+           "fjb_fma_probe", "fjb_fock_build_noalloc", "fjb_set_class_config",
+           "fjb_fock_build_graph")
 
 
 class LaunchStat_t(C.Structure):

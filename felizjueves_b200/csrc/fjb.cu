@@ -588,6 +588,16 @@ struct fjb_handle {
     std::vector<fjb_launch_stat> lstat;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> cev;
     bool built = false;
+    // the captured build (fjb_fock_build_graph)
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    const void *g_sig[4] = {nullptr, nullptr, nullptr, nullptr};
+    int g_prec = -1;
+    double g_thr = 0.0;
+    void drop_graph() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+    }
 
     void free_class_events() {
         for (auto &e : cev) {
@@ -596,7 +606,11 @@ struct fjb_handle {
         }
         cev.clear();
     }
-    ~fjb_handle() { free_class_events(); }
+    ~fjb_handle() {
+        drop_graph();
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+        free_class_events();
+    }
 
     ClassEntry &cls(int la, int lb, int lc, int ld) {
         auto key = std::make_tuple(la, lb, lc, ld);
@@ -772,6 +786,7 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     if (h->device >= 0) cudaSetDevice(h->device);
     h->planned = false;
     h->lstat.clear();
+    h->drop_graph();
     try {
         unsigned nt = std::max(1u, std::thread::hardware_concurrency());
         h->plan = f_launches(h->basis, D_host, tau, n_mag, (int)nt);
@@ -1064,6 +1079,41 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
     return FJB_OK;
 }
 
+int fjb_fock_build_graph(fjb_handle *h, const double *D_dev, double *J_dev, double *K_dev, double *G_dev,
+                         int precision, double threshold, void *stream) {
+    if (!h || !D_dev) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    CUDA_OK(h, cudaSetDevice(h->device));
+    const void *sig[4] = {D_dev, J_dev, K_dev, G_dev};
+    const bool same = h->gexec && std::equal(sig, sig + 4, h->g_sig) && h->g_prec == precision &&
+                      h->g_thr == threshold;
+    if (!same) {
+        h->drop_graph();
+        if (!h->cap_stream) CUDA_OK(h, cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
+        CUDA_OK(h, cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = fjb_fock_build(h, D_dev, J_dev, K_dev, G_dev, precision, threshold, h->cap_stream);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(h->cap_stream, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ec != cudaSuccess) return fail(h, FJB_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+        const cudaError_t ei = cudaGraphInstantiate(&h->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) {
+            h->gexec = nullptr;
+            return fail(h, FJB_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+        }
+        std::copy(sig, sig + 4, h->g_sig);
+        h->g_prec = precision;
+        h->g_thr = threshold;
+    }
+    CUDA_OK(h, cudaGraphLaunch(h->gexec, (cudaStream_t)stream));
+    return FJB_OK;
+}
+
 int fjb_fock_build_host(fjb_handle *h, const double *D_host, double *J_host, double *K_host,
                         double *G_host, int precision, double threshold) {
     if (!h || !D_host) return fail(h, FJB_E_ARG, "null argument");
@@ -1240,6 +1290,7 @@ int fjb_set_class_config(fjb_handle *h, int la, int lb, int lc, int ld, int thre
         return fail(h, FJB_E_ARG, "threads must be 0, 1 (register kernel), 32, 64, 128, 256 or 512");
     if (slots < 0 || slots > kMaxThreads) return fail(h, FJB_E_ARG, "slots out of range");
     auto key = std::make_tuple(la, lb, lc, ld);
+    h->drop_graph();  // a captured build holds the old launches
     if (threads == 0 && slots == 0)
         h->cfg.erase(key);
     else

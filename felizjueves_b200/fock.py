@@ -245,9 +245,11 @@ class FockEngine:
             raise RuntimeError("no plan: call plan(D, tau, n) first")
 
     def build(self, D, *, J=None, K=None, G=None, precision: int = _lib.FJB_FP64,
-              threshold: float = 0.0, stream=None):
+              threshold: float = 0.0, stream=None, graph: bool = False):
         """Device build: D (torch, cuda, float64, n x n, symmetric) in; J, K,
-        G (allocated if not given) out.  Stream-ordered, not synchronised."""
+        G (allocated if not given) out.  Stream-ordered, not synchronised.
+        `graph=True` replays the build as a captured CUDA graph (captured on
+        the first call for these tensors; update D in place between calls)."""
         import torch
         self._require_plan()
         n = self.n_ao
@@ -260,10 +262,10 @@ class FockEngine:
                 M = torch.empty((n, n), dtype=torch.float64, device=D.device)
             out.append(M)
         st = stream if stream is not None else torch.cuda.current_stream(D.device)
-        _lib.check(self._L.fjb_fock_build(self._h, D.data_ptr(), out[0].data_ptr(),
-                                          out[1].data_ptr(), out[2].data_ptr(),
-                                          int(precision), float(threshold),
-                                          C.c_void_p(st.cuda_stream)), self._h)
+        fn = self._L.fjb_fock_build_graph if graph else self._L.fjb_fock_build
+        _lib.check(fn(self._h, D.data_ptr(), out[0].data_ptr(), out[1].data_ptr(),
+                      out[2].data_ptr(), int(precision), float(threshold),
+                      C.c_void_p(st.cuda_stream)), self._h)
         return tuple(out)
 
     def build_host(self, D, *, precision: int = _lib.FJB_FP64, threshold: float = 0.0):
@@ -361,3 +363,24 @@ def fock_two_electron(basis: Basis, D, *, tau: float = 0.0, n: int = 4, device: 
 
 def eri_block(basis: Basis, a: int, b: int, c: int, d: int, device: int = 0) -> np.ndarray:
     return FockEngine(basis, device).eri_blocks([(a, b, c, d)])[0]
+
+
+def diagonal_matrix(basis: Basis, device: int = 0) -> np.ndarray:
+    """(mn|mn) for every AO pair, n_ao x n_ao (eri/schwarz.py:86-93): the
+    diagonals of the (ab|ab) blocks of every shell pair a <= b, computed on
+    the GPU by the build's own HGP recurrences, placed at (m, n) and (n, m)."""
+    sh, off = basis.shells, basis.offsets
+    quartets = [(a, b, a, b) for a in range(len(sh)) for b in range(a, len(sh))]
+    blocks = FockEngine(basis, device, tuned=False).eri_blocks(quartets)
+    M = np.zeros((basis.n_ao, basis.n_ao))
+    for (a, b, _, _), blk in zip(quartets, blocks):
+        na, nb = sh[a].n_cart, sh[b].n_cart
+        d = np.diagonal(blk).reshape(na, nb)
+        M[off[a]:off[a] + na, off[b]:off[b] + nb] = d
+        M[off[b]:off[b] + nb, off[a]:off[a] + na] = d.T
+    return M
+
+
+def schwarz_matrix(basis: Basis, device: int = 0) -> np.ndarray:
+    """Q[m][n] = sqrt(max((mn|mn), 0)), symmetric (eri/schwarz.py:102)."""
+    return np.sqrt(np.maximum(diagonal_matrix(basis, device), 0.0))

@@ -132,6 +132,15 @@ int fjb_screen_mask(fjb_handle *h, const double *D_dev, uint8_t *mask_dev,
 int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_dev,
                    double *G_dev, int precision, double threshold, void *stream);
 
+/* fjb_fock_build as a CUDA graph: the first call for a given (D_dev, J_dev,
+ * K_dev, G_dev, precision, threshold) captures the build's whole kernel
+ * sequence on a handle-owned stream and instantiates it; every call then
+ * launches that graph on `stream`.  An SCF loop that updates D in place
+ * replays one graph per iteration.  A new plan, or other pointers, capture
+ * again. */
+int fjb_fock_build_graph(fjb_handle *h, const double *D_dev, double *J_dev, double *K_dev,
+                         double *G_dev, int precision, double threshold, void *stream);
+
 /* The same build through host buffers: D_host in, J/K/G_host out (any of
  * the outputs may be NULL).  Copies in, builds, copies out, synchronises. */
 int fjb_fock_build_host(fjb_handle *h, const double *D_host, double *J_host,

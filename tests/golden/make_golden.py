@@ -92,6 +92,19 @@ def part_libcint():
                                               f"{dj['provenance']['pyscf']}, libcint "
                                               f"{dj['provenance']['libcint']})"))
         print("libcint", name, n)
+    for name in ("h2_sto3g", "h2o_sto3g", "h2o_631g"):
+        ds = json.load(open(os.path.join(fx, name + "_schwarz.json")))
+        assert ds["provenance"]["cart"] is True
+        conv = ds["converted"]["shells"]
+        n = ds["nao"]
+        diag = np.asarray(ds["arrays"]["int2e_diag"]["values"]).reshape(n, n)
+        sh = flat_shells([s["l"] for s in conv], [s["centre"] for s in conv],
+                         [s["exponents"] for s in conv],
+                         [s["coefficients"] for s in conv])
+        np.savez_compressed(os.path.join(HERE, f"libcint_{name}_schwarz.npz"),
+                            int2e_diag=diag, **sh,
+                            source=np.asarray(f"test/oracle/fixtures/{name}_schwarz.json"))
+        print("libcint schwarz", name, n)
 
 
 # --- Boys -------------------------------------------------------------------

@@ -162,6 +162,32 @@ def test_routed_build_within_budget(cuda, lib_built, oracle_lib, atoms, seed):
     assert d64 <= 1e-8 and dor <= 1e-8
 
 
+def test_graph_build_replays_the_build(cuda, lib_built):
+    """The captured build equals the direct one, and replaying it after D is
+    updated in place gives the new density's result (the SCF-loop use)."""
+    import torch
+    from felizjueves_b200 import _lib
+    w = configs.cluster(2, 3)
+    eng = FockEngine(w.basis)
+    eng.plan(w.D, w.tau, w.n_mag)
+    D = torch.tensor(w.D, device=cuda)
+    D2 = torch.tensor(configs.perturbed_density(w.D, 3), device=cuda)
+    for prec in (_lib.FJB_FP64, _lib.FJB_ROUTED):
+        ref1 = [t.clone() for t in eng.build(D, precision=prec)]
+        ref2 = [t.clone() for t in eng.build(D2, precision=prec)]
+        Dw = D.clone()
+        out = [torch.empty_like(D) for _ in range(3)]
+        eng.build(Dw, J=out[0], K=out[1], G=out[2], precision=prec, graph=True)
+        torch.cuda.synchronize()
+        for a, b in zip(out, ref1):
+            assert float((a - b).abs().max()) <= 1e-11
+        Dw.copy_(D2)
+        eng.build(Dw, J=out[0], K=out[1], G=out[2], precision=prec, graph=True)
+        torch.cuda.synchronize()
+        for a, b in zip(out, ref2):
+            assert float((a - b).abs().max()) <= 1e-11
+
+
 def test_device_build_matches_host_build(cuda, lib_built):
     import torch
     w = configs.c0()
@@ -206,3 +232,18 @@ def test_refuses_asymmetric_density(cuda, lib_built):
     D[2, 5] *= 1 + 1e-15
     with pytest.raises(ValueError, match="not symmetric"):
         eng.plan(D, w.tau, 4)
+
+
+@pytest.mark.parametrize("name", ["h2_sto3g", "h2o_sto3g", "h2o_631g"])
+def test_schwarz_diagonal_matches_libcint(cuda, lib_built, name):
+    """(mn|mn) of every AO pair (eri/schwarz.py:86-102) against libcint's
+    int2e diagonal the reference tracks; Q = sqrt(max(., 0))."""
+    from felizjueves_b200.fock import diagonal_matrix, schwarz_matrix
+    g = golden(f"libcint_{name}_schwarz.npz")
+    B = _basis_from_npz(g)
+    M = diagonal_matrix(B)
+    ref = g["int2e_diag"]
+    assert np.abs(M - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert np.array_equal(M, M.T)
+    Q = schwarz_matrix(B)
+    assert np.allclose(Q, np.sqrt(np.maximum(ref, 0.0)), rtol=1e-11, atol=1e-14)
