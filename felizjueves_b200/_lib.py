@@ -75,6 +75,8 @@ def load():
     L.fjb_fock_build_noalloc.argtypes = [vp, vp, vp, vp, vp, vp]
     L.fjb_set_class_config.argtypes = [vp] + [C.c_int] * 6
     L.fjb_fock_build_graph.argtypes = [vp, vp, vp, vp, vp, C.c_int, dbl, vp]
+    L.fjb_create_df.argtypes = [C.POINTER(vp), C.POINTER(Basis_t), C.POINTER(Basis_t), C.c_int]
+    L.fjb_df_blocks.argtypes = [vp, C.c_int, vp, C.c_int, vp, vp]
     _lib = L
     return L
 
@@ -84,7 +86,7 @@ EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_
            "fjb_fock_build", "fjb_fock_build_host", "fjb_eri_blocks", "fjb_boys",
            "fjb_last_build_stats", "fjb_launch_stats", "fjb_class_stats",
            "fjb_fma_probe", "fjb_fock_build_noalloc", "fjb_set_class_config",
-           "fjb_fock_build_graph")
+           "fjb_fock_build_graph", "fjb_create_df", "fjb_df_blocks")
 
 
 class LaunchStat_t(C.Structure):

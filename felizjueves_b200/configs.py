@@ -169,3 +169,20 @@ def by_name(name: str) -> Workload:
     if name.startswith("cluster") and name[7:].isdigit():
         return cluster(int(name[7:]), 5)
     raise ValueError(f"unknown workload {name!r}")
+
+
+# The auxiliary basis recipe (even-tempered s..g, exponents 0.1 * 2.2^k,
+# uncontracted, coefficient primitive_norm): per atom s x10, p x7, d x4, f x2,
+# g x1 -> 90 Cartesian functions, about 3x the 31 of the c1 shell recipe.
+AUX_COUNTS = (10, 7, 4, 2, 1)
+
+
+def aux_basis(w: Workload) -> Basis:
+    shells = []
+    for c in w.coords:
+        centre = tuple(map(float, c))
+        for l, count in enumerate(AUX_COUNTS):
+            for k in range(count):
+                a = 0.1 * 2.2 ** k
+                shells.append(Shell(l, centre, [a], [primitive_norm(l, a)]))
+    return Basis(tuple(shells))

@@ -588,6 +588,9 @@ struct fjb_handle {
     std::vector<fjb_launch_stat> lstat;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> cev;
     bool built = false;
+    // a density-fitting handle: AO shells, then aux shells, then the unit shell
+    bool df = false;
+    int df_ao_shells = 0, df_aux_shells = 0;
     // the captured build (fjb_fock_build_graph)
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -723,18 +726,22 @@ const char *fjb_last_error(const fjb_handle *h) { return h ? h->err.c_str() : g_
 
 const char *fjb_version(void) { return "fjb 0.1 sm_100a"; }
 
-int fjb_create(fjb_handle **out, const fjb_basis *b, int device) {
-    if (!out || !b || b->n_shells <= 0) return fail(nullptr, FJB_E_ARG, "no basis");
-    auto h = std::make_unique<fjb_handle>();
-    h->device = device;
-    int n = 0;
+}  // extern "C"
+
+namespace {
+
+// Append a basis's shells to the handle's, refusing what the reference
+// refuses (ao/shell.py:110-140) and l above `max_l`.
+int append_shells(fjb_handle *h, const fjb_basis *b, int max_l) {
+    if (!b || b->n_shells <= 0) return fail(nullptr, FJB_E_ARG, "no basis");
+    int n = h->basis.n_ao;
     for (int s = 0; s < b->n_shells; ++s) {
         HostShell sh;
         sh.l = b->l[s];
         if (sh.l < 0) return fail(nullptr, FJB_E_ARG, "angular momentum is not an int >= 0");
-        if (sh.l > FJB_MAX_L)
+        if (sh.l > max_l)
             return fail(nullptr, FJB_E_LIMIT, "l = " + std::to_string(sh.l) + " above the compiled maximum " +
-                                                   std::to_string(FJB_MAX_L));
+                                                   std::to_string(max_l));
         for (int d = 0; d < 3; ++d) {
             sh.centre[d] = b->centre[3 * s + d];
             if (!std::isfinite(sh.centre[d])) return fail(nullptr, FJB_E_ARG, "centre has a non-finite entry");
@@ -752,6 +759,13 @@ int fjb_create(fjb_handle **out, const fjb_basis *b, int device) {
         h->basis.shells.push_back(std::move(sh));
     }
     h->basis.n_ao = n;
+    return FJB_OK;
+}
+
+// Device staging common to every handle: the Boys table, shell offsets and
+// sizes, the build events.
+int finish_create(std::unique_ptr<fjb_handle> &h, fjb_handle **out) {
+    const int device = h->device;
     if (device < 0) {  // host-only handle: plans and exports, no builds
         *out = h.release();
         return FJB_OK;
@@ -772,6 +786,39 @@ int fjb_create(fjb_handle **out, const fjb_basis *b, int device) {
     return FJB_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int fjb_create(fjb_handle **out, const fjb_basis *b, int device) {
+    if (!out || !b || b->n_shells <= 0) return fail(nullptr, FJB_E_ARG, "no basis");
+    auto h = std::make_unique<fjb_handle>();
+    h->device = device;
+    if (int rc = append_shells(h.get(), b, FJB_MAX_L)) return rc;
+    return finish_create(h, out);
+}
+
+int fjb_create_df(fjb_handle **out, const fjb_basis *ao, const fjb_basis *aux, int device) {
+    if (!out || !ao || !aux) return fail(nullptr, FJB_E_ARG, "no basis");
+    if (device < 0) return fail(nullptr, FJB_E_ARG, "the integrals need a device");
+    auto h = std::make_unique<fjb_handle>();
+    h->device = device;
+    if (int rc = append_shells(h.get(), ao, FJB_MAX_L)) return rc;
+    h->df_ao_shells = (int)h->basis.shells.size();
+    if (int rc = append_shells(h.get(), aux, FJB_MAX_L_AUX)) return rc;
+    h->df_aux_shells = (int)h->basis.shells.size() - h->df_ao_shells;
+    HostShell unit;  // the aux primitives' partner: exponent 0, coefficient 1
+    unit.l = 0;
+    unit.centre[0] = unit.centre[1] = unit.centre[2] = 0.0;
+    unit.exps.push_back(0.0);
+    unit.coefs.push_back(1.0);
+    h->basis.offsets.push_back(h->basis.n_ao);
+    h->basis.n_ao += 1;
+    h->basis.shells.push_back(unit);
+    h->df = true;
+    return finish_create(h, out);
+}
+
 void fjb_destroy(fjb_handle *h) {
     if (!h) return;
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -783,6 +830,7 @@ int fjb_n_ao(const fjb_handle *h) { return h ? h->basis.n_ao : -1; }
 
 int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     if (!h || !D_host) return fail(h, FJB_E_ARG, "null argument");
+    if (h->df) return fail(h, FJB_E_STATE, "a density-fitting handle has no pair stream");
     if (h->device >= 0) cudaSetDevice(h->device);
     h->planned = false;
     h->lstat.clear();
@@ -1231,6 +1279,34 @@ int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_de
         return fail(h, FJB_E_CUDA, e.what());
     }
     return FJB_OK;
+}
+
+int fjb_df_blocks(fjb_handle *h, int kind, const int32_t *items, int n, double *out_dev, int64_t *offsets) {
+    if (!h || !items || n < 0 || !offsets) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->df) return fail(h, FJB_E_STATE, "not a density-fitting handle (fjb_create_df)");
+    const int nao_sh = h->df_ao_shells, nx = h->df_aux_shells, unit = nao_sh + nx;
+    std::vector<int32_t> q((size_t)4 * n);
+    for (int i = 0; i < n; ++i) {
+        if (kind == FJB_DF_METRIC) {
+            const int P = items[2 * i], Q = items[2 * i + 1];
+            if (P < 0 || P >= nx || Q < 0 || Q >= nx) return fail(h, FJB_E_ARG, "aux shell index out of range");
+            q[4 * i + 0] = nao_sh + P;
+            q[4 * i + 1] = unit;
+            q[4 * i + 2] = nao_sh + Q;
+            q[4 * i + 3] = unit;
+        } else if (kind == FJB_DF_ERI3) {
+            const int a = items[3 * i], b = items[3 * i + 1], P = items[3 * i + 2];
+            if (a < 0 || a >= nao_sh || b < 0 || b >= nao_sh || P < 0 || P >= nx)
+                return fail(h, FJB_E_ARG, "shell index out of range");
+            q[4 * i + 0] = a;
+            q[4 * i + 1] = b;
+            q[4 * i + 2] = nao_sh + P;
+            q[4 * i + 3] = unit;
+        } else {
+            return fail(h, FJB_E_ARG, "unknown density-fitting kind");
+        }
+    }
+    return fjb_eri_blocks(h, q.data(), n, out_dev, offsets);
 }
 
 int fjb_boys(int m, const double *T_dev, int n, double *F_dev) {

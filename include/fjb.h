@@ -154,6 +154,28 @@ int fjb_fock_build_host(fjb_handle *h, const double *D_host, double *J_host,
 int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_dev,
                    int64_t *offsets);
 
+/* Density fitting (eri/density_fit/metric.py:228 metric_matrix,
+ * eri3.py:226 eri3_tensor).  fjb_create_df makes a handle over the AO basis
+ * (l <= 3) and an auxiliary basis (l <= FJB_MAX_L_AUX); an auxiliary
+ * primitive is the reference's single-Gaussian "pair" (metric.py:1-60),
+ * realised here as the primitive paired with a unit s function (exponent 0,
+ * coefficient 1), which gives exactly its dressing c (pi/alpha)^{3/2}.
+ * fjb_df_blocks computes, on the device, by the build's HGP recurrences:
+ *   kind FJB_DF_METRIC: items[2i..2i+1] = aux shells (P, Q) -> (P|Q) block,
+ *                       rows cartesians(lP), columns cartesians(lQ);
+ *   kind FJB_DF_ERI3:   items[3i..3i+2] = (a, b, P), AO shells a, b and aux
+ *                       shell P -> (ab|P) block, rows a outer then b,
+ *                       columns cartesians(lP) (the reference's [m][n][P]
+ *                       layout, aux fastest).
+ * Blocks land back to back in out_dev (DEVICE); offsets[n+1] (HOST) says
+ * where.  Synchronises. */
+#define FJB_MAX_L_AUX 6
+#define FJB_DF_METRIC 0
+#define FJB_DF_ERI3 1
+int fjb_create_df(fjb_handle **out, const fjb_basis *ao, const fjb_basis *aux, int device);
+int fjb_df_blocks(fjb_handle *h, int kind, const int32_t *items, int n, double *out_dev,
+                  int64_t *offsets);
+
 /* Device Boys F_0..F_m(T[i]) for n arguments into F_dev[i*(m+1) + k]
  * (DEVICE pointers).  Synchronises. */
 int fjb_boys(int m, const double *T_dev, int n, double *F_dev);

@@ -107,6 +107,50 @@ def part_libcint():
         print("libcint schwarz", name, n)
 
 
+# --- density fitting: libcint (P|Q) rows and (mn|P) columns -------------------
+
+DF_SETS = {
+    "prim_spd_f_auxi_metric": ("metric", "prim_spd_f", ["rows0_56", "rows56_104", "rows104_140",
+                                                        "rows140_168"]),
+    "h2o_ccpvtz_jkfit_metric": ("metric", "h2o_ccpvdz_j", ["rows0_43", "rows43_81", "rows81_121",
+                                                          "rows121_166"]),
+    "prim_spd_f_auxi_3c": ("three_center", "prim_spd_f", ["cols0_35", "cols35_84", "cols84_119",
+                                                         "cols119_140", "cols140_168"]),
+    "h2o_sto3g_jkfit_3c": ("three_center", "h2o_sto3g_j", ["cols0_166"]),
+}
+
+
+def part_df():
+    import ast
+    fx = os.path.join(REF, "test", "oracle", "fixtures")
+    for set_name, (kind, parent, pieces) in DF_SETS.items():
+        parts, aux = [], None
+        for piece in pieces:
+            d = json.load(open(os.path.join(fx, f"{set_name}_{piece}.json")))
+            meta = d[kind]
+            conv = meta["converted"]
+            conv = ast.literal_eval(conv) if isinstance(conv, str) else conv
+            if aux is None:
+                aux = conv["shells"]
+            assert conv["shells"] == aux
+            key = [k for k in d["arrays"] if k.startswith("int2c2e_cart" if kind == "metric"
+                                                          else "int3c2e_cart")][0]
+            a = d["arrays"][key]
+            parts.append(np.asarray(a["values"]).reshape(a["shape"]))
+        full = np.concatenate(parts, axis=0 if kind == "metric" else 2)
+        pj = json.load(open(os.path.join(fx, f"{parent}.json")))
+        ao = pj["converted"]["shells"]
+        shA = flat_shells([s["l"] for s in ao], [s["centre"] for s in ao],
+                          [s["exponents"] for s in ao], [s["coefficients"] for s in ao])
+        shX = flat_shells([s["l"] for s in aux], [s["centre"] for s in aux],
+                          [s["exponents"] for s in aux], [s["coefficients"] for s in aux])
+        np.savez_compressed(os.path.join(HERE, f"df_{set_name}.npz"), value=full, kind=kind,
+                            **{"ao_" + k: v for k, v in shA.items()},
+                            **{"aux_" + k: v for k, v in shX.items()},
+                            source=np.asarray(f"test/oracle/fixtures/{set_name}_*.json"))
+        print("df", set_name, full.shape)
+
+
 # --- Boys -------------------------------------------------------------------
 
 
@@ -370,7 +414,7 @@ def part_cost():
     print("cost", len(rows), "classes")
 
 
-PARTS = {"libcint": part_libcint, "boys": part_boys, "eri": part_eri,
+PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_eri,
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "jk_small": part_jk_small,
          "cost": part_cost}

@@ -76,3 +76,29 @@ def test_wrong_weight_fails(oracle_lib):
     J2, _ = oracle_lib.jk(ob, w.D, ordered=True)
     wrong = 0.5 * J  # what weight 1 on the Coulomb blocks would give
     assert np.abs(wrong - J2).max() > 1e3 * 1e-13 * np.abs(J2).max()
+
+
+def _df_bases(z):
+    from felizjueves_b200.shell import Basis, Shell
+
+    def mk(prefix):
+        out = []
+        for s in range(len(z[prefix + "l"])):
+            p0, n = int(z[prefix + "prim0"][s]), int(z[prefix + "nprim"][s])
+            out.append(Shell(int(z[prefix + "l"][s]), tuple(z[prefix + "centre"][s]),
+                             z[prefix + "exps"][p0:p0 + n], z[prefix + "coefs"][p0:p0 + n]))
+        return Basis(tuple(out))
+    return mk("ao_"), mk("aux_")
+
+
+@pytest.mark.parametrize("name", ["h2o_ccpvtz_jkfit_metric", "h2o_sto3g_jkfit_3c"])
+def test_df_integrals_match_libcint(oracle_lib, name):
+    """(P|Q) and (mn|P) by the oracle's eri_block with every aux primitive
+    paired with a unit s function, against libcint's (the fixtures the
+    reference tracks for eri/density_fit)."""
+    from oracle import df as odf
+    z = golden(f"df_{name}.npz")
+    ao, aux = _df_bases(z)
+    got = odf.metric(aux) if str(z["kind"]) == "metric" else odf.eri3(ao, aux)
+    ref = z["value"]
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
