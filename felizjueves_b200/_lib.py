@@ -77,6 +77,13 @@ def load():
     L.fjb_fock_build_graph.argtypes = [vp, vp, vp, vp, vp, C.c_int, dbl, vp]
     L.fjb_create_df.argtypes = [C.POINTER(vp), C.POINTER(Basis_t), C.POINTER(Basis_t), C.c_int]
     L.fjb_df_blocks.argtypes = [vp, C.c_int, vp, C.c_int, vp, vp]
+    L.fjb_mlp_n_params.argtypes = []
+    L.fjb_router_set.argtypes = [vp, vp, C.c_float]
+    L.fjb_router_features.argtypes = [vp, vp, vp, C.c_int, vp, vp]
+    L.fjb_mlp_forward.argtypes = [vp, vp, C.c_int, vp, vp]
+    L.fjb_mlp_gradient.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp, vp]
+    L.fjb_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_float, C.c_int, vp]
+    L.fjb_route_stats.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
     _lib = L
     return L
 
@@ -86,7 +93,9 @@ EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_
            "fjb_fock_build", "fjb_fock_build_host", "fjb_eri_blocks", "fjb_boys",
            "fjb_last_build_stats", "fjb_launch_stats", "fjb_class_stats",
            "fjb_fma_probe", "fjb_fock_build_noalloc", "fjb_set_class_config",
-           "fjb_fock_build_graph", "fjb_create_df", "fjb_df_blocks")
+           "fjb_fock_build_graph", "fjb_create_df", "fjb_df_blocks", "fjb_mlp_n_params",
+           "fjb_router_set", "fjb_router_features", "fjb_mlp_forward", "fjb_mlp_gradient",
+           "fjb_mlp_adam", "fjb_route_stats")
 
 
 class LaunchStat_t(C.Structure):

@@ -25,6 +25,7 @@
 #include "fock_kernels.cuh"
 #include "hgp_tables.h"
 #include "plan.h"
+#include "router.cuh"
 
 namespace fjb {
 std::vector<double> boys_table();
@@ -128,6 +129,64 @@ __global__ void route_units_kernel(const Unit *units, int unit0, int n_units, co
                 list64[atomicAdd(counts + 1, 1)] = i;
         }
     }
+}
+
+// The learned router's unit split: as route_units_kernel, but a quartet the
+// rigorous bound calls high may still go to FP32 when the network predicts
+// its deposit under 10^log_thr.  Screening is untouched (the bound decides
+// what is skipped).
+__global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units, const LaunchRec *launches,
+                                       const PairRec *pairs, const PrimRec *prims, const double *Dsh, int n_sh,
+                                       double tau, double thresh, const float *params, float log_thr, int la,
+                                       int lb, int lc, int ld, int *list32, int *list64, int *counts) {
+    __shared__ float sp[kNParams];
+    for (int i = threadIdx.x; i < kNParams; i += blockDim.x) sp[i] = params[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int i = warp; i < n_units; i += nwarps) {
+        const Unit U = units[unit0 + i];
+        const LaunchRec L = launches[U.launch];
+        const PairRec bra = pairs[L.bra_pair0 + U.ib];
+        const int ik = U.k0 + lane;
+        bool active = false, low = true;
+        if (ik < U.k1) {
+            const PairRec ket = pairs[L.ket_pair0 + ik];
+            const double dmax = six_block_dmax(Dsh, n_sh, bra.a, bra.b, ket.a, ket.b);
+            const double b = __dmul_rn(bra.G, __dmul_rn(ket.G, dmax));
+            active = !(b < tau);
+            if (active && !(b < thresh)) {
+                float f[kFeat];
+                quartet_features(bra, ket, prims, la, lb, lc, ld, dmax, f);
+                low = mlp_forward(sp, f, nullptr, nullptr) < log_thr;
+            }
+        }
+        const bool any = __any_sync(0xffffffffu, active);
+        const bool all_low = __all_sync(0xffffffffu, low);
+        if (lane == 0 && any) {
+            if (all_low)
+                list32[atomicAdd(counts + 0, 1)] = i;
+            else
+                list64[atomicAdd(counts + 1, 1)] = i;
+        }
+    }
+}
+
+// Features (and the six-block bound) of sampled launched quartets
+// (launch, bra index, ket index), for the router's training set.
+__global__ void router_features_kernel(const int32_t *samples, int n, const LaunchRec *launches,
+                                       const PairRec *pairs, const PrimRec *prims, const double *Dsh, int n_sh,
+                                       const int32_t *cls, float *feat, double *bound) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const LaunchRec L = launches[samples[3 * s]];
+    const PairRec bra = pairs[L.bra_pair0 + samples[3 * s + 1]];
+    const PairRec ket = pairs[L.ket_pair0 + samples[3 * s + 2]];
+    const int32_t *c = cls + 4 * samples[3 * s];
+    const double dmax = six_block_dmax(Dsh, n_sh, bra.a, bra.b, ket.a, ket.b);
+    quartet_features(bra, ket, prims, c[0], c[1], c[2], c[3], dmax, feat + (size_t)kFeat * s);
+    bound[s] = __dmul_rn(bra.G, __dmul_rn(ket.G, dmax));
 }
 
 // The HGP Fock kernel (file header of fock_kernels.cuh).  All floating-point
@@ -588,6 +647,12 @@ struct fjb_handle {
     std::vector<fjb_launch_stat> lstat;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> cev;
     bool built = false;
+    // the learned router (fjb_router_set) and the per-launch class table it reads
+    DevBuf<float> router_p;
+    float router_log_thr = 0.f;
+    bool router_on = false;
+    bool last_routed = false;
+    DevBuf<int32_t> launch_cls;
     // a density-fitting handle: AO shells, then aux shells, then the unit shell
     bool df = false;
     int df_ao_shells = 0, df_aux_shells = 0;
@@ -946,6 +1011,14 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     }
     try {
         h->computed.alloc(std::max<size_t>(1, lr.size()));
+        std::vector<int32_t> lc;
+        for (auto &s : h->lstat) {
+            lc.push_back(s.la);
+            lc.push_back(s.lb);
+            lc.push_back(s.lc);
+            lc.push_back(s.ld);
+        }
+        h->launch_cls.upload(lc);
         h->route_list.alloc(std::max<size_t>(1, 2 * units.size()));
         h->route_counts.alloc(std::max<size_t>(1, 2 * h->runs.size()));
     } catch (const std::exception &e) {
@@ -1072,6 +1145,7 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
     CUDA_OK(h, cudaMemsetAsync(h->Kp.p, 0, nn * sizeof(double), st));
     CUDA_OK(h, cudaMemsetAsync(h->computed.p, 0, h->computed.n * sizeof(unsigned long long), st));
     const bool routed = route > 0.0;
+    h->last_routed = routed;
     if (routed) CUDA_OK(h, cudaMemsetAsync(h->route_counts.p, 0, h->route_counts.n * sizeof(int), st));
     CUDA_OK(h, cudaEventRecord(h->ev0, st));
     for (size_t ri = 0; ri < h->runs.size(); ++ri) {
@@ -1101,9 +1175,15 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
             int *l64 = h->route_list.p + h->n_units + r.unit0;
             int *cnt = h->route_counts.p + 2 * ri;
             const int rgrid = std::max(1, std::min((r.n_units + 3) / 4, 16 * sm_count()));
-            route_units_kernel<<<rgrid, 128, 0, st>>>(h->units.p, r.unit0, r.n_units, h->launches.p,
-                                                      h->pairs.p, h->Dsh.p, nsh, h->plan.tau, route, l32,
-                                                      l64, cnt);
+            if (h->router_on)
+                route_units_mlp_kernel<<<rgrid, 128, 0, st>>>(
+                    h->units.p, r.unit0, r.n_units, h->launches.p, h->pairs.p, h->prims.p, h->Dsh.p, nsh,
+                    h->plan.tau, route, h->router_p.p, h->router_log_thr, r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld,
+                    l32, l64, cnt);
+            else
+                route_units_kernel<<<rgrid, 128, 0, st>>>(h->units.p, r.unit0, r.n_units, h->launches.p,
+                                                          h->pairs.p, h->Dsh.p, nsh, h->plan.tau, route, l32,
+                                                          l64, cnt);
             KArgs a32 = a, a64 = a;
             a32.unit_list = l32;
             a32.unit_count = cnt;
@@ -1278,6 +1358,78 @@ int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_de
     } catch (const std::exception &e) {
         return fail(h, FJB_E_CUDA, e.what());
     }
+    return FJB_OK;
+}
+
+int fjb_route_stats(const fjb_handle *hc, int64_t *n32, int64_t *n64) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h || !n32 || !n64) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->built) return fail(h, FJB_E_STATE, "no build yet");
+    CUDA_OK(h, cudaEventSynchronize(h->ev1));
+    std::vector<int> c(h->route_counts.n, 0);
+    if (!c.empty())
+        CUDA_OK(h, cudaMemcpy(c.data(), h->route_counts.p, c.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    *n32 = 0;
+    *n64 = 0;
+    for (size_t ri = 0; ri < h->runs.size(); ++ri) {
+        if (h->last_routed && h->runs[ri].has32) {
+            *n32 += c[2 * ri];
+            *n64 += c[2 * ri + 1];
+        } else {
+            *n64 += h->runs[ri].n_units;
+        }
+    }
+    return FJB_OK;
+}
+
+int fjb_router_set(fjb_handle *h, const float *params_host, float log10_threshold) {
+    if (!h) return fail(h, FJB_E_ARG, "null handle");
+    h->drop_graph();
+    if (!params_host) {
+        h->router_on = false;
+        return FJB_OK;
+    }
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    CUDA_OK(h, cudaSetDevice(h->device));
+    try {
+        h->router_p.upload(std::vector<float>(params_host, params_host + kNParams));
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, e.what());
+    }
+    h->router_log_thr = log10_threshold;
+    h->router_on = true;
+    return FJB_OK;
+}
+
+int fjb_router_features(fjb_handle *h, const double *D_dev, const int32_t *samples, int n, float *feat_dev,
+                        double *bound_dev) {
+    if (!h || !D_dev || !samples || n < 0 || !feat_dev || !bound_dev) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    CUDA_OK(h, cudaSetDevice(h->device));
+    const int nl = (int)h->lstat.size();
+    for (int i = 0; i < n; ++i) {
+        const int li = samples[3 * i], ib = samples[3 * i + 1], ik = samples[3 * i + 2];
+        if (li < 0 || li >= nl) return fail(h, FJB_E_ARG, "sample launch out of range");
+        const PlanBatch &br = h->plan.batches[h->plan.launches[li].first];
+        const PlanBatch &kt = h->plan.batches[h->plan.launches[li].second];
+        if (ib < 0 || ib >= (int)br.pairs.size() || ik < 0 || ik >= (int)kt.pairs.size())
+            return fail(h, FJB_E_ARG, "sample pair index out of range");
+    }
+    const int nsh = (int)h->basis.shells.size();
+    density_blocks_kernel<<<(nsh * nsh + 255) / 256, 256>>>(D_dev, h->basis.n_ao, nsh, h->sh_off.p, h->sh_nc.p,
+                                                          h->Dsh.p);
+    if (n == 0) return FJB_OK;
+    DevBuf<int32_t> ds;
+    try {
+        ds.upload(std::vector<int32_t>(samples, samples + 3 * (size_t)n));
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, e.what());
+    }
+    router_features_kernel<<<(n + 127) / 128, 128>>>(ds.p, n, h->launches.p, h->pairs.p, h->prims.p, h->Dsh.p,
+                                                     nsh, h->launch_cls.p, feat_dev, bound_dev);
+    CUDA_OK(h, cudaGetLastError());
+    CUDA_OK(h, cudaDeviceSynchronize());
     return FJB_OK;
 }
 

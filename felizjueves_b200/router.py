@@ -1,0 +1,222 @@
+"""The learned precision router: training data from the FP64 method, GPU
+training with the library's own kernels, calibration, installation.
+
+The network (csrc/router.cuh) maps 12 pair features of a quartet to the
+predicted log10 of its largest deposit into G, max|(ab|cd)| x dmax (dmax the
+six-block weighted density maximum the screen reads), as the log10 Schwarz x
+density bound (a fixed skip term) plus a learned gap below it.  Training targets are
+computed by the FP64 method itself: the ERI blocks of sampled launched
+quartets from the HGP tap (`FockEngine.eri_blocks`).  Training runs on the
+GPU: `fjb_mlp_gradient` (forward + backward) and `fjb_mlp_adam`, mini-batch
+Adam on the mean squared error.
+
+Routing is conservative by construction: a unit of work goes to FP32 only
+when every computed quartet of it is under the rigorous Schwarz x density
+bound, or predicted under the threshold after subtracting a calibrated
+margin (a high quantile of the validation residuals y - y_pred).  Skipping is
+never the router's: the six-block screen decides it.  `validate` builds the
+routed and the FP64 G once and turns the learned router off if the
+difference breaks the error budget (the FP64 fallback).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from .fock import FockEngine
+
+N_FEAT = 12
+
+
+def n_params() -> int:
+    return int(_lib.load().fjb_mlp_n_params())
+
+
+def init_params(X: np.ndarray, y: np.ndarray | None = None, seed: int = 0) -> np.ndarray:
+    """mu, sd from the training features; Glorot-scaled random weights; the
+    output bias at the mean gap y - bound of the training targets (when
+    given), so training starts from "deposit = bound x typical gap"."""
+    rng = np.random.default_rng(seed)
+    mu = X.mean(0)
+    sd = X.std(0)
+    sd[sd < 1e-3] = 1.0
+    W1 = rng.normal(0, 1 / math.sqrt(N_FEAT), (64, N_FEAT))
+    W2 = rng.normal(0, 1 / math.sqrt(64), (64, 64))
+    w3 = rng.normal(0, 0.1 / math.sqrt(64), 64)
+    b3 = 0.0 if y is None else float(np.mean(y - bound_log10(X)))
+    p = np.concatenate([mu, sd, W1.ravel(), np.zeros(64), W2.ravel(), np.zeros(64), w3, [b3]])
+    assert p.size == n_params()
+    return p.astype(np.float32)
+
+
+def bound_log10(X: np.ndarray) -> np.ndarray:
+    """log10 of the Schwarz x density bound of each sample (features 9-11),
+    the fixed skip term of the network's output."""
+    return X[:, 9:12].astype(np.float64).sum(1)
+
+
+class MLP:
+    """Parameters and Adam state on the device."""
+
+    def __init__(self, params: np.ndarray, device: int = 0):
+        import torch
+        self.dev = torch.device(f"cuda:{device}")
+        self.p = torch.tensor(params, dtype=torch.float32, device=self.dev)
+        self.m = torch.zeros_like(self.p)
+        self.v = torch.zeros_like(self.p)
+        self.step = 0
+        self._L = _lib.load()
+
+    def params(self) -> np.ndarray:
+        return self.p.cpu().numpy()
+
+    def predict(self, X):
+        import torch
+        X = torch.as_tensor(X, dtype=torch.float32, device=self.dev).contiguous()
+        Y = torch.empty(len(X), dtype=torch.float32, device=self.dev)
+        _lib.check(self._L.fjb_mlp_forward(self.p.data_ptr(), X.data_ptr(), len(X), Y.data_ptr(),
+                                           None))
+        return Y
+
+    def gradient(self, X, T):
+        """(gradient, mean squared error) of one batch, by the library's
+        kernels."""
+        import torch
+        X = torch.as_tensor(X, dtype=torch.float32, device=self.dev).contiguous()
+        T = torch.as_tensor(T, dtype=torch.float32, device=self.dev).contiguous()
+        n = len(X)
+        g = torch.zeros_like(self.p)
+        se = torch.empty(n, dtype=torch.float32, device=self.dev)
+        scratch = torch.empty(n * 257, dtype=torch.float32, device=self.dev)
+        _lib.check(self._L.fjb_mlp_gradient(self.p.data_ptr(), X.data_ptr(), T.data_ptr(), n,
+                                            g.data_ptr(), se.data_ptr(), scratch.data_ptr(), None))
+        return g, float(se.mean())
+
+    def train(self, X, T, *, epochs: int = 60, batch: int = 2048, lr: float = 3e-3,
+              seed: int = 0) -> list[float]:
+        """Mini-batch Adam on the mean squared error in log10 units, the
+        learning rate halved every third of the epochs.  Returns the
+        per-epoch mean squared error."""
+        import torch
+        rng = np.random.default_rng(seed)
+        X = torch.as_tensor(X, dtype=torch.float32, device=self.dev)
+        T = torch.as_tensor(T, dtype=torch.float32, device=self.dev)
+        n = len(X)
+        losses = []
+        for ep in range(epochs):
+            rate = lr * 0.5 ** (3 * ep // max(epochs, 1))
+            perm = torch.as_tensor(rng.permutation(n), device=self.dev)
+            tot = 0.0
+            for b0 in range(0, n, batch):
+                idx = perm[b0:b0 + batch]
+                g, mse = self.gradient(X[idx], T[idx])
+                self.step += 1
+                _lib.check(self._L.fjb_mlp_adam(self.p.data_ptr(), g.data_ptr(), self.m.data_ptr(),
+                                                self.v.data_ptr(), C.c_float(rate), self.step, None))
+                tot += mse * len(idx)
+            losses.append(tot / n)
+        return losses
+
+
+def sample_launched(eng: FockEngine, n: int, rng) -> np.ndarray:
+    """n random launched quartets (launch, bra index, ket index), launches
+    drawn by the quartets they hold; the canonical half on the diagonal."""
+    P = eng._plan
+    sizes = np.array([len(P.batches[L.bra].pairs) * len(P.batches[L.ket].pairs) for L in P.launches],
+                     np.float64)
+    li = rng.choice(len(P.launches), size=n, p=sizes / sizes.sum())
+    out = np.empty((n, 3), np.int32)
+    for k, l in enumerate(li):
+        L = P.launches[l]
+        nb, nk = len(P.batches[L.bra].pairs), len(P.batches[L.ket].pairs)
+        ib, ik = int(rng.integers(nb)), int(rng.integers(nk))
+        if L.bra == L.ket and ik < ib:
+            ib, ik = ik, ib
+        out[k] = (l, ib, ik)
+    return out
+
+
+def features(eng: FockEngine, D, samples: np.ndarray):
+    """Device features (n x 12) and six-block bounds of sampled quartets."""
+    import torch
+    n = len(samples)
+    Dt = torch.as_tensor(np.ascontiguousarray(D, np.float64), device=f"cuda:{eng.device}")
+    F = torch.empty((max(n, 1), N_FEAT), dtype=torch.float32, device=Dt.device)
+    B = torch.empty(max(n, 1), dtype=torch.float64, device=Dt.device)
+    s = np.ascontiguousarray(samples, np.int32)
+    _lib.check(eng._L.fjb_router_features(eng._h, Dt.data_ptr(), s.ctypes.data, n, F.data_ptr(),
+                                          B.data_ptr()), eng._h)
+    return F[:n].cpu().numpy(), B[:n].cpu().numpy()
+
+
+def training_set(workloads, n_per: int = 20000, seed: int = 0, zero_gap: float = -6.0):
+    """(X, y): features and log10(max|(ab|cd)| x dmax) of sampled computed
+    quartets of each workload, the targets from the FP64 HGP tap.
+
+    Quartets more than 10^-zero_gap below their Schwarz x density bound are
+    left out: they vanish by symmetry (one-centre quartets of odd total
+    angular momentum), and what decides their FP32 error is the size of
+    their intermediates, which is that of their even siblings, not their
+    zero value.  Without them the network treats such quartets like those
+    siblings, the conservative side."""
+    rng = np.random.default_rng(seed)
+    Xs, ys = [], []
+    for w in workloads:
+        eng = FockEngine(w.basis, tuned=False)
+        P = eng.plan(w.D, w.tau, w.n_mag)
+        s = sample_launched(eng, n_per, rng)
+        X, b = features(eng, w.D, s)
+        keep = b >= w.tau  # computed (not screened) quartets only
+        s, X = s[keep], X[keep]
+        quartets = []
+        for l, ib, ik in s:
+            L = P.launches[l]
+            pb, pk = P.batches[L.bra].pairs[ib], P.batches[L.ket].pairs[ik]
+            quartets.append((pb.a, pb.b, pk.a, pk.b))
+        blocks = eng.eri_blocks(quartets)
+        mx = np.array([np.abs(blk).max() for blk in blocks])
+        y = np.log10(np.maximum(mx, 1e-300)) + X[:, 11]  # + log10 dmax
+        keep = y - bound_log10(X) > zero_gap
+        Xs.append(X[keep])
+        ys.append(y[keep].astype(np.float32))
+        eng.close()
+    return np.concatenate(Xs), np.concatenate(ys)
+
+
+def calibrate(mlp: MLP, X, y, quantile: float = 0.999) -> float:
+    """The margin: the `quantile` of the residuals y - y_pred (log10 units)."""
+    r = y - mlp.predict(X).cpu().numpy()
+    return float(np.quantile(r, quantile))
+
+
+def install(eng: FockEngine, mlp: MLP, *, threshold: float = 1e-9, margin: float = 0.0) -> None:
+    p = np.ascontiguousarray(mlp.params(), np.float32)
+    _lib.check(eng._L.fjb_router_set(eng._h, p.ctypes.data,
+                                     C.c_float(math.log10(threshold) - margin)), eng._h)
+
+
+def uninstall(eng: FockEngine) -> None:
+    _lib.check(eng._L.fjb_router_set(eng._h, None, C.c_float(0.0)), eng._h)
+
+
+def route_stats(eng: FockEngine) -> tuple[int, int]:
+    a, b = C.c_int64(), C.c_int64()
+    _lib.check(eng._L.fjb_route_stats(eng._h, C.byref(a), C.byref(b)), eng._h)
+    return int(a.value), int(b.value)
+
+
+def validate(eng: FockEngine, D, *, threshold: float = 1e-9, budget: float = 1e-8) -> dict:
+    """Build G routed (learned router installed) and in FP64; if max|dG|
+    breaks the budget, turn the learned router off (the FP64-side fallback)
+    and say so."""
+    G64 = eng.build(D, precision=_lib.FJB_FP64)[2].clone()
+    Gr = eng.build(D, precision=_lib.FJB_ROUTED, threshold=threshold)[2]
+    d = float((Gr - G64).abs().max())
+    ok = d <= budget
+    if not ok:
+        uninstall(eng)
+    return {"max_abs_dG": d, "within_budget": ok}

@@ -176,6 +176,35 @@ int fjb_create_df(fjb_handle **out, const fjb_basis *ao, const fjb_basis *aux, i
 int fjb_df_blocks(fjb_handle *h, int kind, const int32_t *items, int n, double *out_dev,
                   int64_t *offsets);
 
+/* The learned precision router (no counterpart in the reference; its
+ * fmixed lever, eri/fock/levers/mixed.py, is the FP32 path it routes to).
+ * A 12 -> 64 -> 64 -> 1 tanh MLP predicts log10 of a quartet's largest
+ * deposit from pair features; in FJB_ROUTED builds a unit whose every
+ * computed quartet is under the rigorous bound (threshold), or predicted
+ * under 10^log10_threshold, runs its recurrences in FP32.  Skipping stays
+ * the six-block screen's.  fjb_mlp_n_params() floats, packed
+ * mu[12] sd[12] W1[64][12] b1[64] W2[64][64] b2[64] w3[64] b3.
+ * params_host NULL turns the learned router off. */
+int fjb_mlp_n_params(void);
+int fjb_router_set(fjb_handle *h, const float *params_host, float log10_threshold);
+/* Features (n x 12 floats) and six-block bounds (n doubles) of sampled
+ * launched quartets, samples[3i..3i+2] = (launch, bra index, ket index) in
+ * the plan's order (HOST); feat_dev, bound_dev DEVICE.  Synchronises. */
+int fjb_router_features(fjb_handle *h, const double *D_dev, const int32_t *samples, int n, float *feat_dev,
+                        double *bound_dev);
+/* Training and inference kernels (DEVICE pointers, FP32): the forward pass;
+ * the mean-squared-error gradient of a batch (scratch_dev holds n x 257
+ * floats, sq_err_dev n floats); one Adam step (step counts from 1). */
+int fjb_mlp_forward(const float *params_dev, const float *X_dev, int n, float *Y_dev, void *stream);
+int fjb_mlp_gradient(const float *params_dev, const float *X_dev, const float *T_dev, int n, float *grad_dev,
+                     float *sq_err_dev, float *scratch_dev, void *stream);
+int fjb_mlp_adam(float *params_dev, const float *grad_dev, float *m_dev, float *v_dev, float lr, int step,
+                 void *stream);
+/* Work units the last routed build sent to the FP32 and FP64 queues (units
+ * of classes without an FP32 body, and of FP64 builds, count as FP64).
+ * Synchronises on the last build. */
+int fjb_route_stats(const fjb_handle *h, int64_t *units_fp32, int64_t *units_fp64);
+
 /* Device Boys F_0..F_m(T[i]) for n arguments into F_dev[i*(m+1) + k]
  * (DEVICE pointers).  Synchronises. */
 int fjb_boys(int m, const double *T_dev, int n, double *F_dev);
