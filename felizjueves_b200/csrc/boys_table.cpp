@@ -7,7 +7,11 @@
 // falls below 1e-22 of the sum, then rounded once to double.  The device
 // evaluates F_M(T) = sum_{k<7} F_{M+k}(T_i) (T_i - T)^k / k! at the nearest
 // node (|T_i - T| <= kBoysDelta/2 = 0.025, so the truncation is below
-// 0.025^7/7! = 1.2e-15 relative) and recurs downward for m < M.
+// 0.025^7/7! = 1.2e-15 relative) and recurs downward for m < M.  The last
+// entry of each row is exp(-T_i), from which the device takes
+// exp(-T) = exp(-T_i) exp(T_i - T) with an 8-term Taylor polynomial of the
+// second factor (truncation below 0.025^9/9! = 1e-20 relative): the downward
+// recursion's exp costs no call.
 #include <cmath>
 #include <vector>
 
@@ -16,7 +20,7 @@
 namespace fjb {
 
 std::vector<double> boys_table() {
-    std::vector<double> tab((size_t)kBoysNT * (kBoysMaxM + 1));
+    std::vector<double> tab((size_t)kBoysNT * kBoysRow);
     for (int i = 0; i < kBoysNT; ++i) {
         long double T = (long double)((double)i * kBoysDelta);  // the node the device uses
         long double ex = expl(-T);
@@ -27,8 +31,9 @@ std::vector<double> boys_table() {
                 sum += term;
                 if (term < 1e-22L * sum) break;
             }
-            tab[(size_t)i * (kBoysMaxM + 1) + m] = (double)(ex * sum);
+            tab[(size_t)i * kBoysRow + m] = (double)(ex * sum);
         }
+        tab[(size_t)i * kBoysRow + kBoysMaxM + 1] = (double)ex;
     }
     return tab;
 }

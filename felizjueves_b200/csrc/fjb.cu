@@ -191,12 +191,23 @@ __global__ void router_features_kernel(const int32_t *samples, int n, const Laun
 
 // The HGP Fock kernel (file header of fock_kernels.cuh).  All floating-point
 // work is FP64.
+//
+// One CTA per work unit.  The unit's ket pairs are first screened and
+// compacted (warp 0, one lane per ket); the computed kets are then taken in
+// groups of G = min(C.group, slots / K) (K = the unit's primitive quartets
+// per contracted quartet): the VRR runs over every (ket, primitive quartet)
+// of a group at once, slot s of a chunk being flat index c0 + s = g K + t,
+// so each level's barrier covers G quartets' work; each ket's boundary is
+// kept apart (bound[g]), then the HRR and the digest run ket by ket.  With
+// one slot the registers-held single-slot path runs instead.
 template <int NT>
 __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
     extern __shared__ __align__(16) double sm[];
+    __shared__ int s_list[kKetChunk];
+    __shared__ int s_n;
     const ClassDev &C = A.C;
     double *V = sm + C.sm_V;
-    double *bound = sm + C.sm_bound;
+    double *bound_all = sm + C.sm_bound;
     double *S = sm + C.sm_S;
     double *braP = sm + C.sm_braP;
     double *ketP = sm + C.sm_ketP;
@@ -213,6 +224,7 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
     const int slots = C.slots;
     const int na = C.na, nb = C.nb, nc = C.nc, nd = C.nd, nab = C.nab, ncd = C.ncd;
     const int nbe = C.nbe, nbf = C.nbf, L = C.L, n_ao = A.n_ao;
+    const int nbnd = nbe * nbf;
     const bool tap = A.tap_out != nullptr;
 
     const int n_todo = A.unit_list ? *A.unit_count : A.n_units;
@@ -224,7 +236,7 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
         const int kab = bra.nprim;
         {
             const double *src = reinterpret_cast<const double *>(A.prims + bra.prim0);
-            for (int i = tid; i < kab * 8; i += nt) braP[i] = src[i];
+            for (int i = tid; i < kab * kPrimWords; i += nt) braP[i] = src[i];
         }
         for (int i = tid; i < C.n_cb; i += nt) {
             const HCoef h = C.cb[i];
@@ -236,66 +248,72 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                 Dab[i] = A.D[(size_t)(bra.ao_a + i / nb) * n_ao + bra.ao_b + i % nb];
                 Jab[i] = 0.0;
             }
+        // the unit's computed kets, in ket order (units hold <= 32 kets)
+        if (tid < 32) {
+            const int ik = U.k0 + tid;
+            bool on = false;
+            if (ik < U.k1) {
+                if (tap) {
+                    on = true;
+                } else {
+                    const PairRec ket = A.pairs[LR.ket_pair0 + ik];
+                    on = !skip6(A.Dsh, A.n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G, A.tau);
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, on);
+            if (on) s_list[__popc(m & ((1u << tid) - 1u))] = ik;
+            if (tid == 0) s_n = __popc(m);
+        }
         __syncthreads();
-        int n_computed = 0;
-        for (int ik = U.k0; ik < U.k1; ++ik) {
-            const PairRec ket = A.pairs[LR.ket_pair0 + ik];
-            if (!tap && skip6(A.Dsh, A.n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G, A.tau))
-                continue;
-            ++n_computed;
-            const double deg = (bra.a == bra.b ? 0.5 : 1.0) * (ket.a == ket.b ? 0.5 : 1.0) *
-                               ((LR.diag && ik == U.ib) ? 0.5 : 1.0);
-            const int kcd = ket.nprim;
-            {
-                const double *src = reinterpret_cast<const double *>(A.prims + ket.prim0);
-                for (int i = tid; i < kcd * 8; i += nt) ketP[i] = src[i];
+        const int n_list = s_n;
+        const int kcd = A.pairs[LR.ket_pair0 + U.k0].nprim;  // a ket batch has one degree
+        const int K = kab * kcd;
+        const int G = slots == 1 ? 1 : max(1, min(C.group, slots / K));
+
+        for (int g0 = 0; g0 < n_list; g0 += G) {
+            const int ng = min(G, n_list - g0);
+            for (int i = tid; i < ng * kcd * kPrimWords; i += nt) {
+                const int g = i / (kcd * kPrimWords), r = i - g * (kcd * kPrimWords);
+                const PairRec ket = A.pairs[LR.ket_pair0 + s_list[g0 + g]];
+                ketP[i] = reinterpret_cast<const double *>(A.prims + ket.prim0)[r];
             }
-            for (int i = tid; i < C.n_ck; i += nt) {
-                const HCoef h = C.ck[i];
-                ck[i] = (double)h.binom * ipow(ket.AB[0], h.px) * ipow(ket.AB[1], h.py) *
-                        ipow(ket.AB[2], h.pz);
-            }
-            if (!tap) {
-                const int oa = bra.ao_a, ob = bra.ao_b, oc = ket.ao_a, od = ket.ao_b;
-                for (int i = tid; i < ncd; i += nt)
-                    Dcd[i] = A.D[(size_t)(oc + i / nd) * n_ao + od + i % nd];
-                for (int i = tid; i < na * nc; i += nt)
-                    Dac[i] = A.D[(size_t)(oa + i / nc) * n_ao + oc + i % nc];
-                for (int i = tid; i < na * nd; i += nt)
-                    Dad[i] = A.D[(size_t)(oa + i / nd) * n_ao + od + i % nd];
-                for (int i = tid; i < nb * nc; i += nt)
-                    Dbc[i] = A.D[(size_t)(ob + i / nc) * n_ao + oc + i % nc];
-                for (int i = tid; i < nb * nd; i += nt)
-                    Dbd[i] = A.D[(size_t)(ob + i / nd) * n_ao + od + i % nd];
-            }
-            for (int i = tid; i < nbe * nbf; i += nt) bound[i] = 0.0;
+            for (int i = tid; i < ng * nbnd; i += nt) bound_all[i] = 0.0;
             __syncthreads();
 
-            const int K = kab * kcd;
             if (slots == 1) {
-                // One primitive quartet at a time: every thread holds its
-                // scalars in registers; one thread evaluates the Boys leaves.
+                // One primitive quartet at a time (ng == 1): every thread
+                // holds its scalars in registers; the Boys leaves of all K
+                // primitive quartets are evaluated first, one thread each.
+                double *Fq = sm + C.sm_F;
+                for (int t = tid; t < K; t += nt) {
+                    const int ikcd = t / kab, ikab = t - ikcd * kab;
+                    const double *pb = braP + kPrimWords * ikab, *pk = ketP + kPrimWords * ikcd;
+                    const double p = pb[6], q = pk[6];
+                    const double rho = p * q * (1.0 / (p + q));
+                    const double PQx = pb[0] - pk[0], PQy = pb[1] - pk[1], PQz = pb[2] - pk[2];
+                    const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+                    double F[kMaxLQuartet + 1];
+                    boys_eval(L, T, F, A.boys_tab);
+                    const double seed = pb[7] * pk[7] * kTwoOverSqrtPi * sqrt(rho);
+                    for (int m = 0; m <= L; ++m) Fq[t * (L + 1) + m] = seed * F[m];
+                }
+                __syncthreads();
                 for (int t = 0; t < K; ++t) {
                     const int ikcd = t / kab, ikab = t - ikcd * kab;
-                    const double *pb = braP + 8 * ikab, *pk = ketP + 8 * ikcd;
+                    const double *pb = braP + kPrimWords * ikab, *pk = ketP + kPrimWords * ikcd;
                     const double p = pb[6], q = pk[6];
                     const double ppq = p + q, inv = 1.0 / ppq, rho = p * q * inv;
                     const double PQx = pb[0] - pk[0], PQy = pb[1] - pk[1], PQz = pb[2] - pk[2];
                     const double wp = -q * inv, wq = p * inv;
-                    const double i2p = 0.5 / p, i2q = 0.5 / q;
-                    const double rp = i2p * rho / p, rq = i2q * rho / q, e2 = 0.5 * inv;
+                    const double i2p = pb[8], i2q = pk[8];
+                    const double rp = i2p * (q * inv), rq = i2q * (p * inv), e2 = 0.5 * inv;
                     const double pa0 = pb[3], pa1 = pb[4], pa2 = pb[5];
                     const double qc0 = pk[3], qc1 = pk[4], qc2 = pk[5];
                     const double wp0 = wp * PQx, wp1 = wp * PQy, wp2 = wp * PQz;
                     const double wq0 = wq * PQx, wq1 = wq * PQy, wq2 = wq * PQz;
-                    if (tid == 0) {
-                        const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-                        double F[kMaxLQuartet + 1];
-                        boys_eval(L, T, F, A.boys_tab);
-                        const double seed = pb[7] * pk[7] * kTwoOverSqrtPi * sqrt(rho);
-                        V[0] = 0.0;
-                        for (int m = 0; m <= L; ++m) V[__ldg(C.leaf + m)] = seed * F[m];
-                    }
+                    (void)rho;
+                    if (tid == 0) V[0] = 0.0;
+                    if (tid <= L) V[__ldg(C.leaf + tid)] = Fq[t * (L + 1) + tid];
                     __syncthreads();
                     for (int lv = 0; lv < C.n_levels; ++lv) {
                         const int o0 = __ldg(C.level_off + lv), o1 = __ldg(C.level_off + lv + 1);
@@ -323,157 +341,191 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                         }
                         __syncthreads();
                     }
-                    for (int i = tid; i < nbe * nbf; i += nt) bound[i] += V[__ldg(C.tgt + i)];
+                    for (int i = tid; i < nbnd; i += nt) bound_all[i] += V[__ldg(C.tgt + i)];
                     __syncthreads();
                 }
-            }
-            for (int c0 = 0; slots > 1 && c0 < K; c0 += slots) {
-                const int ns = min(slots, K - c0);
-                for (int s = tid; s < ns; s += nt) {
-                    const int t = c0 + s, ikcd = t / kab, ikab = t - ikcd * kab;
-                    const double *pb = braP + 8 * ikab, *pk = ketP + 8 * ikcd;
-                    const double p = pb[6], q = pk[6];
-                    const double ppq = p + q, inv = 1.0 / ppq, rho = p * q * inv;
-                    const double PQx = pb[0] - pk[0], PQy = pb[1] - pk[1], PQz = pb[2] - pk[2];
-                    const double wp = -q * inv, wq = p * inv;
-                    const double inv2p = 0.5 / p, inv2q = 0.5 / q;
-                    double *Ss = S + s;
-                    Ss[0 * slots] = pb[3];
-                    Ss[1 * slots] = pb[4];
-                    Ss[2 * slots] = pb[5];
-                    Ss[3 * slots] = wp * PQx;
-                    Ss[4 * slots] = wp * PQy;
-                    Ss[5 * slots] = wp * PQz;
-                    Ss[6 * slots] = inv2p;
-                    Ss[7 * slots] = inv2p * rho / p;
-                    Ss[8 * slots] = pk[3];
-                    Ss[9 * slots] = pk[4];
-                    Ss[10 * slots] = pk[5];
-                    Ss[11 * slots] = wq * PQx;
-                    Ss[12 * slots] = wq * PQy;
-                    Ss[13 * slots] = wq * PQz;
-                    Ss[14 * slots] = inv2q;
-                    Ss[15 * slots] = inv2q * rho / q;
-                    Ss[16 * slots] = 0.5 * inv;
-                    const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-                    double F[kMaxLQuartet + 1];
-                    boys_eval(L, T, F, A.boys_tab);
-                    const double seed = pb[7] * pk[7] * kTwoOverSqrtPi * sqrt(rho);
-                    V[s] = 0.0;
-                    for (int m = 0; m <= L; ++m) V[(size_t)__ldg(C.leaf + m) * slots + s] = seed * F[m];
-                }
-                __syncthreads();
-                for (int lv = 0; lv < C.n_levels; ++lv) {
-                    const int o0 = __ldg(C.level_off + lv), o1 = __ldg(C.level_off + lv + 1);
-                    const int items = (o1 - o0) * ns;
-                    for (int it = tid; it < items; it += nt) {
-                        const int oi = o0 + it / ns, s = it - (it / ns) * ns;
-                        const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(C.ops) + oi);
-                        VOp op;
-                        memcpy(&op, &raw, sizeof(op));
-                        const double *Ss = S + s;
-                        const int base = op.kind * 8;
-                        const double a = Ss[(base + op.d) * slots];
-                        const double b = Ss[(base + 3 + op.d) * slots];
-                        const double c = Ss[(base + 6) * slots];
-                        const double dd = Ss[(base + 7) * slots];
-                        const double e = Ss[16 * slots];
-                        double v = a * V[(size_t)op.s0 * slots + s] + b * V[(size_t)op.s1 * slots + s];
-                        v += (double)op.c2 * (c * V[(size_t)op.s2 * slots + s] - dd * V[(size_t)op.s3 * slots + s]);
-                        v += (double)op.c4 * e * V[(size_t)op.s4 * slots + s];
-                        V[(size_t)op.dst * slots + s] = v;
+            } else {
+                const int total = ng * K;
+                for (int c0 = 0; c0 < total; c0 += slots) {
+                    const int ns = min(slots, total - c0);
+                    for (int s = tid; s < ns; s += nt) {
+                        const int fl = c0 + s, g = fl / K, t = fl - g * K;
+                        const int ikcd = t / kab, ikab = t - ikcd * kab;
+                        const double *pb = braP + kPrimWords * ikab, *pk = ketP + kPrimWords * (g * kcd + ikcd);
+                        const double p = pb[6], q = pk[6];
+                        const double ppq = p + q, inv = 1.0 / ppq, rho = p * q * inv;
+                        const double PQx = pb[0] - pk[0], PQy = pb[1] - pk[1], PQz = pb[2] - pk[2];
+                        const double wp = -q * inv, wq = p * inv;
+                        const double inv2p = pb[8], inv2q = pk[8];
+                        double *Ss = S + s;
+                        Ss[0 * slots] = pb[3];
+                        Ss[1 * slots] = pb[4];
+                        Ss[2 * slots] = pb[5];
+                        Ss[3 * slots] = wp * PQx;
+                        Ss[4 * slots] = wp * PQy;
+                        Ss[5 * slots] = wp * PQz;
+                        Ss[6 * slots] = inv2p;
+                        Ss[7 * slots] = inv2p * (q * inv);
+                        Ss[8 * slots] = pk[3];
+                        Ss[9 * slots] = pk[4];
+                        Ss[10 * slots] = pk[5];
+                        Ss[11 * slots] = wq * PQx;
+                        Ss[12 * slots] = wq * PQy;
+                        Ss[13 * slots] = wq * PQz;
+                        Ss[14 * slots] = inv2q;
+                        Ss[15 * slots] = inv2q * (p * inv);
+                        Ss[16 * slots] = 0.5 * inv;
+                        const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+                        double F[kMaxLQuartet + 1];
+                        boys_eval(L, T, F, A.boys_tab);
+                        const double seed = pb[7] * pk[7] * kTwoOverSqrtPi * sqrt(rho);
+                        V[s] = 0.0;
+                        for (int m = 0; m <= L; ++m) V[(size_t)__ldg(C.leaf + m) * slots + s] = seed * F[m];
+                    }
+                    __syncthreads();
+                    for (int lv = 0; lv < C.n_levels; ++lv) {
+                        const int o0 = __ldg(C.level_off + lv), o1 = __ldg(C.level_off + lv + 1);
+                        const int items = (o1 - o0) * ns;
+                        for (int it = tid; it < items; it += nt) {
+                            const int oi = o0 + it / ns, s = it - (it / ns) * ns;
+                            const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(C.ops) + oi);
+                            VOp op;
+                            memcpy(&op, &raw, sizeof(op));
+                            const double *Ss = S + s;
+                            const int base = op.kind * 8;
+                            const double a = Ss[(base + op.d) * slots];
+                            const double b = Ss[(base + 3 + op.d) * slots];
+                            const double c = Ss[(base + 6) * slots];
+                            const double dd = Ss[(base + 7) * slots];
+                            const double e = Ss[16 * slots];
+                            double v = a * V[(size_t)op.s0 * slots + s] + b * V[(size_t)op.s1 * slots + s];
+                            v += (double)op.c2 * (c * V[(size_t)op.s2 * slots + s] - dd * V[(size_t)op.s3 * slots + s]);
+                            v += (double)op.c4 * e * V[(size_t)op.s4 * slots + s];
+                            V[(size_t)op.dst * slots + s] = v;
+                        }
+                        __syncthreads();
+                    }
+                    // each ket's share of this chunk into its boundary
+                    const int glo = c0 / K, ghi = (c0 + ns - 1) / K;
+                    for (int it = tid; it < (ghi - glo + 1) * nbnd; it += nt) {
+                        const int g = glo + it / nbnd, t = it - (it / nbnd) * nbnd;
+                        const int s0 = max(c0, g * K) - c0, s1 = min(c0 + ns, (g + 1) * K) - c0;
+                        const size_t node = __ldg(C.tgt + t);
+                        double acc = 0.0;
+                        for (int s = s0; s < s1; ++s) acc += V[node * slots + s];
+                        bound_all[(size_t)g * nbnd + t] += acc;
                     }
                     __syncthreads();
                 }
-                for (int t = tid; t < nbe * nbf; t += nt) {
-                    const size_t node = __ldg(C.tgt + t);
+            }
+
+            for (int g = 0; g < ng; ++g) {
+                const int ik = s_list[g0 + g];
+                const PairRec ket = A.pairs[LR.ket_pair0 + ik];
+                const double *bound = bound_all + (size_t)g * nbnd;
+                const double deg = (bra.a == bra.b ? 0.5 : 1.0) * (ket.a == ket.b ? 0.5 : 1.0) *
+                                   ((LR.diag && ik == U.ib) ? 0.5 : 1.0);
+                // HRR, bra side: X[ab][f] = sum_k coefB(b,k) (a+k, 0 | f);
+                // alongside, the ket's HRR coefficients and density blocks
+                double *X = V, *Y = V + (size_t)nab * nbf;
+                for (int i = tid; i < nab * nbf; i += nt) {
+                    const int ab = i / nbf, jf = i - ab * nbf;
+                    const int t0 = __ldg(C.bra_off + ab), t1 = __ldg(C.bra_off + ab + 1);
                     double acc = 0.0;
-                    for (int s = 0; s < ns; ++s) acc += V[node * slots + s];
-                    bound[t] += acc;
+                    for (int t = t0; t < t1; ++t) {
+                        const HTerm h = C.bra_terms[t];
+                        acc += cb[h.cidx] * bound[h.src * nbf + jf];
+                    }
+                    X[i] = acc;
+                }
+                for (int i = tid; i < C.n_ck; i += nt) {
+                    const HCoef h = C.ck[i];
+                    ck[i] = (double)h.binom * ipow(ket.AB[0], h.px) * ipow(ket.AB[1], h.py) *
+                            ipow(ket.AB[2], h.pz);
+                }
+                if (!tap) {
+                    const int oa = bra.ao_a, ob = bra.ao_b, oc = ket.ao_a, od = ket.ao_b;
+                    for (int i = tid; i < ncd; i += nt)
+                        Dcd[i] = A.D[(size_t)(oc + i / nd) * n_ao + od + i % nd];
+                    for (int i = tid; i < na * nc; i += nt)
+                        Dac[i] = A.D[(size_t)(oa + i / nc) * n_ao + oc + i % nc];
+                    for (int i = tid; i < na * nd; i += nt)
+                        Dad[i] = A.D[(size_t)(oa + i / nd) * n_ao + od + i % nd];
+                    for (int i = tid; i < nb * nc; i += nt)
+                        Dbc[i] = A.D[(size_t)(ob + i / nc) * n_ao + oc + i % nc];
+                    for (int i = tid; i < nb * nd; i += nt)
+                        Dbd[i] = A.D[(size_t)(ob + i / nd) * n_ao + od + i % nd];
                 }
                 __syncthreads();
-            }
-            // HRR, bra side: X[ab][f] = sum_k coefB(b,k) (a+k, 0 | f)
-            double *X = V, *Y = V + (size_t)nab * nbf;
-            for (int i = tid; i < nab * nbf; i += nt) {
-                const int ab = i / nbf, jf = i - ab * nbf;
-                const int t0 = __ldg(C.bra_off + ab), t1 = __ldg(C.bra_off + ab + 1);
-                double acc = 0.0;
-                for (int t = t0; t < t1; ++t) {
-                    const HTerm h = C.bra_terms[t];
-                    acc += cb[h.cidx] * bound[h.src * nbf + jf];
-                }
-                X[i] = acc;
-            }
-            __syncthreads();
-            // HRR, ket side: Y[ab][cd] = sum_k coefK(d,k) X[ab][c+k]
-            for (int i = tid; i < nab * ncd; i += nt) {
-                const int ab = i / ncd, cd = i - ab * ncd;
-                const int t0 = __ldg(C.ket_off + cd), t1 = __ldg(C.ket_off + cd + 1);
-                double acc = 0.0;
-                for (int t = t0; t < t1; ++t) {
-                    const HTerm h = C.ket_terms[t];
-                    acc += ck[h.cidx] * X[ab * nbf + h.src];
-                }
-                Y[i] = acc;
-            }
-            __syncthreads();
-            if (tap) {
-                double *out = A.tap_out + A.tap_off[u];
-                for (int i = tid; i < nab * ncd; i += nt) out[i] = Y[i];
-                __syncthreads();
-                continue;
-            }
-            // the six-block digest
-            {
-                const int oa = bra.ao_a, ob = bra.ao_b, oc = ket.ao_a, od = ket.ao_b;
-                const int n1 = nab, n2 = n1 + ncd, n3 = n2 + na * nc, n4 = n3 + na * nd,
-                          n5 = n4 + nb * nc, n6 = n5 + nb * nd;
-                const double w2 = 2.0 * deg;
-                for (int o = tid; o < n6; o += nt) {
+                // HRR, ket side: Y[ab][cd] = sum_k coefK(d,k) X[ab][c+k]
+                for (int i = tid; i < nab * ncd; i += nt) {
+                    const int ab = i / ncd, cd = i - ab * ncd;
+                    const int t0 = __ldg(C.ket_off + cd), t1 = __ldg(C.ket_off + cd + 1);
                     double acc = 0.0;
-                    if (o < n1) {
-                        const double *y = Y + (size_t)o * ncd;
-                        for (int kl = 0; kl < ncd; ++kl) acc += Dcd[kl] * y[kl];
-                        Jab[o] += w2 * acc;
-                    } else if (o < n2) {
-                        const int kl = o - n1;
-                        for (int ij = 0; ij < nab; ++ij) acc += Dab[ij] * Y[(size_t)ij * ncd + kl];
-                        atomicAdd(A.Jp + (size_t)(oc + kl / nd) * n_ao + od + kl % nd, w2 * acc);
-                    } else if (o < n3) {
-                        const int r = o - n2, i = r / nc, k = r % nc;
-                        for (int j = 0; j < nb; ++j)
-                            for (int l = 0; l < nd; ++l)
-                                acc += Dbd[j * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                        atomicAdd(A.Kp + (size_t)(oa + i) * n_ao + oc + k, deg * acc);
-                    } else if (o < n4) {
-                        const int r = o - n3, i = r / nd, l = r % nd;
-                        for (int j = 0; j < nb; ++j)
-                            for (int k = 0; k < nc; ++k)
-                                acc += Dbc[j * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                        atomicAdd(A.Kp + (size_t)(oa + i) * n_ao + od + l, deg * acc);
-                    } else if (o < n5) {
-                        const int r = o - n4, j = r / nc, k = r % nc;
-                        for (int i = 0; i < na; ++i)
-                            for (int l = 0; l < nd; ++l)
-                                acc += Dad[i * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                        atomicAdd(A.Kp + (size_t)(ob + j) * n_ao + oc + k, deg * acc);
-                    } else {
-                        const int r = o - n5, j = r / nd, l = r % nd;
-                        for (int i = 0; i < na; ++i)
-                            for (int k = 0; k < nc; ++k)
-                                acc += Dac[i * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                        atomicAdd(A.Kp + (size_t)(ob + j) * n_ao + od + l, deg * acc);
+                    for (int t = t0; t < t1; ++t) {
+                        const HTerm h = C.ket_terms[t];
+                        acc += ck[h.cidx] * X[ab * nbf + h.src];
+                    }
+                    Y[i] = acc;
+                }
+                __syncthreads();
+                if (tap) {
+                    double *out = A.tap_out + A.tap_off[u] + (size_t)(ik - U.k0) * nab * ncd;
+                    for (int i = tid; i < nab * ncd; i += nt) out[i] = Y[i];
+                    __syncthreads();
+                    continue;
+                }
+                // the six-block digest
+                {
+                    const int oa = bra.ao_a, ob = bra.ao_b, oc = ket.ao_a, od = ket.ao_b;
+                    const int n1 = nab, n2 = n1 + ncd, n3 = n2 + na * nc, n4 = n3 + na * nd,
+                              n5 = n4 + nb * nc, n6 = n5 + nb * nd;
+                    const double w2 = 2.0 * deg;
+                    for (int o = tid; o < n6; o += nt) {
+                        double acc = 0.0;
+                        if (o < n1) {
+                            const double *y = Y + (size_t)o * ncd;
+                            for (int kl = 0; kl < ncd; ++kl) acc += Dcd[kl] * y[kl];
+                            Jab[o] += w2 * acc;
+                        } else if (o < n2) {
+                            const int kl = o - n1;
+                            for (int ij = 0; ij < nab; ++ij) acc += Dab[ij] * Y[(size_t)ij * ncd + kl];
+                            atomicAdd(A.Jp + (size_t)(oc + kl / nd) * n_ao + od + kl % nd, w2 * acc);
+                        } else if (o < n3) {
+                            const int r = o - n2, i = r / nc, k = r % nc;
+                            for (int j = 0; j < nb; ++j)
+                                for (int l = 0; l < nd; ++l)
+                                    acc += Dbd[j * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                            atomicAdd(A.Kp + (size_t)(oa + i) * n_ao + oc + k, deg * acc);
+                        } else if (o < n4) {
+                            const int r = o - n3, i = r / nd, l = r % nd;
+                            for (int j = 0; j < nb; ++j)
+                                for (int k = 0; k < nc; ++k)
+                                    acc += Dbc[j * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                            atomicAdd(A.Kp + (size_t)(oa + i) * n_ao + od + l, deg * acc);
+                        } else if (o < n5) {
+                            const int r = o - n4, j = r / nc, k = r % nc;
+                            for (int i = 0; i < na; ++i)
+                                for (int l = 0; l < nd; ++l)
+                                    acc += Dad[i * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                            atomicAdd(A.Kp + (size_t)(ob + j) * n_ao + oc + k, deg * acc);
+                        } else {
+                            const int r = o - n5, j = r / nd, l = r % nd;
+                            for (int i = 0; i < na; ++i)
+                                for (int k = 0; k < nc; ++k)
+                                    acc += Dac[i * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                            atomicAdd(A.Kp + (size_t)(ob + j) * n_ao + od + l, deg * acc);
+                        }
                     }
                 }
+                __syncthreads();
             }
-            __syncthreads();
         }
         if (!tap)
             for (int i = tid; i < nab; i += nt)
                 atomicAdd(A.Jp + (size_t)(bra.ao_a + i / nb) * n_ao + bra.ao_b + i % nb, Jab[i]);
-        if (A.computed && tid == 0 && n_computed)
-            atomicAdd(A.computed + U.launch, (unsigned long long)n_computed);
+        if (A.computed && tid == 0 && n_list)
+            atomicAdd(A.computed + U.launch, (unsigned long long)n_list);
         __syncthreads();
     }
 }
@@ -724,6 +776,8 @@ PrimRec prim_record(const HostShell &sa, const HostShell &sb, int k) {
     }
     r.zeta = p;
     r.U = sa.coefs[i] * sb.coefs[j] * std::pow(M_PI / p, 1.5) * std::exp(-x * y / p * ab2);
+    r.h = 0.5 / p;
+    r.pad = 0.0;
     return r;
 }
 
@@ -1147,10 +1201,16 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
     const bool routed = route > 0.0;
     h->last_routed = routed;
     if (routed) CUDA_OK(h, cudaMemsetAsync(h->route_counts.p, 0, h->route_counts.n * sizeof(int), st));
-    CUDA_OK(h, cudaEventRecord(h->ev0, st));
+    // Under stream capture the timing events become event-record nodes of
+    // the graph (External), so every replay records them and the class and
+    // build timings read after a replay are that replay's.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_OK(h, cudaStreamIsCapturing(st, &cap));
+    const unsigned ev_flags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
+    CUDA_OK(h, cudaEventRecordWithFlags(h->ev0, st, ev_flags));
     for (size_t ri = 0; ri < h->runs.size(); ++ri) {
         const ClassRun &r = h->runs[ri];
-        CUDA_OK(h, cudaEventRecord(h->cev[ri].first, st));
+        CUDA_OK(h, cudaEventRecordWithFlags(h->cev[ri].first, st, ev_flags));
         KArgs a{};
         a.computed = h->computed.p;
         a.C = r.dev;
@@ -1196,10 +1256,10 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
             CUDA_OK(h, launch_run(r, st, a));
             ++launches;
         }
-        CUDA_OK(h, cudaEventRecord(h->cev[ri].second, st));
+        CUDA_OK(h, cudaEventRecordWithFlags(h->cev[ri].second, st, ev_flags));
     }
     h->built = true;
-    CUDA_OK(h, cudaEventRecord(h->ev1, st));
+    CUDA_OK(h, cudaEventRecordWithFlags(h->ev1, st, ev_flags));
     close_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(h->Jp.p, h->Kp.p, nao, J_dev, K_dev, G_dev);
     ++launches;
     CUDA_OK(h, cudaGetLastError());

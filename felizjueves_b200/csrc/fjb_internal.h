@@ -12,6 +12,7 @@ constexpr int kBoysTaylor = 7;    // Taylor terms (orders m .. m+6)
 constexpr double kBoysDelta = 0.05;
 constexpr double kBoysTMax = 40.0;  // table covers [0, kBoysTMax]
 constexpr int kBoysNT = 801;        // kBoysTMax / kBoysDelta + 1
+constexpr int kBoysRow = kBoysMaxM + 2;  // F_0 .. F_kBoysMaxM, then exp(-T_i)
 constexpr int kThreads = 128;       // widest CTA of the HGP kernel's default choice
 constexpr int kMaxThreads = 512;    // widest CTA the kernel is instantiated for
 constexpr int kKetChunk = 32;       // ket pairs per work unit (one per lane of a warp)
@@ -40,10 +41,14 @@ struct HCoef {
 };
 
 // A primitive pair as staged for the kernels: P, X = P - A (first centre),
-// zeta, U = c_a c_b (pi/zeta)^{3/2} exp(-alpha beta/zeta |AB|^2).
+// zeta, U = c_a c_b (pi/zeta)^{3/2} exp(-alpha beta/zeta |AB|^2), and
+// h = 1/(2 zeta) (the VRR's e/(2 zeta) factor, so no primitive quartet
+// divides by zeta); 80 bytes.
 struct PrimRec {
-    double P[3], X[3], zeta, U;
+    double P[3], X[3], zeta, U, h, pad;
 };
+constexpr int kPrimWords = 10;  // doubles per PrimRec
+static_assert(sizeof(PrimRec) == kPrimWords * sizeof(double), "PrimRec is kPrimWords doubles");
 
 // A contracted shell pair (canonical: la <= lb, lower index first on a tie).
 struct PairRec {
@@ -74,11 +79,12 @@ struct ClassDev {
     int n_levels;
     int nbe, nbf;     // boundary extents (e with la<=|e|<=la+lb, f likewise)
     int n_cb, n_ck;   // HRR coefficient counts
-    int slots;        // primitive quartets per chunk
-    int threads;      // CTA width: 32, 64, 128 or 256
+    int slots;        // (ket, primitive quartet) slots per VRR chunk
+    int group;        // kets whose VRR runs together (at most kKetChunk)
+    int threads;      // CTA width: 32, 64, 128, 256 or 512
     const int *level_off;   // [n_levels + 1] into ops
     const VOp *ops;
-    const uint16_t *leaf;   // [L + 1] node of [0|0]^(m), 0 if unread
+    const uint16_t *leaf;   // [L + 1] node of [0|0]^(m), 1 (the scratch node) if unread
     const uint16_t *tgt;    // [nbe * nbf] node of boundary (e, f)
     const HCoef *cb;        // [n_cb]
     const int *bra_off;     // [nab + 1]
@@ -87,7 +93,7 @@ struct ClassDev {
     const int *ket_off;     // [ncd + 1]
     const HTerm *ket_terms;
     // shared-memory carve-up, in doubles
-    int sm_V, sm_bound, sm_S, sm_braP, sm_ketP, sm_cb, sm_ck, sm_D, sm_Jab;
+    int sm_V, sm_bound, sm_S, sm_braP, sm_ketP, sm_cb, sm_ck, sm_D, sm_Jab, sm_F;
     int sm_total;
     int vregion;      // doubles in the V region (also holds X and Y)
 };

@@ -47,7 +47,8 @@ __device__ __forceinline__ void boys_t(double T, double *F, const double *__rest
     if (T < kBoysTMax) {
         const int i = __double2int_rn(T * (1.0 / kBoysDelta));
         const double d = (double)i * kBoysDelta - T;
-        const double *row = tab + (size_t)i * (kBoysMaxM + 1) + M;
+        const double *row0 = tab + (size_t)i * kBoysRow;
+        const double *row = row0 + M;
         double f = __ldg(row + 6);
         f = __ldg(row + 5) + f * d * (1.0 / 6.0);
         f = __ldg(row + 4) + f * d * (1.0 / 5.0);
@@ -57,7 +58,7 @@ __device__ __forceinline__ void boys_t(double T, double *F, const double *__rest
         f = __ldg(row + 0) + f * d;
         F[M] = f;
         if (M > 0) {
-            const double e = exp(-T), t2 = 2.0 * T;
+            const double e = boys_exp(row0, d), t2 = 2.0 * T;
 #pragma unroll
             for (int m = M - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0 / (double)(2 * m + 1));
         }
@@ -103,8 +104,8 @@ __device__ __forceinline__ void quartet_compiled(const KArgs &A, const PairRec &
             for (int m = 0; m <= L; ++m) Fs[m] = (R)(seed * F[m]);
             VrrK<R> k;
             const double wp = -q * inv, wq = p * inv;
-            const double i2p = 0.5 / p, i2q = 0.5 / q, rp = i2p * rho / p, rq = i2q * rho / q,
-                         e2 = 0.5 * inv;
+            // rho/p = q/(p+q) and rho/q = p/(p+q): no division beyond 1/(p+q)
+            const double i2p = P.h, i2q = Q.h, rp = i2p * (q * inv), rq = i2q * (p * inv), e2 = 0.5 * inv;
             k.pa[0] = (R)P.X[0];
             k.pa[1] = (R)P.X[1];
             k.pa[2] = (R)P.X[2];

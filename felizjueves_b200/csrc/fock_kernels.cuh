@@ -44,11 +44,32 @@ struct KArgs {
     const int *unit_count;  // its length, on the device
 };
 
+// 1/(2m+1), m = 0 .. kBoysMaxM: the downward recursion multiplies by these
+// (each the correctly rounded quotient) instead of dividing.
+static __constant__ double kRecipOdd[kBoysMaxM + 1] = {1.0 / 1.0, 1.0 / 3.0, 1.0 / 5.0, 1.0 / 7.0, 1.0 / 9.0, 1.0 / 11.0, 1.0 / 13.0, 1.0 / 15.0, 1.0 / 17.0, 1.0 / 19.0, 1.0 / 21.0, 1.0 / 23.0, 1.0 / 25.0, 1.0 / 27.0, 1.0 / 29.0, 1.0 / 31.0, 1.0 / 33.0, 1.0 / 35.0, 1.0 / 37.0, 1.0 / 39.0, 1.0 / 41.0, 1.0 / 43.0, 1.0 / 45.0, 1.0 / 47.0, 1.0 / 49.0};
+
+// exp(-T) at a table node's offset d = T_i - T (|d| <= kBoysDelta/2):
+// exp(-T_i) (the row's last entry) times the degree-8 Taylor polynomial of
+// exp(d), by Horner.
+__device__ __forceinline__ double boys_exp(const double *__restrict__ row0, double d) {
+    double p = 1.0 / 40320.0;
+    p = 1.0 / 5040.0 + d * p;
+    p = 1.0 / 720.0 + d * p;
+    p = 1.0 / 120.0 + d * p;
+    p = 1.0 / 24.0 + d * p;
+    p = 1.0 / 6.0 + d * p;
+    p = 0.5 + d * p;
+    p = 1.0 + d * p;
+    p = 1.0 + d * p;
+    return __ldg(row0 + kBoysMaxM + 1) * p;
+}
+
 __device__ __forceinline__ void boys_eval(int M, double T, double *F, const double *__restrict__ tab) {
     if (T < kBoysTMax) {
         const int i = __double2int_rn(T * (1.0 / kBoysDelta));
         const double d = (double)i * kBoysDelta - T;
-        const double *row = tab + (size_t)i * (kBoysMaxM + 1) + M;
+        const double *row0 = tab + (size_t)i * kBoysRow;
+        const double *row = row0 + M;
         double f = __ldg(row + 6);
         f = __ldg(row + 5) + f * d * (1.0 / 6.0);
         f = __ldg(row + 4) + f * d * (1.0 / 5.0);
@@ -58,8 +79,8 @@ __device__ __forceinline__ void boys_eval(int M, double T, double *F, const doub
         f = __ldg(row + 0) + f * d;
         F[M] = f;
         if (M > 0) {
-            const double e = exp(-T), t2 = 2.0 * T;
-            for (int m = M - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) / (double)(2 * m + 1);
+            const double e = boys_exp(row0, d), t2 = 2.0 * T;
+            for (int m = M - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * kRecipOdd[m];
         }
     } else {
         const double e = exp(-T), h = 0.5 / T;

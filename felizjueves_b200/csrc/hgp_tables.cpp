@@ -287,20 +287,28 @@ bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, int 
     o->n_ck = (int)c.ck.size();
     const int hr = c.nab * c.nbf + c.nab * c.ncd;
     const int dblk = c.nab + c.ncd + c.na * c.nc + c.na * c.nd + c.nb * c.nc + c.nb * c.nd;
-    const int fixed = c.nbe * c.nbf + 8 * max_kab + 8 * max_kcd + o->n_cb + o->n_ck + dblk +
-                      c.nab + 16;
-    int want = std::max(1, std::min(max_kab * max_kcd, threads));
+    // the single-slot path's Boys leaves of every primitive quartet of a quartet
+    const int fleaves = max_kab * max_kcd * (c.L + 1);
+    const int fixed = kPrimWords * max_kab + o->n_cb + o->n_ck + dblk + c.nab + fleaves + 18;
+    // per ket of a group: its boundary and its staged primitive pairs
+    const int per_ket = c.nbe * c.nbf + kPrimWords * max_kcd;
+    // Slots span (ket, primitive quartet) pairs: up to one per thread, and
+    // no more than a full unit of kets needs.
+    int want = std::max(1, std::min(threads, kKetChunk * max_kab * max_kcd));
     int slots = force_slots > 0 ? std::min(force_slots, threads) : want;
-    auto total = [&](int s) { return std::max(s * c.n_nodes, hr) + s * kNumScalars + fixed; };
-    // Occupancy first: shrink the chunk of primitive quartets until the CTA
-    // fits its target, unless one slot already needs more; then stay inside
-    // the hard budget.
+    auto group = [&](int s) { return std::max(1, std::min(kKetChunk, s)); };
+    auto total = [&](int s) {
+        return std::max(s * c.n_nodes, hr) + s * kNumScalars + fixed + group(s) * per_ket;
+    };
+    // Occupancy first: shrink the chunk until the CTA fits its target,
+    // unless one slot already needs more; then stay inside the hard budget.
     if (force_slots <= 0)
         while (slots > 1 && total(slots) > target) --slots;
     while (slots > 1 && total(slots) > budget) --slots;
     o->threads = threads;
     if (total(slots) > budget) return false;
     o->slots = slots;
+    o->group = group(slots);
     o->vregion = std::max(slots * c.n_nodes, hr);
     int off = 0;
     auto take = [&](int n) {
@@ -309,14 +317,15 @@ bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, int 
         return r;
     };
     o->sm_V = take(o->vregion);
-    o->sm_bound = take(c.nbe * c.nbf);
+    o->sm_bound = take(o->group * c.nbe * c.nbf);
     o->sm_S = take(slots * kNumScalars);
-    o->sm_braP = take(8 * max_kab);
-    o->sm_ketP = take(8 * max_kcd);
+    o->sm_braP = take(kPrimWords * max_kab);
+    o->sm_ketP = take(o->group * kPrimWords * max_kcd);
     o->sm_cb = take(o->n_cb);
     o->sm_ck = take(o->n_ck);
     o->sm_D = take(dblk);
     o->sm_Jab = take(c.nab);
+    o->sm_F = take(fleaves);
     o->sm_total = off;
     return off <= budget;
 }

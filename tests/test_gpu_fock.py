@@ -186,6 +186,10 @@ def test_graph_build_replays_the_build(cuda, lib_built):
         torch.cuda.synchronize()
         for a, b in zip(out, ref2):
             assert float((a - b).abs().max()) <= 1e-11
+        # the build and class timings read after a replay are that replay's
+        ms, n_launches = eng.last_build_stats()
+        assert ms > 0.0 and n_launches > 0
+        assert all(r["ms"] >= 0.0 for r in eng.class_stats())
 
 
 def test_device_build_matches_host_build(cuda, lib_built):
