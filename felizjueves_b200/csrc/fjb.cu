@@ -189,8 +189,11 @@ __global__ void router_features_kernel(const int32_t *samples, int n, const Laun
     bound[s] = __dmul_rn(bra.G, __dmul_rn(ket.G, dmax));
 }
 
-// The HGP Fock kernel (file header of fock_kernels.cuh).  All floating-point
-// work is FP64.
+// The HGP Fock kernel (file header of fock_kernels.cuh).  R is the
+// recurrence type: double for the plain FP64 path; float for the routed
+// path's low-magnitude units, where the VRR, the boundary and the HRR run in
+// FP32 while the primitive scalars are formed, the Boys leaves evaluated
+// and the digest into J and K accumulated in FP64.
 //
 // One CTA per work unit.  The unit's ket pairs are first screened and
 // compacted (warp 0, one lane per ket); the computed kets are then taken in
@@ -200,19 +203,19 @@ __global__ void router_features_kernel(const int32_t *samples, int n, const Laun
 // so each level's barrier covers G quartets' work; each ket's boundary is
 // kept apart (bound[g]), then the HRR and the digest run ket by ket.  With
 // one slot the registers-held single-slot path runs instead.
-template <int NT>
+template <int NT, typename R>
 __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
     extern __shared__ __align__(16) double sm[];
     __shared__ int s_list[kKetChunk];
     __shared__ int s_n;
     const ClassDev &C = A.C;
-    double *V = sm + C.sm_V;
-    double *bound_all = sm + C.sm_bound;
-    double *S = sm + C.sm_S;
+    R *V = reinterpret_cast<R *>(sm + C.sm_V);
+    R *bound_all = reinterpret_cast<R *>(sm + C.sm_bound);
+    R *S = reinterpret_cast<R *>(sm + C.sm_S);
     double *braP = sm + C.sm_braP;
     double *ketP = sm + C.sm_ketP;
-    double *cb = sm + C.sm_cb;
-    double *ck = sm + C.sm_ck;
+    R *cb = reinterpret_cast<R *>(sm + C.sm_cb);
+    R *ck = reinterpret_cast<R *>(sm + C.sm_ck);
     double *Dab = sm + C.sm_D;
     double *Dcd = Dab + C.nab;
     double *Dac = Dcd + C.ncd;
@@ -240,8 +243,8 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
         }
         for (int i = tid; i < C.n_cb; i += nt) {
             const HCoef h = C.cb[i];
-            cb[i] = (double)h.binom * ipow(bra.AB[0], h.px) * ipow(bra.AB[1], h.py) *
-                    ipow(bra.AB[2], h.pz);
+            cb[i] = (R)((double)h.binom * ipow(bra.AB[0], h.px) * ipow(bra.AB[1], h.py) *
+                        ipow(bra.AB[2], h.pz));
         }
         if (!tap)
             for (int i = tid; i < nab; i += nt) {
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                 const PairRec ket = A.pairs[LR.ket_pair0 + s_list[g0 + g]];
                 ketP[i] = reinterpret_cast<const double *>(A.prims + ket.prim0)[r];
             }
-            for (int i = tid; i < ng * nbnd; i += nt) bound_all[i] = 0.0;
+            for (int i = tid; i < ng * nbnd; i += nt) bound_all[i] = (R)0;
             __syncthreads();
 
             if (slots == 1) {
@@ -305,15 +308,15 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                     const double ppq = p + q, inv = 1.0 / ppq, rho = p * q * inv;
                     const double PQx = pb[0] - pk[0], PQy = pb[1] - pk[1], PQz = pb[2] - pk[2];
                     const double wp = -q * inv, wq = p * inv;
-                    const double i2p = pb[8], i2q = pk[8];
-                    const double rp = i2p * (q * inv), rq = i2q * (p * inv), e2 = 0.5 * inv;
-                    const double pa0 = pb[3], pa1 = pb[4], pa2 = pb[5];
-                    const double qc0 = pk[3], qc1 = pk[4], qc2 = pk[5];
-                    const double wp0 = wp * PQx, wp1 = wp * PQy, wp2 = wp * PQz;
-                    const double wq0 = wq * PQx, wq1 = wq * PQy, wq2 = wq * PQz;
+                    const R i2p = (R)pb[8], i2q = (R)pk[8];
+                    const R rp = (R)(pb[8] * (q * inv)), rq = (R)(pk[8] * (p * inv)), e2 = (R)(0.5 * inv);
+                    const R pa0 = (R)pb[3], pa1 = (R)pb[4], pa2 = (R)pb[5];
+                    const R qc0 = (R)pk[3], qc1 = (R)pk[4], qc2 = (R)pk[5];
+                    const R wp0 = (R)(wp * PQx), wp1 = (R)(wp * PQy), wp2 = (R)(wp * PQz);
+                    const R wq0 = (R)(wq * PQx), wq1 = (R)(wq * PQy), wq2 = (R)(wq * PQz);
                     (void)rho;
-                    if (tid == 0) V[0] = 0.0;
-                    if (tid <= L) V[__ldg(C.leaf + tid)] = Fq[t * (L + 1) + tid];
+                    if (tid == 0) V[0] = (R)0;
+                    if (tid <= L) V[__ldg(C.leaf + tid)] = (R)Fq[t * (L + 1) + tid];
                     __syncthreads();
                     for (int lv = 0; lv < C.n_levels; ++lv) {
                         const int o0 = __ldg(C.level_off + lv), o1 = __ldg(C.level_off + lv + 1);
@@ -322,7 +325,7 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                             VOp op;
                             memcpy(&op, &raw, sizeof(op));
                             const int d = op.d;
-                            double a, b, c, dd;
+                            R a, b, c, dd;
                             if (op.kind) {
                                 a = d == 0 ? qc0 : (d == 1 ? qc1 : qc2);
                                 b = d == 0 ? wq0 : (d == 1 ? wq1 : wq2);
@@ -334,9 +337,9 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                                 c = i2p;
                                 dd = rp;
                             }
-                            double v = a * V[op.s0] + b * V[op.s1];
-                            v += (double)op.c2 * (c * V[op.s2] - dd * V[op.s3]);
-                            v += (double)op.c4 * e2 * V[op.s4];
+                            R v = a * V[op.s0] + b * V[op.s1];
+                            v += (R)op.c2 * (c * V[op.s2] - dd * V[op.s3]);
+                            v += (R)op.c4 * e2 * V[op.s4];
                             V[op.dst] = v;
                         }
                         __syncthreads();
@@ -357,7 +360,7 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                         const double PQx = pb[0] - pk[0], PQy = pb[1] - pk[1], PQz = pb[2] - pk[2];
                         const double wp = -q * inv, wq = p * inv;
                         const double inv2p = pb[8], inv2q = pk[8];
-                        double *Ss = S + s;
+                        R *Ss = S + s;
                         Ss[0 * slots] = pb[3];
                         Ss[1 * slots] = pb[4];
                         Ss[2 * slots] = pb[5];
@@ -379,8 +382,8 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                         double F[kMaxLQuartet + 1];
                         boys_eval(L, T, F, A.boys_tab);
                         const double seed = pb[7] * pk[7] * kTwoOverSqrtPi * sqrt(rho);
-                        V[s] = 0.0;
-                        for (int m = 0; m <= L; ++m) V[(size_t)__ldg(C.leaf + m) * slots + s] = seed * F[m];
+                        V[s] = (R)0;
+                        for (int m = 0; m <= L; ++m) V[(size_t)__ldg(C.leaf + m) * slots + s] = (R)(seed * F[m]);
                     }
                     __syncthreads();
                     for (int lv = 0; lv < C.n_levels; ++lv) {
@@ -391,16 +394,16 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                             const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(C.ops) + oi);
                             VOp op;
                             memcpy(&op, &raw, sizeof(op));
-                            const double *Ss = S + s;
+                            const R *Ss = S + s;
                             const int base = op.kind * 8;
-                            const double a = Ss[(base + op.d) * slots];
-                            const double b = Ss[(base + 3 + op.d) * slots];
-                            const double c = Ss[(base + 6) * slots];
-                            const double dd = Ss[(base + 7) * slots];
-                            const double e = Ss[16 * slots];
-                            double v = a * V[(size_t)op.s0 * slots + s] + b * V[(size_t)op.s1 * slots + s];
-                            v += (double)op.c2 * (c * V[(size_t)op.s2 * slots + s] - dd * V[(size_t)op.s3 * slots + s]);
-                            v += (double)op.c4 * e * V[(size_t)op.s4 * slots + s];
+                            const R a = Ss[(base + op.d) * slots];
+                            const R b = Ss[(base + 3 + op.d) * slots];
+                            const R c = Ss[(base + 6) * slots];
+                            const R dd = Ss[(base + 7) * slots];
+                            const R e = Ss[16 * slots];
+                            R v = a * V[(size_t)op.s0 * slots + s] + b * V[(size_t)op.s1 * slots + s];
+                            v += (R)op.c2 * (c * V[(size_t)op.s2 * slots + s] - dd * V[(size_t)op.s3 * slots + s]);
+                            v += (R)op.c4 * e * V[(size_t)op.s4 * slots + s];
                             V[(size_t)op.dst * slots + s] = v;
                         }
                         __syncthreads();
@@ -411,7 +414,7 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                         const int g = glo + it / nbnd, t = it - (it / nbnd) * nbnd;
                         const int s0 = max(c0, g * K) - c0, s1 = min(c0 + ns, (g + 1) * K) - c0;
                         const size_t node = __ldg(C.tgt + t);
-                        double acc = 0.0;
+                        R acc = (R)0;
                         for (int s = s0; s < s1; ++s) acc += V[node * slots + s];
                         bound_all[(size_t)g * nbnd + t] += acc;
                     }
@@ -422,16 +425,16 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
             for (int g = 0; g < ng; ++g) {
                 const int ik = s_list[g0 + g];
                 const PairRec ket = A.pairs[LR.ket_pair0 + ik];
-                const double *bound = bound_all + (size_t)g * nbnd;
+                const R *bound = bound_all + (size_t)g * nbnd;
                 const double deg = (bra.a == bra.b ? 0.5 : 1.0) * (ket.a == ket.b ? 0.5 : 1.0) *
                                    ((LR.diag && ik == U.ib) ? 0.5 : 1.0);
                 // HRR, bra side: X[ab][f] = sum_k coefB(b,k) (a+k, 0 | f);
                 // alongside, the ket's HRR coefficients and density blocks
-                double *X = V, *Y = V + (size_t)nab * nbf;
+                R *X = V, *Y = V + (size_t)nab * nbf;
                 for (int i = tid; i < nab * nbf; i += nt) {
                     const int ab = i / nbf, jf = i - ab * nbf;
                     const int t0 = __ldg(C.bra_off + ab), t1 = __ldg(C.bra_off + ab + 1);
-                    double acc = 0.0;
+                    R acc = (R)0;
                     for (int t = t0; t < t1; ++t) {
                         const HTerm h = C.bra_terms[t];
                         acc += cb[h.cidx] * bound[h.src * nbf + jf];
@@ -440,8 +443,8 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                 }
                 for (int i = tid; i < C.n_ck; i += nt) {
                     const HCoef h = C.ck[i];
-                    ck[i] = (double)h.binom * ipow(ket.AB[0], h.px) * ipow(ket.AB[1], h.py) *
-                            ipow(ket.AB[2], h.pz);
+                    ck[i] = (R)((double)h.binom * ipow(ket.AB[0], h.px) * ipow(ket.AB[1], h.py) *
+                                ipow(ket.AB[2], h.pz));
                 }
                 if (!tap) {
                     const int oa = bra.ao_a, ob = bra.ao_b, oc = ket.ao_a, od = ket.ao_b;
@@ -461,7 +464,7 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                 for (int i = tid; i < nab * ncd; i += nt) {
                     const int ab = i / ncd, cd = i - ab * ncd;
                     const int t0 = __ldg(C.ket_off + cd), t1 = __ldg(C.ket_off + cd + 1);
-                    double acc = 0.0;
+                    R acc = (R)0;
                     for (int t = t0; t < t1; ++t) {
                         const HTerm h = C.ket_terms[t];
                         acc += ck[h.cidx] * X[ab * nbf + h.src];
@@ -484,7 +487,7 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                     for (int o = tid; o < n6; o += nt) {
                         double acc = 0.0;
                         if (o < n1) {
-                            const double *y = Y + (size_t)o * ncd;
+                            const R *y = Y + (size_t)o * ncd;
                             for (int kl = 0; kl < ncd; ++kl) acc += Dcd[kl] * y[kl];
                             Jab[o] += w2 * acc;
                         } else if (o < n2) {
@@ -590,7 +593,8 @@ struct ClassEntry {
         ket_terms.upload(host.ket_terms);
     }
     // threads/slots <= 0: the class's default configuration
-    ClassDev dev(int max_kab, int max_kcd, int threads = 0, int slots = 0) const {
+    // rsize: bytes of the recurrence type (8 FP64, 4 the routed FP32 kernel)
+    ClassDev dev(int max_kab, int max_kcd, int threads = 0, int slots = 0, int rsize = 8) const {
         ClassDev d;
         int th = 0, target = 0;
         default_config(host, kSmemBudgetDoubles, &th, &target);
@@ -598,7 +602,7 @@ struct ClassEntry {
             th = threads;
             target = kSmemBudgetDoubles * threads / (16 * 32);
         }
-        if (!layout_class(host, max_kab, max_kcd, kSmemBudgetDoubles, th, target, slots, &d))
+        if (!layout_class(host, max_kab, max_kcd, kSmemBudgetDoubles, th, target, slots, &d, rsize))
             throw std::length_error("class does not fit in shared memory");
         d.level_off = level_off.p;
         d.ops = ops.p;
@@ -616,31 +620,33 @@ struct ClassEntry {
 
 struct ClassRun {
     ClassDev dev;  // the interpreter kernel's layout (kept valid for every class)
+    ClassDev dev32;  // the FP32 interpreter's layout (routed builds of classes without has32)
     int unit0 = 0, n_units = 0;
     int grid = 0;
     int max_kab = 1, max_kcd = 1;
     bool compiled = false;  // FP64 units run on the class-templated register kernel
     bool has32 = false;     // the class has an FP32 register body (routed builds)
-    int grid32 = 0;         // grid of the FP32 register kernel
+    int grid32 = 0;         // grid of the routed path's FP32 kernel (register or interpreter)
 };
 
-template <int NT>
+template <int NT, typename R>
 int occupancy(const ClassDev &d) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hgp_fock_kernel<NT>, NT,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hgp_fock_kernel<NT, R>, NT,
                                                   (size_t)d.sm_total * sizeof(double));
     return per_sm;
 }
 
 // Launch the HGP kernel instantiated for the class's CTA width.
+template <typename R>
 cudaError_t launch_hgp(const ClassDev &d, int grid, cudaStream_t st, const KArgs &a) {
     const size_t smem = (size_t)d.sm_total * sizeof(double);
     switch (d.threads) {
-        case 32: hgp_fock_kernel<32><<<grid, 32, smem, st>>>(a); break;
-        case 64: hgp_fock_kernel<64><<<grid, 64, smem, st>>>(a); break;
-        case 128: hgp_fock_kernel<128><<<grid, 128, smem, st>>>(a); break;
-        case 256: hgp_fock_kernel<256><<<grid, 256, smem, st>>>(a); break;
-        case 512: hgp_fock_kernel<512><<<grid, 512, smem, st>>>(a); break;
+        case 32: hgp_fock_kernel<32, R><<<grid, 32, smem, st>>>(a); break;
+        case 64: hgp_fock_kernel<64, R><<<grid, 64, smem, st>>>(a); break;
+        case 128: hgp_fock_kernel<128, R><<<grid, 128, smem, st>>>(a); break;
+        case 256: hgp_fock_kernel<256, R><<<grid, 256, smem, st>>>(a); break;
+        case 512: hgp_fock_kernel<512, R><<<grid, 512, smem, st>>>(a); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -660,12 +666,16 @@ int run_grid(const ClassRun &r);
 // The FP64 path of a class run (its register kernel, else the interpreter).
 cudaError_t launch_run(const ClassRun &r, cudaStream_t st, const KArgs &a) {
     if (r.compiled) return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, false, r.grid, st, a);
-    return launch_hgp(r.dev, r.grid, st, a);
+    return launch_hgp<double>(r.dev, r.grid, st, a);
 }
 
-// The FP32 register kernel of a class run (routed builds).
+// The FP32 kernel of a class run (routed builds): its register kernel, else
+// the interpreter in FP32 with its own layout.
 cudaError_t launch_run32(const ClassRun &r, cudaStream_t st, const KArgs &a) {
-    return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, true, r.grid32, st, a);
+    if (r.has32) return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, true, r.grid32, st, a);
+    KArgs a32 = a;
+    a32.C = r.dev32;
+    return launch_hgp<float>(r.dev32, r.grid32, st, a32);
 }
 
 }  // namespace
@@ -794,14 +804,15 @@ PairRec pair_record(const HostBasis &B, int a, int b, double G, int prim0, int n
     return r;
 }
 
+template <typename R = double>
 int grid_for(const ClassDev &d, int n_units) {
     int per_sm = 0;
     switch (d.threads) {
-        case 32: per_sm = occupancy<32>(d); break;
-        case 64: per_sm = occupancy<64>(d); break;
-        case 128: per_sm = occupancy<128>(d); break;
-        case 256: per_sm = occupancy<256>(d); break;
-        default: per_sm = occupancy<512>(d); break;
+        case 32: per_sm = occupancy<32, R>(d); break;
+        case 64: per_sm = occupancy<64, R>(d); break;
+        case 128: per_sm = occupancy<128, R>(d); break;
+        case 256: per_sm = occupancy<256, R>(d); break;
+        default: per_sm = occupancy<512, R>(d); break;
     }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -818,7 +829,7 @@ int run_grid(const ClassRun &r) {
 }
 
 int run_grid32(const ClassRun &r) {
-    if (!r.has32) return 0;
+    if (!r.has32) return grid_for<float>(r.dev32, r.n_units);
     const int per_sm = std::max(1, compiled_blocks_per_sm(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, true));
     const int warps_needed = (r.n_units + 3) / 4;
     return std::max(1, std::min(warps_needed, per_sm * sm_count()));
@@ -828,11 +839,16 @@ int ensure_smem_attr(fjb_handle *h) {
     static bool done = false;
     if (done) return 0;
     const int bytes = kSmemBudgetDoubles * (int)sizeof(double);
-    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<32, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<64, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<128, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<256, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<512, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<32, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<64, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<128, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<256, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CUDA_OK(h, cudaFuncSetAttribute(hgp_fock_kernel<512, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     done = true;
     return 0;
 }
@@ -1030,6 +1046,9 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
             const int th = ov == h->cfg.end() ? 0 : ov->second.first;
             run.dev = ov == h->cfg.end() || th == 1 ? ce.dev(deg.first, deg.second)
                                                      : ce.dev(deg.first, deg.second, th, ov->second.second);
+            run.dev32 = ov == h->cfg.end() || th == 1
+                            ? ce.dev(deg.first, deg.second, 0, 0, 4)
+                            : ce.dev(deg.first, deg.second, th, ov->second.second, 4);
             run.compiled = compiled_available(la, lb, lc, ld, false) && (th == 0 || th == 1);
             run.has32 = compiled_available(la, lb, lc, ld, true);
             run.unit0 = (int)units.size();
@@ -1228,7 +1247,7 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
         a.Kp = h->Kp.p;
         a.boys_tab = h->boys.p;
         a.route_thresh = route;
-        if (routed && r.has32) {
+        if (routed) {
             // the precision router splits the class's units into an FP32 and
             // an FP64 queue; each queue has its own kernel
             int *l32 = h->route_list.p + r.unit0;
@@ -1410,7 +1429,7 @@ int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_de
             a.tap_out = out_dev;
             a.tap_off = dto.p;
             a.boys_tab = h->boys.p;
-            CUDA_OK(h, launch_hgp(dev, grid_for(dev, a.n_units), nullptr, a));
+            CUDA_OK(h, launch_hgp<double>(dev, grid_for(dev, a.n_units), nullptr, a));
             CUDA_OK(h, cudaDeviceSynchronize());
         }
     } catch (const std::length_error &e) {
@@ -1432,7 +1451,7 @@ int fjb_route_stats(const fjb_handle *hc, int64_t *n32, int64_t *n64) {
     *n32 = 0;
     *n64 = 0;
     for (size_t ri = 0; ri < h->runs.size(); ++ri) {
-        if (h->last_routed && h->runs[ri].has32) {
+        if (h->last_routed) {
             *n32 += c[2 * ri];
             *n64 += c[2 * ri + 1];
         } else {
@@ -1589,11 +1608,14 @@ int fjb_set_class_config(fjb_handle *h, int la, int lb, int lc, int ld, int thre
         try {
             if (threads == 1 && !compiled_available(la, lb, lc, ld, false))
                 return fail(h, FJB_E_LIMIT, "this class has no compiled register kernel");
-            ClassDev d = threads == 1 ? h->cls(la, lb, lc, ld).dev(r.max_kab, r.max_kcd)
-                                      : h->cls(la, lb, lc, ld).dev(r.max_kab, r.max_kcd, threads, slots);
+            ClassEntry &ce = h->cls(la, lb, lc, ld);
+            ClassDev d = threads == 1 ? ce.dev(r.max_kab, r.max_kcd) : ce.dev(r.max_kab, r.max_kcd, threads, slots);
+            r.dev32 = threads == 1 ? ce.dev(r.max_kab, r.max_kcd, 0, 0, 4)
+                                   : ce.dev(r.max_kab, r.max_kcd, threads, slots, 4);
             r.dev = d;
             r.compiled = compiled_available(la, lb, lc, ld, false) && (threads == 0 || threads == 1);
             r.grid = run_grid(r);
+            r.grid32 = run_grid32(r);
         } catch (const std::length_error &e) {
             return fail(h, FJB_E_LIMIT, e.what());
         }

@@ -266,7 +266,7 @@ void default_config(const ClassHost &c, int budget, int *threads, int *target) {
 }
 
 bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, int threads, int target,
-                  int force_slots, ClassDev *o) {
+                  int force_slots, ClassDev *o, int rsize) {
     *o = ClassDev{};
     o->la = c.la;
     o->lb = c.lb;
@@ -285,20 +285,25 @@ bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, int 
     o->nbf = c.nbf;
     o->n_cb = (int)c.cb.size();
     o->n_ck = (int)c.ck.size();
+    // regions of recurrence values (V, bound, S, cb, ck) hold R (rsize
+    // bytes); the rest is FP64.  rd(): R elements -> doubles, rounded up
+    // to an even count (16-byte alignment).
+    auto rd = [&](long n) { return (int)((((n * rsize + 7) / 8) + 1) & ~1L); };
+    auto dd = [&](long n) { return (int)((n + 1) & ~1L); };
     const int hr = c.nab * c.nbf + c.nab * c.ncd;
     const int dblk = c.nab + c.ncd + c.na * c.nc + c.na * c.nd + c.nb * c.nc + c.nb * c.nd;
     // the single-slot path's Boys leaves of every primitive quartet of a quartet
     const int fleaves = max_kab * max_kcd * (c.L + 1);
-    const int fixed = kPrimWords * max_kab + o->n_cb + o->n_ck + dblk + c.nab + fleaves + 18;
-    // per ket of a group: its boundary and its staged primitive pairs
-    const int per_ket = c.nbe * c.nbf + kPrimWords * max_kcd;
+    const int fixed = dd(kPrimWords * max_kab) + rd(o->n_cb) + rd(o->n_ck) + dd(dblk) + dd(c.nab) + dd(fleaves);
     // Slots span (ket, primitive quartet) pairs: up to one per thread, and
     // no more than a full unit of kets needs.
     int want = std::max(1, std::min(threads, kKetChunk * max_kab * max_kcd));
     int slots = force_slots > 0 ? std::min(force_slots, threads) : want;
     auto group = [&](int s) { return std::max(1, std::min(kKetChunk, s)); };
+    // per ket of a group: its boundary and its staged primitive pairs
     auto total = [&](int s) {
-        return std::max(s * c.n_nodes, hr) + s * kNumScalars + fixed + group(s) * per_ket;
+        return rd(std::max((long)s * c.n_nodes, (long)hr)) + rd((long)s * kNumScalars) + fixed +
+               rd((long)group(s) * c.nbe * c.nbf) + dd((long)group(s) * kPrimWords * max_kcd);
     };
     // Occupancy first: shrink the chunk until the CTA fits its target,
     // unless one slot already needs more; then stay inside the hard budget.
@@ -311,21 +316,21 @@ bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, int 
     o->group = group(slots);
     o->vregion = std::max(slots * c.n_nodes, hr);
     int off = 0;
-    auto take = [&](int n) {
+    auto take = [&](int n_doubles) {
         int r = off;
-        off += (n + 1) & ~1;  // keep 16-byte alignment
+        off += n_doubles;
         return r;
     };
-    o->sm_V = take(o->vregion);
-    o->sm_bound = take(o->group * c.nbe * c.nbf);
-    o->sm_S = take(slots * kNumScalars);
-    o->sm_braP = take(kPrimWords * max_kab);
-    o->sm_ketP = take(o->group * kPrimWords * max_kcd);
-    o->sm_cb = take(o->n_cb);
-    o->sm_ck = take(o->n_ck);
-    o->sm_D = take(dblk);
-    o->sm_Jab = take(c.nab);
-    o->sm_F = take(fleaves);
+    o->sm_V = take(rd(o->vregion));
+    o->sm_bound = take(rd((long)o->group * c.nbe * c.nbf));
+    o->sm_S = take(rd((long)slots * kNumScalars));
+    o->sm_braP = take(dd(kPrimWords * max_kab));
+    o->sm_ketP = take(dd((long)o->group * kPrimWords * max_kcd));
+    o->sm_cb = take(rd(o->n_cb));
+    o->sm_ck = take(rd(o->n_ck));
+    o->sm_D = take(dd(dblk));
+    o->sm_Jab = take(dd(c.nab));
+    o->sm_F = take(dd(fleaves));
     o->sm_total = off;
     return off <= budget;
 }

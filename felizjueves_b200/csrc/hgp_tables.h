@@ -35,11 +35,13 @@ struct ClassHost {
 ClassHost build_class(int la, int lb, int lc, int ld);
 
 // Shared-memory carve-up of a class for staging degrees up to kab/kcd, a
-// CTA of `threads`, and a chunk of primitive quartets sized so the CTA
-// stays within `target_doubles` when it can (`slots` > 0 forces the chunk).
-// Returns false if the class cannot fit the hard budget.
+// CTA of `threads`, and a chunk of (ket, primitive quartet) slots sized so
+// the CTA stays within `target_doubles` when it can (`slots` > 0 forces the
+// chunk).  The recurrence regions hold values of `rsize` bytes (8: the FP64
+// kernel; 4: the routed path's FP32 kernel).  Returns false if the class
+// cannot fit the hard budget.
 bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget_doubles, int threads,
-                  int target_doubles, int slots, ClassDev *out);
+                  int target_doubles, int slots, ClassDev *out, int rsize = 8);
 
 // The default CTA width and shared-memory target of a class: narrow CTAs
 // (a warp) for small programs so many CTAs share an SM, wider ones for the

@@ -162,6 +162,27 @@ def test_routed_build_within_budget(cuda, lib_built, oracle_lib, atoms, seed):
     assert d64 <= 1e-8 and dor <= 1e-8
 
 
+def test_all_fp32_build_at_fp32_accuracy(cuda, lib_built):
+    """With a routing threshold above every bound, every unit of every class
+    runs an FP32 kernel (the register bodies and, for the classes without
+    one, the interpreter in FP32): G then agrees with the FP64 build to FP32
+    accuracy, relative to G's size."""
+    import torch
+    from felizjueves_b200 import _lib, router
+    w = configs.cluster(3, 5)
+    eng = FockEngine(w.basis)
+    eng.plan(w.D, w.tau, w.n_mag)
+    D = torch.tensor(w.D, device=cuda)
+    G64 = eng.build(D)[2].clone()
+    G32 = eng.build(D, precision=_lib.FJB_ROUTED, threshold=1e30)[2].clone()
+    torch.cuda.synchronize()
+    n32, n64 = router.route_stats(eng)
+    rel = float((G32 - G64).abs().max() / G64.abs().max())
+    print(f"all-FP32 build: {n32} FP32 units, {n64} FP64; max|dG|/max|G| {rel:.2e}")
+    assert n64 == 0 and n32 > 0
+    assert rel <= 1e-5
+
+
 def test_graph_build_replays_the_build(cuda, lib_built):
     """The captured build equals the direct one, and replaying it after D is
     updated in place gives the new density's result (the SCF-loop use)."""
