@@ -40,6 +40,10 @@ class PlanLists_t(C.Structure):
         "launches", "screened", "deleted", "magnitudes", "eps", "g_max")]
 
 
+class JLists_t(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("a", "b", "prim", "L", "G", "key", "ket_order", "L_off")]
+
+
 _lib = None
 
 
@@ -84,6 +88,9 @@ def load():
     L.fjb_mlp_gradient.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp, vp]
     L.fjb_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_float, C.c_int, vp]
     L.fjb_route_stats.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
+    L.fjb_coulomb.argtypes = [vp, vp, vp, dbl, vp]
+    L.fjb_j_last_launches.argtypes = [vp]
+    L.fjb_j_plan_lists.argtypes = [vp, vp, C.POINTER(JLists_t), C.POINTER(i64)]
     _lib = L
     return L
 
@@ -95,7 +102,8 @@ EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_
            "fjb_fma_probe", "fjb_fock_build_noalloc", "fjb_set_class_config",
            "fjb_fock_build_graph", "fjb_create_df", "fjb_df_blocks", "fjb_mlp_n_params",
            "fjb_router_set", "fjb_router_features", "fjb_mlp_forward", "fjb_mlp_gradient",
-           "fjb_mlp_adam", "fjb_route_stats")
+           "fjb_mlp_adam", "fjb_route_stats", "fjb_coulomb", "fjb_j_last_launches",
+           "fjb_j_plan_lists")
 
 
 class LaunchStat_t(C.Structure):

@@ -24,6 +24,7 @@
 #include "fjb_internal.h"
 #include "fock_kernels.cuh"
 #include "hgp_tables.h"
+#include "jengine.h"
 #include "plan.h"
 #include "router.cuh"
 
@@ -683,6 +684,8 @@ cudaError_t launch_run32(const ClassRun &r, cudaStream_t st, const KArgs &a) {
 struct fjb_handle {
     int device = 0;
     HostBasis basis;
+    fjb::JEngine *jeng = nullptr;  // the J-engine, built on first use
+    int j_launches = 0;            // kernel launches of the last J-engine build
     std::string err;
     std::map<std::tuple<int, int, int, int>, std::unique_ptr<ClassEntry>> classes;
     std::map<std::tuple<int, int, int, int>, std::pair<int, int>> cfg;  // (threads, slots) overrides
@@ -956,6 +959,7 @@ int fjb_create_df(fjb_handle **out, const fjb_basis *ao, const fjb_basis *aux, i
 
 void fjb_destroy(fjb_handle *h) {
     if (!h) return;
+    if (h->jeng) jengine_destroy(h->jeng);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     delete h;
@@ -1539,6 +1543,52 @@ int fjb_df_blocks(fjb_handle *h, int kind, const int32_t *items, int n, double *
     }
     return fjb_eri_blocks(h, q.data(), n, out_dev, offsets);
 }
+
+int fjb_coulomb(fjb_handle *h, const double *D_dev, double *J_dev, double tau, void *stream) {
+    if (!h || !D_dev || !J_dev) return fail(h, FJB_E_ARG, "null argument");
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    if (h->df) return fail(h, FJB_E_STATE, "a density-fitting handle has no J-engine");
+    if (!std::isfinite(tau) || tau < 0.0) return fail(h, FJB_E_ARG, "tau must be finite and >= 0");
+    CUDA_OK(h, cudaSetDevice(h->device));
+    std::string err;
+    if (!h->jeng) {
+        h->jeng = jengine_create(h->basis, h->device, &err);
+        if (!h->jeng) return fail(h, FJB_E_CUDA, err);
+    }
+    int nl = 0;
+    if (jengine_build(h->jeng, D_dev, J_dev, tau, h->boys.p, (cudaStream_t)stream, &err, &nl))
+        return fail(h, FJB_E_CUDA, err);
+    h->j_launches = nl;
+    return FJB_OK;
+}
+
+int fjb_j_plan_lists(const fjb_handle *hc, const double *D_host, fjb_j_lists *out, int64_t *n_records) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h || !D_host || !n_records) return fail(h, FJB_E_ARG, "null argument");
+    if (h->df) return fail(h, FJB_E_STATE, "a density-fitting handle has no J-engine");
+    JHostLists L;
+    try {
+        jengine_host_lists(h->basis, D_host, &L);
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_PLAN, e.what());
+    }
+    *n_records = (int64_t)L.a.size();
+    if (!out) return FJB_OK;
+    auto put = [](auto *dst, const auto &src) {
+        if (dst) std::copy(src.begin(), src.end(), dst);
+    };
+    put(out->a, L.a);
+    put(out->b, L.b);
+    put(out->prim, L.prim);
+    put(out->L, L.L);
+    put(out->G, L.G);
+    put(out->key, L.key);
+    put(out->ket_order, L.ket_order);
+    put(out->L_off, L.L_off);
+    return FJB_OK;
+}
+
+int fjb_j_last_launches(const fjb_handle *h) { return h ? h->j_launches : -1; }
 
 int fjb_boys(int m, const double *T_dev, int n, double *F_dev) {
     if (m < 0 || m > kBoysMaxM - kBoysTaylor + 1 || n < 0 || !T_dev || !F_dev)

@@ -1,0 +1,534 @@
+// jengine.cu -- the McMurchie-Davidson J-engine on sm_100a.
+//
+// Device layout.  The unique sweep's records (one per primitive pair of each
+// shell pair a >= b, i outer; eri/j_coulomb/j.py:395-405) are stored grouped
+// by L = l_a + l_b (stable, so each group keeps sweep order and a shell
+// pair's records stay contiguous).  Each record owns a Hermite vector of
+// NH(L) = (L+1)(L+2)(L+3)/6 doubles at dq_off in two buffers: D_q (its ket
+// role) and J_p (its bra role).
+//
+// Kernels, in stream order, per build:
+//   j_dq_kernel      warp per record: the per-axis Hermite tables E^{ij}_t
+//                    (mmd/hermite.py:61-79) in shared memory, lanes over q:
+//                    D_q = w pre sum_cd D_cd E^{cd}_q, then key = I_pair *
+//                    max_q |D_q| (ao/density.py:120-148, launch.py:300-310).
+//   segmented radix sort (CUB) of the keys, descending and stable, one
+//                    segment per L: the ket order of launch.py:325.
+//   j_pq_kernel<LP, LQ>  one launch per (bra L, ket L) class: a warp per bra
+//                    record walks the class's sorted kets 32 at a time, one
+//                    lane per ket, and stops after the chunk holding the
+//                    first ket with I_bra * key < tau (the sorted break,
+//                    j.py:520-536).  A lane forms [0]^(m) = (2/sqrt(pi))
+//                    theta (-2 theta^2)^m F_m(theta^2 |PQ|^2) (reference/
+//                    pq.py:40-58), raises R_{tuv} in registers by
+//                    [r]^(m) = PQ_d [r-1_d]^(m+1) + (r_d - 1) [r-2_d]^(m+1)
+//                    along the first nonzero axis (pq.py:103-114), and adds
+//                    (-1)^|q| R_{p+q} D_q into its J_p partials; the warp
+//                    reduces them by shuffles and one lane adds them to the
+//                    record's J_p.
+//   j_jab_kernel     warp per unique shell pair: J_ab = sum_records pre
+//                    sum_p E^{ab}_p J_p, written to J[a][b] and mirrored to
+//                    J[b][a]; on a diagonal pair only the lower triangle
+//                    i >= j writes (both positions), so every element of J
+//                    has exactly one writer: no atomics and no zeroing
+//                    (j.py:303-326's scatter).
+// Roofline: j_pq_kernel is FP64-pipe bound (R recursion + NH(LP) x NH(LQ)
+// FMAs per bra-ket record pair); the others are small.
+#include "jengine.h"
+
+#include <cub/device/device_segmented_radix_sort.cuh>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <memory>
+#include <numeric>
+#include <utility>
+
+#include "fock_compiled.cuh"
+
+namespace fjb {
+
+namespace {
+
+constexpr int kJMaxL = 2 * kMaxL;  // L of one record
+constexpr int kNHMax = (kJMaxL + 1) * (kJMaxL + 2) * (kJMaxL + 3) / 6;  // 84
+
+__host__ __device__ constexpr int nh(int L) { return (L + 1) * (L + 2) * (L + 3) / 6; }
+
+// cartesians(l) components for l <= 3, at offset l(l+1)(l+2)/6.
+__constant__ int8_t kCart[20][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0}, {1, 1, 0}, {1, 0, 1},
+                                    {0, 2, 0}, {0, 1, 1}, {0, 0, 2}, {3, 0, 0}, {2, 1, 0}, {2, 0, 1}, {1, 2, 0},
+                                    {1, 1, 1}, {1, 0, 2}, {0, 3, 0}, {0, 2, 1}, {0, 1, 2}, {0, 0, 3}};
+
+// Hermite indices (t, u, v) of hermite_order(2 * kJMaxL), for R tables.
+constexpr int kNRMax = nh(2 * kJMaxL);  // 455
+__constant__ int8_t kHermR[kNRMax][3];
+
+struct JRec {
+    double P[3], PA[3], PB[3];
+    double zeta, pre, G;  // pre = c_a c_b (pi/zeta)^{3/2} exp(-alpha beta/zeta |AB|^2)
+    int32_t la, lb, ao_a, ao_b;
+    int32_t L, pair, dq_off, pad;
+};
+static_assert(sizeof(JRec) == 128, "JRec is 128 bytes");
+
+constexpr int kETab = 4 * 4 * (kJMaxL + 1);  // E[i][j][t], i, j <= 3, t <= 6
+
+// One axis's E^{ij}_t for i <= la, j <= lb (E^{00}_0 = 1: the Gaussian
+// product factor is in pre), zero beyond t = i + j.
+__device__ void e_table(int la, int lb, double h, double pa, double pb, double *E) {
+    for (int k = 0; k < kETab; ++k) E[k] = 0.0;
+    auto at = [&](int i, int j, int t) -> double & { return E[(i * 4 + j) * (kJMaxL + 1) + t]; };
+    at(0, 0, 0) = 1.0;
+    for (int i = 0; i < la; ++i)
+        for (int t = 0; t <= i + 1; ++t) {
+            double v = pa * at(i, 0, t);
+            if (t >= 1) v += h * at(i, 0, t - 1);
+            if (t + 1 <= i) v += (double)(t + 1) * at(i, 0, t + 1);
+            at(i + 1, 0, t) = v;
+        }
+    for (int i = 0; i <= la; ++i)
+        for (int j = 0; j < lb; ++j)
+            for (int t = 0; t <= i + j + 1; ++t) {
+                double v = pb * at(i, j, t);
+                if (t >= 1) v += h * at(i, j, t - 1);
+                if (t + 1 <= i + j) v += (double)(t + 1) * at(i, j, t + 1);
+                at(i, j + 1, t) = v;
+            }
+}
+
+__device__ __forceinline__ double etab(const double *E, int i, int j, int t) {
+    return E[(i * 4 + j) * (kJMaxL + 1) + t];
+}
+
+__global__ void j_dq_kernel(const JRec *__restrict__ recs, int n, const double *__restrict__ D, int n_ao,
+                            double *__restrict__ Dq, double *__restrict__ key) {
+    __shared__ double Es[4][3][kETab];
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int r = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); r < n; r += nw) {
+        const JRec R = recs[r];
+        if (lane < 3) e_table(R.la, R.lb, 0.5 / R.zeta, R.PA[lane], R.PB[lane], Es[wl][lane]);
+        __syncwarp();
+        const double *Ex = Es[wl][0], *Ey = Es[wl][1], *Ez = Es[wl][2];
+        const int na = (R.la + 1) * (R.la + 2) / 2, nb = (R.lb + 1) * (R.lb + 2) / 2;
+        const int ca = R.la * (R.la + 1) * (R.la + 2) / 6, cb = R.lb * (R.lb + 1) * (R.lb + 2) / 6;
+        const double w = R.ao_a == R.ao_b ? 1.0 : 2.0;
+        double m = 0.0;
+        for (int q = lane; q < nh(R.L); q += 32) {
+            const int t = kHermR[q][0], u = kHermR[q][1], v = kHermR[q][2];
+            double acc = 0.0;
+            for (int i = 0; i < na; ++i) {
+                const int8_t *c = kCart[ca + i];
+                const double *Drow = D + (size_t)(R.ao_a + i) * n_ao + R.ao_b;
+                for (int j = 0; j < nb; ++j) {
+                    const int8_t *d = kCart[cb + j];
+                    const double e = etab(Ex, c[0], d[0], t) * etab(Ey, c[1], d[1], u) * etab(Ez, c[2], d[2], v);
+                    acc += Drow[j] * e;
+                }
+            }
+            const double dq = w * (R.pre * acc);
+            Dq[R.dq_off + q] = dq;
+            m = fmax(m, fabs(dq));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) key[r] = R.G * m;
+        __syncwarp();
+    }
+}
+
+__device__ __forceinline__ int h_index(int t, int u, int v) {
+    const int n = t + u + v;
+    return (n == 0 ? 0 : nh(n - 1)) + (n - t) * (n - t + 1) / 2 + (n - t - u);
+}
+
+// One (bra L, ket L) class at total order L = lp + lq (runtime lp, lq).
+template <int L>
+__global__ void __launch_bounds__(128) j_pq_kernel(const JRec *__restrict__ recs, int lp, int lq, int bra0, int nbra,
+                                                   int ket0, int nket, const int *__restrict__ order,
+                                                   const double *__restrict__ skey, const double *__restrict__ Dq,
+                                                   double *__restrict__ Jp, double tau,
+                                                   const double *__restrict__ boys_tab) {
+    constexpr int NR = nh(L), NPMAX = nh(L < kJMaxL ? L : kJMaxL);
+    constexpr double kTwoOverSqrtPi = 1.1283791670955126;
+    const int NP = nh(lp), NQ = nh(lq);
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int bi = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); bi < nbra; bi += nw) {
+        const JRec B = recs[bra0 + bi];
+        double jp[NPMAX];
+        for (int p = 0; p < NP; ++p) jp[p] = 0.0;
+        for (int k0 = 0; k0 < nket; k0 += 32) {
+            const int k = k0 + lane;
+            const bool on = k < nket && !(B.G * skey[ket0 + k] < tau);
+            if (on) {
+                const JRec K = recs[order[ket0 + k]];
+                const double p = B.zeta, q = K.zeta;
+                const double rho = p * q / (p + q);
+                const double X = B.P[0] - K.P[0], Y = B.P[1] - K.P[1], Z = B.P[2] - K.P[2];
+                const double T = rho * (X * X + Y * Y + Z * Z);
+                double F[L + 1];
+                boys_t<L>(T, F, boys_tab);
+                const double pref = kTwoOverSqrtPi * sqrt(rho), m2r = -2.0 * rho;
+                double f[L + 1];
+                double pw = pref;
+#pragma unroll
+                for (int m = 0; m <= L; ++m) {
+                    f[m] = pw * F[m];
+                    pw *= m2r;
+                }
+                // R_{tuv}: level m = L holds [0]^(L); each lower level
+                // rewrites totals L-m .. 1 from the level above (read before
+                // they are overwritten: totals descend), then [0]^(m).
+                double R[NR];
+                R[0] = f[L];
+                for (int m = L - 1; m >= 0; --m) {
+                    for (int s = L - m; s >= 1; --s) {
+                        for (int i = nh(s - 1); i < nh(s); ++i) {
+                            const int t = kHermR[i][0], u = kHermR[i][1], v = kHermR[i][2];
+                            double x;
+                            if (t > 0) {
+                                x = X * R[h_index(t - 1, u, v)];
+                                if (t >= 2) x += (double)(t - 1) * R[h_index(t - 2, u, v)];
+                            } else if (u > 0) {
+                                x = Y * R[h_index(0, u - 1, v)];
+                                if (u >= 2) x += (double)(u - 1) * R[h_index(0, u - 2, v)];
+                            } else {
+                                x = Z * R[h_index(0, 0, v - 1)];
+                                if (v >= 2) x += (double)(v - 1) * R[h_index(0, 0, v - 2)];
+                            }
+                            R[i] = x;
+                        }
+                    }
+                    R[0] = f[m];
+                }
+                const double *dq = Dq + K.dq_off;
+                for (int qi = 0; qi < NQ; ++qi) {
+                    const int tq = kHermR[qi][0], uq = kHermR[qi][1], vq = kHermR[qi][2];
+                    const double d = (((tq + uq + vq) & 1) ? -1.0 : 1.0) * __ldg(dq + qi);
+                    for (int pi = 0; pi < NP; ++pi)
+                        jp[pi] += R[h_index(kHermR[pi][0] + tq, kHermR[pi][1] + uq, kHermR[pi][2] + vq)] * d;
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, on);
+            if (__popc(bal) < min(32, nket - k0)) break;  // the first ket under tau is in this chunk
+        }
+        for (int pi = 0; pi < NP; ++pi) {
+            double v = jp[pi];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) Jp[B.dq_off + pi] += v;
+        }
+    }
+}
+
+__global__ void j_jab_kernel(const JRec *__restrict__ recs, const int *__restrict__ pair_rec0,
+                             const int *__restrict__ pair_nrec, int n_pairs, const double *__restrict__ Jp,
+                             double *__restrict__ J, int n_ao) {
+    __shared__ double Es[4][3][kETab];
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int pr = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); pr < n_pairs; pr += nw) {
+        const int r0 = pair_rec0[pr], nr = pair_nrec[pr];
+        const JRec R0 = recs[r0];
+        const int na = (R0.la + 1) * (R0.la + 2) / 2, nb = (R0.lb + 1) * (R0.lb + 2) / 2;
+        const int ca = R0.la * (R0.la + 1) * (R0.la + 2) / 6, cb = R0.lb * (R0.lb + 1) * (R0.lb + 2) / 6;
+        const int nab = na * nb, np = nh(R0.L);
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};  // elements lane, lane + 32, ... (nab <= 100)
+        for (int r = r0; r < r0 + nr; ++r) {
+            const JRec R = recs[r];
+            if (lane < 3) e_table(R.la, R.lb, 0.5 / R.zeta, R.PA[lane], R.PB[lane], Es[wl][lane]);
+            __syncwarp();
+            const double *Ex = Es[wl][0], *Ey = Es[wl][1], *Ez = Es[wl][2];
+            const double *jp = Jp + R.dq_off;
+            for (int e = lane, s = 0; e < nab; e += 32, ++s) {
+                const int8_t *c = kCart[ca + e / nb];
+                const int8_t *d = kCart[cb + e % nb];
+                double x = 0.0;
+                for (int p = 0; p < np; ++p)
+                    x += etab(Ex, c[0], d[0], kHermR[p][0]) * etab(Ey, c[1], d[1], kHermR[p][1]) *
+                         etab(Ez, c[2], d[2], kHermR[p][2]) * jp[p];
+                acc[s] += R.pre * x;
+            }
+            __syncwarp();
+        }
+        for (int e = lane, s = 0; e < nab; e += 32, ++s) {
+            const int i = e / nb, j = e % nb;
+            if (R0.ao_a == R0.ao_b && i < j) continue;  // diagonal pair: its lower triangle writes both
+            const int x = R0.ao_a + i, y = R0.ao_b + j;
+            J[(size_t)x * n_ao + y] = acc[s];
+            if (x != y) J[(size_t)y * n_ao + x] = acc[s];
+        }
+    }
+}
+
+using PqLaunch = void (*)(int grid, cudaStream_t st, const JRec *, int, int, int, int, int, int, const int *,
+                          const double *, const double *, double *, double, const double *);
+
+template <int L>
+void pq_launch(int grid, cudaStream_t st, const JRec *recs, int lp, int lq, int bra0, int nbra, int ket0, int nket,
+               const int *order, const double *skey, const double *Dq, double *Jp, double tau, const double *boys) {
+    j_pq_kernel<L><<<grid, 128, 0, st>>>(recs, lp, lq, bra0, nbra, ket0, nket, order, skey, Dq, Jp, tau, boys);
+}
+
+template <int... L>
+constexpr std::array<PqLaunch, sizeof...(L)> pq_table(std::integer_sequence<int, L...>) {
+    return {&pq_launch<L>...};
+}
+const auto kPqTable = pq_table(std::make_integer_sequence<int, 2 * kJMaxL + 1>{});
+
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t count) {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = count;
+        return count ? cudaMalloc(&p, count * sizeof(T)) : cudaSuccess;
+    }
+    cudaError_t upload(const std::vector<T> &v) {
+        cudaError_t e = alloc(v.size());
+        if (e != cudaSuccess || v.empty()) return e;
+        return cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    }
+};
+
+// The sweep's records of one ordered shell pair (a, b), i outer
+// (ao/pairs.py:249-267), with I_pair = fsum_p I_p (ao/pairs.py:299-301).
+void pair_records(const HostBasis &B, int a, int b, std::vector<JRec> *out, std::vector<int> *prim) {
+    const HostShell &sa = B.shells[a], &sb = B.shells[b];
+    const int L = sa.l + sb.l;
+    const auto hs = herm_order(L);
+    std::vector<double> I(hs.size());
+    for (size_t i = 0; i < sa.exps.size(); ++i)
+        for (size_t j = 0; j < sb.exps.size(); ++j) {
+            const double alpha = sa.exps[i], beta = sb.exps[j], zeta = alpha + beta;
+            JRec r{};
+            double ex = 1.0;
+            for (int d = 0; d < 3; ++d) {
+                r.P[d] = (alpha * sa.centre[d] + beta * sb.centre[d]) / zeta;
+                r.PA[d] = r.P[d] - sa.centre[d];
+                r.PB[d] = r.P[d] - sb.centre[d];
+                ex *= std::exp(zeta * r.PA[d] * r.PB[d]);  // e_axis's E^{00}_0 per axis
+            }
+            r.zeta = zeta;
+            r.pre = sa.coefs[i] * sb.coefs[j] * std::pow(M_PI / zeta, 1.5) * ex;
+            hermite_bounds(zeta, L, hs, I.data());
+            r.G = fsum(I.data(), I.size());
+            r.la = sa.l;
+            r.lb = sb.l;
+            r.ao_a = B.offsets[a];
+            r.ao_b = B.offsets[b];
+            r.L = L;
+            out->push_back(r);
+            if (prim) prim->push_back((int)(i * sb.exps.size() + j));
+        }
+}
+
+}  // namespace
+
+struct JEngine {
+    int device = 0, n_ao = 0;
+    int n_rec = 0, n_pairs = 0;
+    std::vector<int> L_off;       // [kJMaxL + 2] record groups by L
+    DBuf<JRec> recs;
+    DBuf<int> pair_rec0, pair_nrec, seg_off, iota, order;
+    DBuf<double> Dq, Jp, key, skey;
+    DBuf<unsigned char> sort_tmp;
+    size_t sort_bytes = 0;
+};
+
+JEngine *jengine_create(const HostBasis &basis, int device, std::string *err) {
+    auto e = std::make_unique<JEngine>();
+    e->device = device;
+    e->n_ao = basis.n_ao;
+    const int nsh = (int)basis.shells.size();
+    for (const auto &s : basis.shells)
+        if (s.l > kMaxL) {
+            *err = "J-engine: l above the compiled maximum";
+            return nullptr;
+        }
+    // the sweep: pairs a >= b, a outer; records grouped by L, stable
+    std::vector<std::vector<JRec>> byL(kJMaxL + 1);
+    std::vector<std::vector<int>> pairs_byL(kJMaxL + 1);  // first record (within its L group) per pair
+    std::vector<std::vector<int>> pairn_byL(kJMaxL + 1);
+    for (int a = 0; a < nsh; ++a)
+        for (int b = 0; b <= a; ++b) {
+            std::vector<JRec> rs;
+            pair_records(basis, a, b, &rs, nullptr);
+            const int L = rs[0].L;
+            pairs_byL[L].push_back((int)byL[L].size());
+            pairn_byL[L].push_back((int)rs.size());
+            for (auto &r : rs) byL[L].push_back(r);
+        }
+    std::vector<JRec> all;
+    std::vector<int> p0, pn;
+    e->L_off.assign(kJMaxL + 2, 0);
+    int dq = 0;
+    for (int L = 0; L <= kJMaxL; ++L) {
+        e->L_off[L] = (int)all.size();
+        for (size_t k = 0; k < pairs_byL[L].size(); ++k) {
+            p0.push_back(e->L_off[L] + pairs_byL[L][k]);  // group-relative start, shifted
+            pn.push_back(pairn_byL[L][k]);
+        }
+        for (auto &r : byL[L]) {
+            r.dq_off = dq;
+            dq += nh(L);
+            all.push_back(r);
+        }
+    }
+    e->L_off[kJMaxL + 1] = (int)all.size();
+    e->n_rec = (int)all.size();
+    e->n_pairs = (int)p0.size();
+    if (cudaSetDevice(device) != cudaSuccess) {
+        *err = "cudaSetDevice failed";
+        return nullptr;
+    }
+    std::vector<int8_t> herm;
+    for (const auto &h : herm_order(2 * kJMaxL))
+        for (int d = 0; d < 3; ++d) herm.push_back((int8_t)h[d]);
+    std::vector<int> io(e->n_rec);
+    std::iota(io.begin(), io.end(), 0);
+    cudaError_t ce = cudaMemcpyToSymbol(kHermR, herm.data(), herm.size());
+    if (ce == cudaSuccess) ce = e->recs.upload(all);
+    if (ce == cudaSuccess) ce = e->pair_rec0.upload(p0);
+    if (ce == cudaSuccess) ce = e->pair_nrec.upload(pn);
+    if (ce == cudaSuccess) ce = e->seg_off.upload(e->L_off);
+    if (ce == cudaSuccess) ce = e->iota.upload(io);
+    if (ce == cudaSuccess) ce = e->order.alloc(e->n_rec);
+    if (ce == cudaSuccess) ce = e->Dq.alloc(std::max(dq, 1));
+    if (ce == cudaSuccess) ce = e->Jp.alloc(std::max(dq, 1));
+    if (ce == cudaSuccess) ce = e->key.alloc(std::max(e->n_rec, 1));
+    if (ce == cudaSuccess) ce = e->skey.alloc(std::max(e->n_rec, 1));
+    if (ce == cudaSuccess)
+        ce = cub::DeviceSegmentedRadixSort::SortPairsDescending(
+            nullptr, e->sort_bytes, e->key.p, e->skey.p, e->iota.p, e->order.p, e->n_rec, kJMaxL + 1,
+            e->seg_off.p, e->seg_off.p + 1);
+    if (ce == cudaSuccess) ce = e->sort_tmp.alloc(std::max<size_t>(e->sort_bytes, 1));
+    if (ce != cudaSuccess) {
+        *err = std::string("J-engine setup: ") + cudaGetErrorString(ce);
+        return nullptr;
+    }
+    return e.release();
+}
+
+void jengine_destroy(JEngine *e) { delete e; }
+
+int jengine_build(JEngine *e, const double *D_dev, double *J_dev, double tau, const double *boys_tab,
+                  cudaStream_t st, std::string *err, int *launches) {
+    int nl = 0;
+    auto check = [&](cudaError_t c, const char *what) {
+        if (c == cudaSuccess) return true;
+        *err = std::string(what) + ": " + cudaGetErrorString(c);
+        return false;
+    };
+    if (!check(cudaSetDevice(e->device), "cudaSetDevice")) return -2;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+    const int rec_grid = std::max(1, std::min((e->n_rec + 3) / 4, sms * 16));
+    j_dq_kernel<<<rec_grid, 128, 0, st>>>(e->recs.p, e->n_rec, D_dev, e->n_ao, e->Dq.p, e->key.p);
+    ++nl;
+    if (!check(cudaGetLastError(), "j_dq_kernel")) return -2;
+    size_t bytes = e->sort_bytes;
+    if (!check(cub::DeviceSegmentedRadixSort::SortPairsDescending(e->sort_tmp.p, bytes, e->key.p, e->skey.p,
+                                                                  e->iota.p, e->order.p, e->n_rec, kJMaxL + 1,
+                                                                  e->seg_off.p, e->seg_off.p + 1, 0,
+                                                                  (int)sizeof(double) * 8, st),
+               "segmented sort"))
+        return -2;
+    ++nl;
+    if (!check(cudaMemsetAsync(e->Jp.p, 0, e->Jp.n * sizeof(double), st), "memset")) return -2;
+    for (int lp = 0; lp <= kJMaxL; ++lp) {
+        const int b0 = e->L_off[lp], nb = e->L_off[lp + 1] - b0;
+        if (nb == 0) continue;
+        const int grid = std::max(1, std::min((nb + 3) / 4, sms * 8));
+        for (int lq = 0; lq <= kJMaxL; ++lq) {
+            const int k0 = e->L_off[lq], nk = e->L_off[lq + 1] - k0;
+            if (nk == 0) continue;
+            kPqTable[lp + lq](grid, st, e->recs.p, lp, lq, b0, nb, k0, nk, e->order.p, e->skey.p, e->Dq.p, e->Jp.p,
+                              tau, boys_tab);
+            ++nl;
+            if (!check(cudaGetLastError(), "j_pq_kernel")) return -2;
+        }
+    }
+    const int pair_grid = std::max(1, std::min((e->n_pairs + 3) / 4, sms * 16));
+    j_jab_kernel<<<pair_grid, 128, 0, st>>>(e->recs.p, e->pair_rec0.p, e->pair_nrec.p, e->n_pairs, e->Jp.p, J_dev,
+                                            e->n_ao);
+    ++nl;
+    if (!check(cudaGetLastError(), "j_jab_kernel")) return -2;
+    if (launches) *launches = nl;
+    return 0;
+}
+
+void jengine_host_lists(const HostBasis &basis, const double *D, JHostLists *out) {
+    *out = JHostLists{};
+    const int nsh = (int)basis.shells.size();
+    const int n = basis.n_ao;
+    for (int a = 0; a < nsh; ++a)
+        for (int b = 0; b <= a; ++b) {
+            const HostShell &sa = basis.shells[a], &sb = basis.shells[b];
+            const int L = sa.l + sb.l;
+            const auto hs = herm_order(L);
+            const auto ca = carts(sa.l), cb = carts(sb.l);
+            std::vector<JRec> rs;
+            std::vector<int> prim;
+            pair_records(basis, a, b, &rs, &prim);
+            const double w = a == b ? 1.0 : 2.0;
+            for (size_t k = 0; k < rs.size(); ++k) {
+                const size_t i = k / sb.exps.size(), j = k % sb.exps.size();
+                const double alpha = sa.exps[i], beta = sb.exps[j], zeta = alpha + beta;
+                const double scale = sa.coefs[i] * sb.coefs[j] * std::pow(M_PI / zeta, 1.5);
+                double P[3];
+                for (int d = 0; d < 3; ++d) P[d] = (alpha * sa.centre[d] + beta * sb.centre[d]) / zeta;
+                // D_q in make_kets' order (ao/density.py:133-141): rows of
+                // the dressed block (c outer), skipping D_cd == 0, then w.
+                std::vector<double> dq(hs.size(), 0.0);
+                int row = 0;
+                for (auto &c : ca)
+                    for (auto &d : cb) {
+                        const double x = D[(size_t)(basis.offsets[a] + row / (int)cb.size()) * n +
+                                           basis.offsets[b] + row % (int)cb.size()];
+                        ++row;
+                        if (x == 0.0) continue;
+                        double ax[3][16];
+                        int len[3];
+                        for (int dd = 0; dd < 3; ++dd) {
+                            e_axis(c[dd], d[dd], zeta, P[dd] - sa.centre[dd], P[dd] - sb.centre[dd], ax[dd]);
+                            len[dd] = c[dd] + d[dd] + 1;
+                        }
+                        for (size_t t = 0; t < hs.size(); ++t) {
+                            double v = 1.0;
+                            for (int dd = 0; dd < 3; ++dd) v = hs[t][dd] < len[dd] ? v * ax[dd][hs[t][dd]] : 0.0;
+                            dq[t] += x * (scale * v);
+                        }
+                    }
+                double dmax = 0.0;
+                for (auto &v : dq) dmax = std::max(dmax, std::fabs(w * v));
+                out->a.push_back(a);
+                out->b.push_back(b);
+                out->prim.push_back(prim[k]);
+                out->L.push_back(L);
+                out->G.push_back(rs[k].G);
+                out->key.push_back(rs[k].G * dmax);
+            }
+        }
+    out->L_off.assign(kJMaxL + 2, 0);
+    for (int L = 0; L <= kJMaxL; ++L) {
+        out->L_off[L] = (int64_t)out->ket_order.size();
+        std::vector<int32_t> idx;
+        for (size_t r = 0; r < out->L.size(); ++r)
+            if (out->L[r] == L) idx.push_back((int32_t)r);
+        std::stable_sort(idx.begin(), idx.end(),
+                         [&](int32_t x, int32_t y) { return out->key[x] > out->key[y]; });
+        out->ket_order.insert(out->ket_order.end(), idx.begin(), idx.end());
+    }
+    out->L_off[kJMaxL + 1] = (int64_t)out->ket_order.size();
+}
+
+}  // namespace fjb

@@ -73,9 +73,8 @@ double fsum(const double *x, size_t n) {
 }
 
 namespace {
-
-using Cart3 = std::array<int, 3>;
 constexpr double kPi = 3.141592653589793;
+}  // namespace
 
 std::vector<Cart3> herm_order(int L) {
     std::vector<Cart3> out;
@@ -133,8 +132,6 @@ void hermite_bounds(double zeta, int L, const std::vector<Cart3> &hs, double *I)
         I[k] = std::sqrt(s);
     }
 }
-
-}  // namespace
 
 std::vector<double> primitive_schwarz_bounds(const HostShell &sa, const HostShell &sb) {
     const double *A = sa.centre, *B = sb.centre;

@@ -1,5 +1,6 @@
 // plan.h -- the fused Fock build's pair stream (host side).
 #pragma once
+#include <array>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -47,6 +48,19 @@ struct Plan {
 
 // Correctly rounded sum (Shewchuk's partials with a round-half-even fix).
 double fsum(const double *x, size_t n);
+
+using Cart3 = std::array<int, 3>;
+
+// hermite_order(L) (mmd/hermite.py): totals 0..L, each tx desc then ty desc.
+std::vector<Cart3> herm_order(int L);
+// cartesians(l) (ao/shell.py:68): i desc, then j desc.
+std::vector<Cart3> carts(int l);
+// e_axis (mmd/hermite.py:61-79): E^{ij}_t, t = 0..i+j, with the axis's
+// Gaussian-product factor exp(zeta pa pb) in E^{00}_0.
+void e_axis(int i, int j, double zeta, double pa, double pb, double *e);
+// I_p = sqrt((-1)^|p| [2p]^(0)(PQ = 0, theta = sqrt(zeta/2))) for every p of
+// hs (ao/pairs.py:270-287), with F_M(0) = 1/(2M+1).
+void hermite_bounds(double zeta, int L, const std::vector<Cart3> &hs, double *I);
 
 // G_[ab] of every primitive pair of the ordered shell pair (a, b), in
 // primitive_pairs order (i outer).

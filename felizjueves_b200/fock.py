@@ -280,6 +280,45 @@ class FockEngine:
                                                int(precision), float(threshold)), self._h)
         return J, K, G
 
+    # -- the J-engine (eri/j_coulomb/j.py) ----------------------------------
+    def coulomb(self, D, *, tau: float = 0.0, J=None):
+        """J of the symmetric density D by the McMurchie-Davidson J-engine
+        (the reference's coulomb_matrix / coulomb_matrix_screened sweep,
+        eri/j_coulomb/j.py:436-581): a device tensor D in, a device J out
+        (written in full).  Needs no plan."""
+        import torch
+        tau = _checked_tau(tau)
+        if not isinstance(D, torch.Tensor):
+            D = torch.as_tensor(_checked_density(self.basis, D), device=f"cuda:{self.device}")
+        n = self.n_ao
+        if D.shape != (n, n) or D.dtype != torch.float64 or not D.is_contiguous():
+            raise ValueError(f"D must be a contiguous float64 ({n}, {n}) tensor")
+        if J is None:
+            J = torch.empty_like(D)
+        st = torch.cuda.current_stream(D.device).cuda_stream
+        _lib.check(self._L.fjb_coulomb(self._h, D.data_ptr(), J.data_ptr(), tau, C.c_void_p(st)), self._h)
+        return J
+
+    def j_launches(self) -> int:
+        """Kernel launches of the last `coulomb` call."""
+        return int(self._L.fjb_j_last_launches(self._h))
+
+    def j_plan_lists(self, D) -> dict[str, np.ndarray]:
+        """The J-engine's host plan for D (eri/j_coulomb/launch.py:274-327):
+        per record (sweep order) its shell pair a >= b, primitive index, L,
+        I_pair and ket key; `ket_order` the records sorted descending by key
+        per L (stable), `L_off` the offsets of each L in it."""
+        A = _checked_density(self.basis, D)
+        n = C.c_int64()
+        _lib.check(self._L.fjb_j_plan_lists(self._h, A.ctypes.data, None, C.byref(n)), self._h)
+        m = int(n.value)
+        out = {k: np.empty(m, np.int32) for k in ("a", "b", "prim", "L", "ket_order")}
+        out.update(G=np.empty(m), key=np.empty(m), L_off=np.empty(8, np.int64))
+        lst = _lib.JLists_t(*(out[k].ctypes.data for k in ("a", "b", "prim", "L", "G", "key",
+                                                             "ket_order", "L_off")))
+        _lib.check(self._L.fjb_j_plan_lists(self._h, A.ctypes.data, C.byref(lst), C.byref(n)), self._h)
+        return out
+
     def last_build_stats(self) -> tuple[float, int]:
         ms, nl = C.c_double(), C.c_int()
         _lib.check(self._L.fjb_last_build_stats(self._h, C.byref(ms), C.byref(nl)), self._h)
@@ -359,6 +398,18 @@ def fock_two_electron(basis: Basis, D, *, tau: float = 0.0, n: int = 4, device: 
     eng = FockEngine(basis, device)
     eng.plan(D, tau, n)
     return eng.build_host(D)[2]
+
+
+def coulomb_matrix(basis: Basis, D, *, tau: float = 0.0, device: int = 0) -> np.ndarray:
+    """J_mn of the symmetric density D (numpy) by the J-engine on the GPU:
+    the reference's coulomb_matrix (eri/j_coulomb/j.py:436-450) at tau = 0,
+    its screened sweep (j.py:538-581) at tau > 0."""
+    import torch
+    eng = FockEngine(basis, device)
+    Dt = torch.as_tensor(_checked_density(basis, D), device=f"cuda:{device}")
+    J = eng.coulomb(Dt, tau=tau)
+    torch.cuda.synchronize(Dt.device)
+    return J.cpu().numpy()
 
 
 def eri_block(basis: Basis, a: int, b: int, c: int, d: int, device: int = 0) -> np.ndarray:

@@ -30,6 +30,14 @@
  *   fjb_eri_blocks    eri/eri.py:133-145 eri_block and
  *                     eri/hgp_drive.py:206 (the per-quartet ERI tap)
  *   fjb_boys          emit/_c.py:144-210 fj_boys<M> (device Boys)
+ *   fjb_coulomb       eri/j_coulomb/j.py:436-450 coulomb_matrix(basis, D, *,
+ *                                            pq, tau) and its screened sweep
+ *                                            j.py:538-581 (the MMD J-engine:
+ *                                            kernel_dq.py, mmd/kernel.py,
+ *                                            kernel_jab.py)
+ *   fjb_j_plan_lists  eri/j_coulomb/launch.py:274-327 launches(): the
+ *                                            records, bounds, keys and the
+ *                                            sorted ket order
  *   fjb_last_error,
  *   fjb_destroy       the reference raises ValueError with a message
  *
@@ -208,6 +216,31 @@ int fjb_route_stats(const fjb_handle *h, int64_t *units_fp32, int64_t *units_fp6
 /* Device Boys F_0..F_m(T[i]) for n arguments into F_dev[i*(m+1) + k]
  * (DEVICE pointers).  Synchronises. */
 int fjb_boys(int m, const double *T_dev, int n, double *F_dev);
+
+/* J by the McMurchie-Davidson J-engine: J_dev (n_ao^2, DEVICE) from the
+ * symmetric density D_dev at threshold tau (>= 0; 0 screens nothing), the
+ * reference's unique sweep with the ket weight 2 off the diagonal and the
+ * sorted break on I_bra * (I_ket * max|D_q|) < tau.  Every element of J_dev
+ * is written (no accumulation into it).  Stream-ordered; the first call
+ * stages the records (allocates), later calls allocate nothing and can be
+ * captured in a CUDA graph. */
+int fjb_coulomb(fjb_handle *h, const double *D_dev, double *J_dev, double tau, void *stream);
+/* Kernel launches of the last fjb_coulomb. */
+int fjb_j_last_launches(const fjb_handle *h);
+
+/* The J-engine's plan on the host for density D_host: per record (sweep
+ * order: shell pairs a >= b, a outer; primitive pairs i outer) its shell
+ * pair, primitive index i*K_b + j, L, I_pair and ket key I_pair*max|D_q|;
+ * the ket order per L (descending key, stable) with L_off[2*FJB_MAX_L + 2]
+ * offsets into it.  Caller-allocated arrays of *n_records entries; with
+ * out == NULL only *n_records is set.  Host-only handles allowed. */
+typedef struct fjb_j_lists {
+    int32_t *a, *b, *prim, *L;
+    double *G, *key;
+    int32_t *ket_order;
+    int64_t *L_off;
+} fjb_j_lists;
+int fjb_j_plan_lists(const fjb_handle *h, const double *D_host, fjb_j_lists *out, int64_t *n_records);
 
 /* Elapsed device milliseconds of the last fjb_fock_build's class kernels
  * (events recorded on the build's stream); and the number of kernel

@@ -9,7 +9,7 @@ files this script writes.
 
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
-parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost (default: all
+parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost jplan_c0 (default: all
 but plan_c1 and jk_small, which take minutes).
 """
 
@@ -383,6 +383,35 @@ def part_jk_small():
         print("jk", name, w.n_ao, "J", round(tj, 1), "s K", round(tk, 1), "s")
 
 
+# --- the J-engine's launch plan (eri/j_coulomb/launch.py:274-327) on c0 -----
+
+
+def part_jplan_c0():
+    _ref_imports()
+    from felizjueves.eri.j_coulomb import j as JJ
+    from felizjueves.eri.j_coulomb import launch as JL
+    from felizjueves.reference.pq import pq
+    from felizjueves_b200 import configs
+    w = configs.c0()
+    rb = ref_basis(w.basis)
+    t = time.time()
+    plan = JL.launches(rb, w.D.tolist(), bound=lambda z, L: JJ.pair_bound_pq(z, L, pq=pq),
+                       n_batches=1, tau=w.tau)
+    bras, kets = {}, {}
+    for c in plan:
+        bras[c.lp] = c.bras
+        kets[c.lq] = c.kets
+    out = {"tau": w.tau}
+    for L, recs in bras.items():
+        out[f"bra{L}_ijp"] = np.array([(r.i, r.j, r.prim) for r in recs], np.int32)
+        out[f"bra{L}_G"] = np.array([r.G for r in recs])
+    for L, recs in kets.items():
+        out[f"ket{L}_ijp"] = np.array([(r.i, r.j, r.prim) for r in recs], np.int32)
+        out[f"ket{L}_key"] = np.array([r.key for r in recs])
+    np.savez_compressed(os.path.join(HERE, "jplan_c0.npz"), **out)
+    print("jplan_c0", sum(len(v) for v in bras.values()), "records,", round(time.time() - t, 1), "s")
+
+
 # --- the reference's FLOP model (hgp/cost.py) for every class to L=3 ---------
 
 
@@ -417,8 +446,8 @@ def part_cost():
 PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_eri,
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "jk_small": part_jk_small,
-         "cost": part_cost}
-DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri"]
+         "cost": part_cost, "jplan_c0": part_jplan_c0}
+DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0"]
 
 
 def main():
