@@ -14,7 +14,9 @@
 //                    max_q |D_q| (ao/density.py:120-148, launch.py:300-310).
 //   segmented radix sort (CUB) of the keys, descending and stable, one
 //                    segment per L: the ket order of launch.py:325.
-//   j_pq_kernel<LP, LQ>  one launch per (bra L, ket L) class: a warp per bra
+//   j_pq_small_kernel<LP, LQ> (lp + lq <= 6: every Hermite index a template
+//   constant, R in registers) / j_pq_kernel<L> (the rest, table-indexed)
+//                    one launch per (bra L, ket L) class: a warp per bra
 //                    record walks the class's sorted kets 32 at a time, one
 //                    lane per ket, and stops after the chunk holding the
 //                    first ket with I_bra * key < tau (the sorted break,
@@ -142,6 +144,159 @@ __global__ void j_dq_kernel(const JRec *__restrict__ recs, int n, const double *
 __device__ __forceinline__ int h_index(int t, int u, int v) {
     const int n = t + u + v;
     return (n == 0 ? 0 : nh(n - 1)) + (n - t) * (n - t + 1) / 2 + (n - t - u);
+}
+
+// hermite_order index -> (t, u, v), constexpr, for the unrolled kernels.
+__host__ __device__ constexpr int hc_total(int idx) {
+    int n = 0;
+    while (nh(n) <= idx) ++n;
+    return n;
+}
+__host__ __device__ constexpr int hc_t(int idx) {
+    const int n = hc_total(idx);
+    int r = idx - (n == 0 ? 0 : nh(n - 1)), t = n;
+    while (r >= n - t + 1) {
+        r -= n - t + 1;
+        --t;
+    }
+    return t;
+}
+__host__ __device__ constexpr int hc_u(int idx) {
+    const int n = hc_total(idx);
+    int r = idx - (n == 0 ? 0 : nh(n - 1)), t = n;
+    while (r >= n - t + 1) {
+        r -= n - t + 1;
+        --t;
+    }
+    return n - t - r;
+}
+__host__ __device__ constexpr int hc_v(int idx) { return hc_total(idx) - hc_t(idx) - hc_u(idx); }
+__host__ __device__ constexpr int hc_idx(int t, int u, int v) {
+    const int n = t + u + v;
+    return (n == 0 ? 0 : nh(n - 1)) + (n - t) * (n - t + 1) / 2 + (n - t - u);
+}
+
+// Compile-time walks of the small classes: every index below is a template
+// constant (fold expressions over integer sequences), so R, the signed D_q
+// and the J_p partials stay in registers.
+// One entry I of the R recursion: [r]^(m) = PQ_d [r-1_d]^(m+1) + (r_d - 1)
+// [r-2_d]^(m+1), d the first nonzero axis.
+template <int I>
+__device__ __forceinline__ void r_entry(double *R, double X, double Y, double Z) {
+    constexpr int t = hc_t(I), u = hc_u(I), v = hc_v(I);
+    if constexpr (t > 0) {
+        double x = X * R[hc_idx(t - 1, u, v)];
+        if constexpr (t >= 2) x += (double)(t - 1) * R[hc_idx(t - 2, u, v)];
+        R[I] = x;
+    } else if constexpr (u > 0) {
+        double x = Y * R[hc_idx(0, u - 1, v)];
+        if constexpr (u >= 2) x += (double)(u - 1) * R[hc_idx(0, u - 2, v)];
+        R[I] = x;
+    } else {
+        double x = Z * R[hc_idx(0, 0, v - 1)];
+        if constexpr (v >= 2) x += (double)(v - 1) * R[hc_idx(0, 0, v - 2)];
+        R[I] = x;
+    }
+}
+template <int I0, int... K>
+__device__ __forceinline__ void r_entries(double *R, double X, double Y, double Z, std::integer_sequence<int, K...>) {
+    (r_entry<I0 + K>(R, X, Y, Z), ...);
+}
+// Totals S, S-1, .. 1 of one level (descending: each reads the level above
+// at totals S-1 and S-2 before they are rewritten).
+template <int S>
+struct RTotals {
+    static __device__ __forceinline__ void run(double *R, double X, double Y, double Z) {
+        if constexpr (S >= 1) {
+            r_entries<nh(S - 1)>(R, X, Y, Z, std::make_integer_sequence<int, nh(S) - nh(S - 1)>{});
+            RTotals<S - 1>::run(R, X, Y, Z);
+        }
+    }
+};
+// Levels M, M-1, .. 0 of R_{tuv} at total order L.
+template <int L, int M>
+struct RLevels {
+    static __device__ __forceinline__ void run(double *R, const double *f, double X, double Y, double Z) {
+        if constexpr (M >= 0) {
+            RTotals<L - M>::run(R, X, Y, Z);
+            R[0] = f[M];
+            RLevels<L, M - 1>::run(R, f, X, Y, Z);
+        }
+    }
+};
+// d[q] = (-1)^|q| D_q.
+template <int... Q>
+__device__ __forceinline__ void signed_dq(double *d, const double *dq, std::integer_sequence<int, Q...>) {
+    ((d[Q] = ((hc_total(Q) & 1) ? -1.0 : 1.0) * __ldg(dq + Q)), ...);
+}
+// jp[p] += R_{p+q} d[q] over I = p * NQ + q.
+template <int NQ, int I>
+struct PQIndex {
+    static constexpr int pi = I / NQ, qi = I % NQ;
+    static constexpr int r = hc_idx(hc_t(pi) + hc_t(qi), hc_u(pi) + hc_u(qi), hc_v(pi) + hc_v(qi));
+};
+template <int NQ, int... I>
+__device__ __forceinline__ void contract(double *jp, const double *R, const double *d,
+                                         std::integer_sequence<int, I...>) {
+    ((jp[PQIndex<NQ, I>::pi] += R[PQIndex<NQ, I>::r] * d[PQIndex<NQ, I>::qi]), ...);
+}
+
+// The classes with lp + lq <= kSmallL: the same walk as j_pq_kernel with
+// every index a compile-time constant.
+constexpr int kSmallL = 6;
+
+template <int LP, int LQ>
+__global__ void __launch_bounds__(128) j_pq_small_kernel(const JRec *__restrict__ recs, int bra0, int nbra,
+                                                         int ket0, int nket, const int *__restrict__ order,
+                                                         const double *__restrict__ skey,
+                                                         const double *__restrict__ Dq, double *__restrict__ Jp,
+                                                         double tau, const double *__restrict__ boys_tab) {
+    constexpr int L = LP + LQ, NP = nh(LP), NQ = nh(LQ), NR = nh(L);
+    constexpr double kTwoOverSqrtPi = 1.1283791670955126;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int bi = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); bi < nbra; bi += nw) {
+        const JRec B = recs[bra0 + bi];
+        double jp[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) jp[p] = 0.0;
+        for (int k0 = 0; k0 < nket; k0 += 32) {
+            const int k = k0 + lane;
+            const bool on = k < nket && !(B.G * skey[ket0 + k] < tau);
+            if (on) {
+                const JRec K = recs[order[ket0 + k]];
+                const double p = B.zeta, q = K.zeta;
+                const double rho = p * q / (p + q);
+                const double X = B.P[0] - K.P[0], Y = B.P[1] - K.P[1], Z = B.P[2] - K.P[2];
+                const double T = rho * (X * X + Y * Y + Z * Z);
+                double F[L + 1];
+                boys_t<L>(T, F, boys_tab);
+                const double pref = kTwoOverSqrtPi * sqrt(rho), m2r = -2.0 * rho;
+                double f[L + 1];
+                double pw = pref;
+#pragma unroll
+                for (int m = 0; m <= L; ++m) {
+                    f[m] = pw * F[m];
+                    pw *= m2r;
+                }
+                double R[NR];
+                R[0] = f[L];
+                RLevels<L, L - 1>::run(R, f, X, Y, Z);
+                double d[NQ];
+                signed_dq(d, Dq + K.dq_off, std::make_integer_sequence<int, NQ>{});
+                contract<NQ>(jp, R, d, std::make_integer_sequence<int, NP * NQ>{});
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, on);
+            if (__popc(bal) < min(32, nket - k0)) break;  // the first ket under tau is in this chunk
+        }
+#pragma unroll
+        for (int pi = 0; pi < NP; ++pi) {
+            double v = jp[pi];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) Jp[B.dq_off + pi] += v;
+        }
+    }
 }
 
 // One (bra L, ket L) class at total order L = lp + lq (runtime lp, lq).
@@ -278,6 +433,29 @@ constexpr std::array<PqLaunch, sizeof...(L)> pq_table(std::integer_sequence<int,
     return {&pq_launch<L>...};
 }
 const auto kPqTable = pq_table(std::make_integer_sequence<int, 2 * kJMaxL + 1>{});
+
+using PqSmallLaunch = void (*)(int grid, cudaStream_t st, const JRec *, int, int, int, int, const int *,
+                               const double *, const double *, double *, double, const double *);
+
+template <int LP, int LQ>
+void pq_small_launch(int grid, cudaStream_t st, const JRec *recs, int bra0, int nbra, int ket0, int nket,
+                     const int *order, const double *skey, const double *Dq, double *Jp, double tau,
+                     const double *boys) {
+    if constexpr (LP + LQ <= kSmallL)
+        j_pq_small_kernel<LP, LQ><<<grid, 128, 0, st>>>(recs, bra0, nbra, ket0, nket, order, skey, Dq, Jp, tau,
+                                                        boys);
+}
+
+template <int LP, int... LQ>
+constexpr std::array<PqSmallLaunch, sizeof...(LQ)> pq_small_row(std::integer_sequence<int, LQ...>) {
+    return {&pq_small_launch<LP, LQ>...};
+}
+template <int... LP>
+constexpr std::array<std::array<PqSmallLaunch, kJMaxL + 1>, sizeof...(LP)> pq_small_table(
+    std::integer_sequence<int, LP...>) {
+    return {pq_small_row<LP>(std::make_integer_sequence<int, kJMaxL + 1>{})...};
+}
+const auto kPqSmall = pq_small_table(std::make_integer_sequence<int, kJMaxL + 1>{});
 
 template <typename T>
 struct DBuf {
@@ -451,8 +629,12 @@ int jengine_build(JEngine *e, const double *D_dev, double *J_dev, double tau, co
         for (int lq = 0; lq <= kJMaxL; ++lq) {
             const int k0 = e->L_off[lq], nk = e->L_off[lq + 1] - k0;
             if (nk == 0) continue;
-            kPqTable[lp + lq](grid, st, e->recs.p, lp, lq, b0, nb, k0, nk, e->order.p, e->skey.p, e->Dq.p, e->Jp.p,
-                              tau, boys_tab);
+            if (lp + lq <= kSmallL)
+                kPqSmall[lp][lq](grid, st, e->recs.p, b0, nb, k0, nk, e->order.p, e->skey.p, e->Dq.p, e->Jp.p, tau,
+                                 boys_tab);
+            else
+                kPqTable[lp + lq](grid, st, e->recs.p, lp, lq, b0, nb, k0, nk, e->order.p, e->skey.p, e->Dq.p,
+                                  e->Jp.p, tau, boys_tab);
             ++nl;
             if (!check(cudaGetLastError(), "j_pq_kernel")) return -2;
         }
