@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libfjb.so")
 
 FJB_FP64 = 0
 FJB_ROUTED = 1
+FJB_FP64_SCATTER = 2  # FP64 without atomics: slot buffer + ordered per-element scatter
 
 _ERRORS = {-1: ValueError, -2: RuntimeError, -3: RuntimeError, -4: ValueError,
            -5: TimeoutError, -6: ValueError}
@@ -91,6 +92,7 @@ def load():
     L.fjb_coulomb.argtypes = [vp, vp, vp, dbl, vp]
     L.fjb_j_last_launches.argtypes = [vp]
     L.fjb_j_plan_lists.argtypes = [vp, vp, C.POINTER(JLists_t), C.POINTER(i64)]
+    L.fjb_scatter_map.argtypes = [vp, C.c_int, vp, vp, vp, C.POINTER(i64), C.POINTER(i64)]
     _lib = L
     return L
 
@@ -103,7 +105,7 @@ EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_
            "fjb_fock_build_graph", "fjb_create_df", "fjb_df_blocks", "fjb_mlp_n_params",
            "fjb_router_set", "fjb_router_features", "fjb_mlp_forward", "fjb_mlp_gradient",
            "fjb_mlp_adam", "fjb_route_stats", "fjb_coulomb", "fjb_j_last_launches",
-           "fjb_j_plan_lists")
+           "fjb_j_plan_lists", "fjb_scatter_map")
 
 
 class LaunchStat_t(C.Structure):

@@ -26,6 +26,7 @@
 #include "hgp_tables.h"
 #include "jengine.h"
 #include "plan.h"
+#include "scatter.h"
 #include "router.cuh"
 
 namespace fjb {
@@ -72,6 +73,51 @@ __global__ void close_kernel(const double *__restrict__ Jp, const double *__rest
     if (J) J[ij] = jv;
     if (K) K[ij] = kv;
     if (G) G[ij] = jv - 0.5 * kv;
+}
+
+// The atomics-free build (scatter.h).  A bra segment is one bra pair of one
+// launch: its units' partial bra blocks are summed in unit order into the
+// segment's bra-block slots.
+struct BraSeg {
+    int64_t slot;     // the launch's first slot + ib * row
+    int64_t wab0;     // the first unit's partial in wab
+    int32_t n_units;  // consecutive units, each nab partials
+    int32_t nab;
+};
+
+__global__ void bra_reduce_kernel(const BraSeg *segs, int n_segs, const double *wab, double *W) {
+    for (int s = blockIdx.x; s < n_segs; s += gridDim.x) {
+        const BraSeg S = segs[s];
+        for (int e = threadIdx.x; e < S.nab; e += blockDim.x) {
+            double v = 0.0;
+            for (int u = 0; u < S.n_units; ++u) v += wab[S.wab0 + (int64_t)u * S.nab + e];
+            W[S.slot + e] = v;
+        }
+    }
+}
+
+// One launch's scatter (kernel_f_scatter.py:1-30): a thread per element of
+// J' / K' the launch touches sums that element's slots in ascending slot
+// order, J' and K' apart (a slot's block, from its position in its row,
+// says which: the bra block and cd are J', the other four K'), then one
+// plain add per matrix.  Deterministic; no atomics.
+__global__ void slot_scatter_kernel(const int32_t *el, const int32_t *ptr, const int32_t *src, int n_el,
+                                    const double *W, int row, int n_ab, int n_ket, int n_cd, double *Jp,
+                                    double *Kp, int n_ao) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_el) return;
+    double sj = 0.0, sk = 0.0;
+    for (int t = ptr[e]; t < ptr[e + 1]; ++t) {
+        const int s = src[t];
+        const int off = s % row;
+        if (off < n_ab || (off - n_ab) / n_ket < n_cd)
+            sj += W[s];
+        else
+            sk += W[s];
+    }
+    const size_t x = (size_t)el[2 * e] * n_ao + el[2 * e + 1];
+    Jp[x] += sj;
+    Kp[x] += sk;
 }
 
 __global__ void boys_kernel(int M, const double *T, int n, double *F, const double *tab) {
@@ -485,8 +531,45 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                     const int n1 = nab, n2 = n1 + ncd, n3 = n2 + na * nc, n4 = n3 + na * nd,
                               n5 = n4 + nb * nc, n6 = n5 + nb * nd;
                     const double w2 = 2.0 * deg;
+                    // the atomics-free build: the five ket blocks (this
+                    // order, n2..n6) into the quartet's own slots
+                    double *wq = A.W ? ket_slots(A, U.launch, LR.n_ket, U.ib, ik, nab, n6 - n1) : nullptr;
                     for (int o = tid; o < n6; o += nt) {
                         double acc = 0.0;
+                        if (o >= n1 && wq) {
+                            const int e = o - n1;
+                            if (o < n2) {
+                                const int kl = o - n1;
+                                for (int ij = 0; ij < nab; ++ij) acc += Dab[ij] * Y[(size_t)ij * ncd + kl];
+                                acc *= w2;
+                            } else if (o < n3) {
+                                const int r = o - n2, i = r / nc, k = r % nc;
+                                for (int j = 0; j < nb; ++j)
+                                    for (int l = 0; l < nd; ++l)
+                                        acc += Dbd[j * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                                acc *= deg;
+                            } else if (o < n4) {
+                                const int r = o - n3, i = r / nd, l = r % nd;
+                                for (int j = 0; j < nb; ++j)
+                                    for (int k = 0; k < nc; ++k)
+                                        acc += Dbc[j * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                                acc *= deg;
+                            } else if (o < n5) {
+                                const int r = o - n4, j = r / nc, k = r % nc;
+                                for (int i = 0; i < na; ++i)
+                                    for (int l = 0; l < nd; ++l)
+                                        acc += Dad[i * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                                acc *= deg;
+                            } else {
+                                const int r = o - n5, j = r / nd, l = r % nd;
+                                for (int i = 0; i < na; ++i)
+                                    for (int k = 0; k < nc; ++k)
+                                        acc += Dac[i * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
+                                acc *= deg;
+                            }
+                            wq[(size_t)e * LR.n_ket] = acc;
+                            continue;
+                        }
                         if (o < n1) {
                             const R *y = Y + (size_t)o * ncd;
                             for (int kl = 0; kl < ncd; ++kl) acc += Dcd[kl] * y[kl];
@@ -525,7 +608,9 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                 __syncthreads();
             }
         }
-        if (!tap)
+        if (!tap && A.W)
+            for (int i = tid; i < nab; i += nt) A.wab[A.wab_off[u] + i] = Jab[i];  // reduced in unit order
+        else if (!tap)
             for (int i = tid; i < nab; i += nt)
                 atomicAdd(A.Jp + (size_t)(bra.ao_a + i / nb) * n_ao + bra.ao_b + i % nb, Jab[i]);
         if (A.computed && tid == 0 && n_list)
@@ -701,6 +786,21 @@ struct fjb_handle {
     std::vector<ClassRun> runs;
     int64_t quartets_launched = 0;
     int n_units = 0;
+    // host copies the atomics-free build's maps are made from
+    std::vector<Unit> units_host;
+    std::vector<LaunchRec> lr_host;
+    std::vector<PairRec> pr_host;
+    // the atomics-free build (FJB_FP64_SCATTER), staged on its first use
+    struct LaunchScatter {
+        int64_t el0, ptr0, src0, w0;
+        int n_el, row, n_ab, n_ket, n_cd;
+    };
+    bool scatter_ready = false;
+    std::vector<LaunchScatter> lsc;
+    DevBuf<double> W, wab;
+    DevBuf<int64_t> w_base, wab_off;
+    DevBuf<int32_t> sc_el, sc_ptr, sc_src;
+    DevBuf<BraSeg> segs;
     // build scratch
     DevBuf<double> Dsh, Jp, Kp;
     DevBuf<double> hD, hJ, hK, hG;  // fjb_fock_build_host staging
@@ -836,6 +936,84 @@ int run_grid32(const ClassRun &r) {
     const int per_sm = std::max(1, compiled_blocks_per_sm(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, true));
     const int warps_needed = (r.n_units + 3) / 4;
     return std::max(1, std::min(warps_needed, per_sm * sm_count()));
+}
+
+// The atomics-free build's maps and buffers (scatter.h), staged once per
+// plan: the per-launch CSR maps, the slot buffer W, the per-unit bra-block
+// partials and the bra segments that reduce them.  Refused when the slots
+// exceed kScatterMaxSlots (2 GiB of W).
+constexpr int64_t kScatterMaxSlots = int64_t(1) << 28;
+
+int ensure_scatter(fjb_handle *h) {
+    if (h->scatter_ready) return FJB_OK;
+    std::vector<int32_t> el, ptr, src;
+    std::vector<int64_t> w_base;
+    h->lsc.clear();
+    int64_t w = 0;
+    try {
+        for (size_t li = 0; li < h->lr_host.size(); ++li) {
+            const LaunchRec &L = h->lr_host[li];
+            const fjb_launch_stat &ls = h->lstat[li];
+            const int l[4] = {ls.la, ls.lb, ls.lc, ls.ld};
+            std::vector<std::pair<int, int>> bra_ao, ket_ao;
+            for (int i = 0; i < L.n_bra; ++i)
+                bra_ao.emplace_back(h->pr_host[L.bra_pair0 + i].ao_a, h->pr_host[L.bra_pair0 + i].ao_b);
+            for (int k = 0; k < L.n_ket; ++k)
+                ket_ao.emplace_back(h->pr_host[L.ket_pair0 + k].ao_a, h->pr_host[L.ket_pair0 + k].ao_b);
+            const ScatterMap m = scatter_map(l, bra_ao, ket_ao);
+            const SlotShape S = slot_shape(l);
+            fjb_handle::LaunchScatter e{};
+            e.el0 = (int64_t)el.size() / 2;
+            e.ptr0 = (int64_t)ptr.size();
+            e.src0 = (int64_t)src.size();
+            e.w0 = w;
+            e.n_el = (int)m.n_el;
+            e.row = S.n_ab + S.s5 * L.n_ket;
+            e.n_ab = S.n_ab;
+            e.n_ket = L.n_ket;
+            e.n_cd = S.n_cd;
+            h->lsc.push_back(e);
+            w_base.push_back(w);
+            w += m.n_slot;
+            if (w > kScatterMaxSlots)
+                return fail(h, FJB_E_LIMIT, "the atomics-free build needs more than 2^28 slots; use FJB_FP64");
+            el.insert(el.end(), m.el.begin(), m.el.end());
+            ptr.insert(ptr.end(), m.ptr.begin(), m.ptr.end());
+            src.insert(src.end(), m.src.begin(), m.src.end());
+        }
+        // per unit its bra-block partial; per (launch, bra) its segment
+        std::vector<int64_t> wab_off;
+        std::vector<BraSeg> segs;
+        int64_t at = 0;
+        for (size_t u = 0; u < h->units_host.size(); ++u) {
+            const Unit &U = h->units_host[u];
+            const fjb_launch_stat &ls = h->lstat[U.launch];
+            const int nab = (ls.la + 1) * (ls.la + 2) / 2 * ((ls.lb + 1) * (ls.lb + 2) / 2);
+            wab_off.push_back(at);
+            const bool same = u > 0 && h->units_host[u - 1].launch == U.launch && h->units_host[u - 1].ib == U.ib;
+            if (same) {
+                ++segs.back().n_units;
+            } else {
+                const auto &e = h->lsc[U.launch];
+                segs.push_back(BraSeg{e.w0 + (int64_t)U.ib * e.row, at, 1, nab});
+            }
+            at += nab;
+        }
+        h->W.alloc(std::max<int64_t>(w, 1));
+        h->wab.alloc(std::max<int64_t>(at, 1));
+        h->w_base.upload(w_base);
+        h->wab_off.upload(wab_off);
+        h->sc_el.upload(el);
+        h->sc_ptr.upload(ptr);
+        h->sc_src.upload(src);
+        h->segs.upload(segs);
+    } catch (const std::length_error &e) {
+        return fail(h, FJB_E_LIMIT, e.what());
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, e.what());
+    }
+    h->scatter_ready = true;
+    return FJB_OK;
 }
 
 int ensure_smem_attr(fjb_handle *h) {
@@ -1031,8 +1209,12 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     }
     std::vector<Unit> units;
     h->runs.clear();
+    h->scatter_ready = false;
+    h->lr_host = lr;
+    h->pr_host = pr;
     if (h->device < 0) {  // host-only: the lists are complete, nothing is staged
         for (auto &kv : by_class) units.insert(units.end(), kv.second.begin(), kv.second.end());
+        h->units_host = units;
         h->quartets_launched = qbase;
         h->n_units = (int)units.size();
         h->planned = true;
@@ -1064,6 +1246,7 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
         h->prims.upload(pm);
         h->launches.upload(lr);
         h->units.upload(units);
+        h->units_host = units;
         const size_t nn = (size_t)h->basis.n_ao * h->basis.n_ao;
         const size_t ns = h->basis.shells.size();
         h->Dsh.alloc(ns * ns);
@@ -1207,10 +1390,14 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
                    int precision, double threshold, void *stream) {
     if (!h || !D_dev) return fail(h, FJB_E_ARG, "null argument");
     if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
-    if (precision != FJB_FP64 && precision != FJB_ROUTED) return fail(h, FJB_E_ARG, "unknown precision mode");
+    if (precision != FJB_FP64 && precision != FJB_ROUTED && precision != FJB_FP64_SCATTER)
+        return fail(h, FJB_E_ARG, "unknown precision mode");
     const double route = precision == FJB_ROUTED ? (threshold > 0.0 ? threshold : 1e-9) : 0.0;
     if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
     cudaSetDevice(h->device);
+    const bool scatter = precision == FJB_FP64_SCATTER;
+    if (scatter)
+        if (int rc = ensure_scatter(h)) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     const int nsh = (int)h->basis.shells.size(), nao = h->basis.n_ao;
     const size_t nn = (size_t)nao * nao;
@@ -1224,6 +1411,10 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
     const bool routed = route > 0.0;
     h->last_routed = routed;
     if (routed) CUDA_OK(h, cudaMemsetAsync(h->route_counts.p, 0, h->route_counts.n * sizeof(int), st));
+    if (scatter) {  // unwritten slots (screened quartets, the canonical half) must hold zero
+        CUDA_OK(h, cudaMemsetAsync(h->W.p, 0, h->W.n * sizeof(double), st));
+        CUDA_OK(h, cudaMemsetAsync(h->wab.p, 0, h->wab.n * sizeof(double), st));
+    }
     // Under stream capture the timing events become event-record nodes of
     // the graph (External), so every replay records them and the class and
     // build timings read after a replay are that replay's.
@@ -1251,6 +1442,12 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
         a.Kp = h->Kp.p;
         a.boys_tab = h->boys.p;
         a.route_thresh = route;
+        if (scatter) {
+            a.W = h->W.p;
+            a.w_base = h->w_base.p;
+            a.wab = h->wab.p;
+            a.wab_off = h->wab_off.p + r.unit0;
+        }
         if (routed) {
             // the precision router splits the class's units into an FP32 and
             // an FP64 queue; each queue has its own kernel
@@ -1281,6 +1478,21 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
         }
         CUDA_OK(h, cudaEventRecordWithFlags(h->cev[ri].second, st, ev_flags));
     }
+    if (scatter) {
+        // the bra blocks' partials in unit order, then each launch's scatter
+        // in launch order: J' and K' are the same sums in the same order on
+        // every build
+        const int ns = (int)h->segs.n;
+        bra_reduce_kernel<<<std::max(1, std::min(ns, 148 * 16)), 128, 0, st>>>(h->segs.p, ns, h->wab.p, h->W.p);
+        ++launches;
+        for (const auto &e : h->lsc) {
+            if (e.n_el == 0) continue;
+            slot_scatter_kernel<<<(e.n_el + 127) / 128, 128, 0, st>>>(
+                h->sc_el.p + 2 * e.el0, h->sc_ptr.p + e.ptr0, h->sc_src.p + e.src0, e.n_el, h->W.p + e.w0, e.row,
+                e.n_ab, e.n_ket, e.n_cd, h->Jp.p, h->Kp.p, nao);
+            ++launches;
+        }
+    }
     h->built = true;
     CUDA_OK(h, cudaEventRecordWithFlags(h->ev1, st, ev_flags));
     close_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(h->Jp.p, h->Kp.p, nao, J_dev, K_dev, G_dev);
@@ -1296,6 +1508,8 @@ int fjb_fock_build_graph(fjb_handle *h, const double *D_dev, double *J_dev, doub
     if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
     if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
     CUDA_OK(h, cudaSetDevice(h->device));
+    if (precision == FJB_FP64_SCATTER)  // staging allocates: before the capture
+        if (int rc = ensure_scatter(h)) return rc;
     const void *sig[4] = {D_dev, J_dev, K_dev, G_dev};
     const bool same = h->gexec && std::equal(sig, sig + 4, h->g_sig) && h->g_prec == precision &&
                       h->g_thr == threshold;
@@ -1542,6 +1756,34 @@ int fjb_df_blocks(fjb_handle *h, int kind, const int32_t *items, int n, double *
         }
     }
     return fjb_eri_blocks(h, q.data(), n, out_dev, offsets);
+}
+
+int fjb_scatter_map(const fjb_handle *hc, int launch, int32_t *el, int32_t *ptr, int32_t *src, int64_t *n_el,
+                    int64_t *n_slot) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h || !n_el || !n_slot) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
+    if (launch < 0 || launch >= (int)h->lr_host.size()) return fail(h, FJB_E_ARG, "launch index out of range");
+    const LaunchRec &L = h->lr_host[launch];
+    const fjb_launch_stat &ls = h->lstat[launch];
+    const int l[4] = {ls.la, ls.lb, ls.lc, ls.ld};
+    std::vector<std::pair<int, int>> bra_ao, ket_ao;
+    for (int i = 0; i < L.n_bra; ++i)
+        bra_ao.emplace_back(h->pr_host[L.bra_pair0 + i].ao_a, h->pr_host[L.bra_pair0 + i].ao_b);
+    for (int k = 0; k < L.n_ket; ++k)
+        ket_ao.emplace_back(h->pr_host[L.ket_pair0 + k].ao_a, h->pr_host[L.ket_pair0 + k].ao_b);
+    ScatterMap m;
+    try {
+        m = scatter_map(l, bra_ao, ket_ao);
+    } catch (const std::length_error &e) {
+        return fail(h, FJB_E_LIMIT, e.what());
+    }
+    *n_el = m.n_el;
+    *n_slot = m.n_slot;
+    if (el) std::copy(m.el.begin(), m.el.end(), el);
+    if (ptr) std::copy(m.ptr.begin(), m.ptr.end(), ptr);
+    if (src) std::copy(m.src.begin(), m.src.end(), src);
+    return FJB_OK;
 }
 
 int fjb_coulomb(fjb_handle *h, const double *D_dev, double *J_dev, double tau, void *stream) {

@@ -80,7 +80,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 // type R.  jab[] collects this lane's share of the bra block (FP64).
 template <int LA, int LB, int LC, int LD, typename R>
 __device__ __forceinline__ void quartet_compiled(const KArgs &A, const PairRec &bra, const PairRec &ket,
-                                                 double deg, double *jab) {
+                                                 double deg, double *jab, double *wq, int wstride) {
     using H = HgpCode<LA, LB, LC, LD>;
     constexpr int NA = cnc(LA), NB = cnc(LB), NC = cnc(LC), ND = cnc(LD);
     constexpr int NAB = NA * NB, NCD = NC * ND, L = LA + LB + LC + LD;
@@ -191,6 +191,21 @@ __device__ __forceinline__ void quartet_compiled(const KArgs &A, const PairRec &
             jab[i * NB + j] += 2.0 * deg * sab;
         }
     const double w2 = 2.0 * deg;
+    if (wq) {
+        // the atomics-free build: each contribution into its own slot
+        constexpr int KAC = NCD, KAD = KAC + NA * NC, KBC = KAD + NA * ND, KBD = KBC + NB * NC;
+#pragma unroll
+        for (int t = 0; t < NCD; ++t) wq[(size_t)t * wstride] = w2 * jcd[t];
+#pragma unroll
+        for (int t = 0; t < NA * NC; ++t) wq[(size_t)(KAC + t) * wstride] = deg * kac[t];
+#pragma unroll
+        for (int t = 0; t < NA * ND; ++t) wq[(size_t)(KAD + t) * wstride] = deg * kad[t];
+#pragma unroll
+        for (int t = 0; t < NB * NC; ++t) wq[(size_t)(KBC + t) * wstride] = deg * kbc[t];
+#pragma unroll
+        for (int t = 0; t < NB * ND; ++t) wq[(size_t)(KBD + t) * wstride] = deg * kbd[t];
+        return;
+    }
 #pragma unroll
     for (int kk = 0; kk < NC; ++kk)
 #pragma unroll
@@ -246,13 +261,19 @@ __global__ void __launch_bounds__(128) hgp_compiled_kernel(const KArgs A) {
         if (active) {
             const double deg = (bra.a == bra.b ? 0.5 : 1.0) * (ket.a == ket.b ? 0.5 : 1.0) *
                                ((LR.diag && ik == U.ib) ? 0.5 : 1.0);
-            quartet_compiled<LA, LB, LC, LD, R>(A, bra, ket, deg, jab);
+            constexpr int NC = cnc(LC), ND = cnc(LD);
+            constexpr int S5 = NC * ND + NA * NC + NA * ND + NB * NC + NB * ND;
+            double *wq = A.W ? ket_slots(A, U.launch, LR.n_ket, U.ib, ik, NAB, S5) : nullptr;
+            quartet_compiled<LA, LB, LC, LD, R>(A, bra, ket, deg, jab, wq, LR.n_ket);
         }
 #pragma unroll
         for (int t = 0; t < NAB; ++t) {
             const double v = warp_sum(jab[t]);
-            if (lane == 0 && v != 0.0)
+            if (A.W) {
+                if (lane == 0) A.wab[A.wab_off[u] + t] = v;  // the unit's partial, reduced in unit order
+            } else if (lane == 0 && v != 0.0) {
                 atomicAdd(A.Jp + (size_t)(bra.ao_a + t / NB) * A.n_ao + bra.ao_b + t % NB, v);
+            }
         }
     }
 }

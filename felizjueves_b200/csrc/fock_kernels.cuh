@@ -42,7 +42,21 @@ struct KArgs {
     unsigned long long *computed;  // per launch: quartets computed (null: not counted)
     const int *unit_list;   // device queue of unit indices (null: every unit)
     const int *unit_count;  // its length, on the device
+    // the atomics-free build (null W: FP64 atomics into Jp/Kp)
+    double *W;               // the launches' slot buffer
+    const int64_t *w_base;   // per launch: its first slot in W
+    double *wab;             // per unit: the bra block's partial sums
+    const int64_t *wab_off;  // per unit of this run: its offset in wab
 };
+
+// A quartet's first ket-block slot (block element 0) in the atomics-free
+// build: bra pair ib, ket position ik of launch `launch`; element e of the
+// five ket blocks (BLOCKS order cd, ac, ad, bc, bd) is at [e * n_ket].
+__device__ __forceinline__ double *ket_slots(const KArgs &A, int launch, int n_ket, int ib, int ik, int n_ab,
+                                             int s5) {
+    const int64_t row = n_ab + (int64_t)s5 * n_ket;
+    return A.W + A.w_base[launch] + (int64_t)ib * row + n_ab + ik;
+}
 
 // 1/(2m+1), m = 0 .. kBoysMaxM: the downward recursion multiplies by these
 // (each the correctly rounded quotient) instead of dividing.

@@ -280,6 +280,22 @@ class FockEngine:
                                                int(precision), float(threshold)), self._h)
         return J, K, G
 
+    def scatter_map(self, launch: int) -> dict[str, np.ndarray]:
+        """The atomics-free build's map of plan launch `launch`
+        (eri/fock/kernel_f_scatter.py:203-260 scatter_map): `el` (n_el x 2,
+        (row, col) ascending), `ptr` (n_el + 1), `src` (each element's slots
+        ascending, in the reference's slot layout)."""
+        self._require_plan()
+        ne, ns = C.c_int64(), C.c_int64()
+        _lib.check(self._L.fjb_scatter_map(self._h, int(launch), None, None, None, C.byref(ne),
+                                           C.byref(ns)), self._h)
+        el = np.empty(2 * ne.value, np.int32)
+        ptr = np.empty(ne.value + 1, np.int32)
+        src = np.empty(ns.value, np.int32)
+        _lib.check(self._L.fjb_scatter_map(self._h, int(launch), el.ctypes.data, ptr.ctypes.data,
+                                           src.ctypes.data, C.byref(ne), C.byref(ns)), self._h)
+        return {"el": el.reshape(-1, 2), "ptr": ptr, "src": src}
+
     # -- the J-engine (eri/j_coulomb/j.py) ----------------------------------
     def coulomb(self, D, *, tau: float = 0.0, J=None):
         """J of the symmetric density D by the McMurchie-Davidson J-engine

@@ -30,6 +30,12 @@
  *   fjb_eri_blocks    eri/eri.py:133-145 eri_block and
  *                     eri/hgp_drive.py:206 (the per-quartet ERI tap)
  *   fjb_boys          emit/_c.py:144-210 fj_boys<M> (device Boys)
+ *   FJB_FP64_SCATTER,
+ *   fjb_scatter_map   eri/fock/levers/scatter.py:141-198 (the slot layout) and
+ *                     eri/fock/kernel_f_scatter.py:203-260 scatter_map(cls,
+ *                                            n_ket, bra_ao, ket_ao); the build
+ *                                            mode is walk_f.py:393-408's
+ *                                            scatter lever
  *   fjb_coulomb       eri/j_coulomb/j.py:436-450 coulomb_matrix(basis, D, *,
  *                                            pq, tau) and its screened sweep
  *                                            j.py:538-581 (the MMD J-engine:
@@ -70,6 +76,7 @@ extern "C" {
 /* precision modes of fjb_fock_build */
 #define FJB_FP64 0   /* every quartet in FP64 */
 #define FJB_ROUTED 1 /* quartets under the magnitude threshold run E/R/VRR in FP32 */
+#define FJB_FP64_SCATTER 2 /* FP64, atomics-free: slot buffer + per-element scatter, bit-reproducible */
 
 typedef struct fjb_handle fjb_handle;
 
@@ -133,9 +140,11 @@ int fjb_screen_mask(fjb_handle *h, const double *D_dev, uint8_t *mask_dev,
                     void *stream);
 
 /* The fused build.  D_dev, J_dev, K_dev, G_dev are DEVICE pointers to
- * n_ao^2 doubles (any of J/K/G may be NULL).  precision: FJB_FP64 or
+ * n_ao^2 doubles (any of J/K/G may be NULL).  precision: FJB_FP64,
  * FJB_ROUTED (then `threshold` is the Schwarz x |D| bound under which a
- * quartet runs its recurrences in FP32; <= 0 means the default 1e-9).
+ * quartet runs its recurrences in FP32; <= 0 means the default 1e-9), or
+ * FJB_FP64_SCATTER (FP64 without atomics, bit-reproducible; see
+ * fjb_scatter_map; its first call stages the maps and allocates).
  * Stream-ordered; nothing is synchronised. */
 int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_dev,
                    double *G_dev, int precision, double threshold, void *stream);
@@ -225,6 +234,18 @@ int fjb_boys(int m, const double *T_dev, int n, double *F_dev);
  * stages the records (allocates), later calls allocate nothing and can be
  * captured in a CUDA graph. */
 int fjb_coulomb(fjb_handle *h, const double *D_dev, double *J_dev, double tau, void *stream);
+/* The atomics-free build's map of plan launch `launch` (plan order): n_el
+ * distinct elements (row, col) of J'/K' ascending in el[2*n_el], CSR offsets
+ * ptr[n_el + 1], and src[n_slot] each element's slots ascending, the slots
+ * numbered by the reference's slot layout.  With the arrays NULL only the
+ * counts are set.  FJB_FP64_SCATTER builds use these maps: each quartet
+ * stores its five ket-dependent blocks into its own slots, bra blocks are
+ * reduced in unit order, and every element sums its slots in order -- no
+ * atomics, the same bits on every build.  It needs the launches' slots to fit
+ * 2^28 (FJB_E_LIMIT otherwise): a small-system mode. */
+int fjb_scatter_map(const fjb_handle *h, int launch, int32_t *el, int32_t *ptr, int32_t *src, int64_t *n_el,
+                    int64_t *n_slot);
+
 /* Kernel launches of the last fjb_coulomb. */
 int fjb_j_last_launches(const fjb_handle *h);
 

@@ -9,7 +9,8 @@ files this script writes.
 
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
-parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost jplan_c0 (default: all
+parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost jplan_c0 scatter_c0
+(default: all
 but plan_c1 and jk_small, which take minutes).
 """
 
@@ -383,6 +384,41 @@ def part_jk_small():
         print("jk", name, w.n_ao, "J", round(tj, 1), "s K", round(tk, 1), "s")
 
 
+# --- the atomic-free scatter's maps (eri/fock/kernel_f_scatter.py) on c0 ----
+
+
+def part_scatter_c0():
+    _ref_imports()
+    from felizjueves.eri.fock import kernel_f_scatter as FS
+    from felizjueves_b200 import configs
+    w = configs.c0()
+    P = _plan(w, parallel_bounds=False)
+    rb = ref_basis(w.basis)
+    off = rb.offsets
+    pick, seen = [], set()
+    for li, L in enumerate(P.launches):  # each class's first launch, and its first diagonal one
+        B, K = P.batches[L.bra], P.batches[L.ket]
+        key = (B.la, B.lb, K.la, K.lb, L.bra == L.ket)
+        if key not in seen:
+            seen.add(key)
+            pick.append(li)
+    el, ptr, src, meta = [], [], [], []
+    for li in pick:
+        L = P.launches[li]
+        B, K = P.batches[L.bra], P.batches[L.ket]
+        bra_ao = [x for p in B.pairs for x in (off[p.a], off[p.b])]
+        ket_ao = [x for p in K.pairs for x in (off[p.a], off[p.b])]
+        m = FS.scatter_map((B.la, B.lb, K.la, K.lb), len(K.pairs), bra_ao, ket_ao)
+        meta.append((li, m.n_el, m.n_slot, len(el) // 2, len(ptr), len(src)))
+        el.extend(m.el)
+        ptr.extend(m.ptr)
+        src.extend(m.src)
+    np.savez_compressed(os.path.join(HERE, "scatter_c0.npz"),
+                        meta=np.asarray(meta, np.int64), el=np.asarray(el, np.int32),
+                        ptr=np.asarray(ptr, np.int32), src=np.asarray(src, np.int32))
+    print("scatter_c0", len(pick), "launches,", len(src), "slots")
+
+
 # --- the J-engine's launch plan (eri/j_coulomb/launch.py:274-327) on c0 -----
 
 
@@ -446,8 +482,8 @@ def part_cost():
 PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_eri,
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "jk_small": part_jk_small,
-         "cost": part_cost, "jplan_c0": part_jplan_c0}
-DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0"]
+         "cost": part_cost, "jplan_c0": part_jplan_c0, "scatter_c0": part_scatter_c0}
+DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
 
 
 def main():

@@ -272,3 +272,36 @@ def test_schwarz_diagonal_matches_libcint(cuda, lib_built, name):
     assert np.array_equal(M, M.T)
     Q = schwarz_matrix(B)
     assert np.allclose(Q, np.sqrt(np.maximum(ref, 0.0)), rtol=1e-11, atol=1e-14)
+
+
+@pytest.mark.parametrize("wname,tau", [("c0", 0.0), ("cluster3", 0.0), ("c0", 1e-12)])
+def test_atomics_free_build_reproducible(cuda, lib_built, oracle_lib, wname, tau):
+    """FJB_FP64_SCATTER (the reference's scatter lever: slots, then an ordered
+    per-element sum) gives the same J, K, G as the atomic build to rounding,
+    the oracle's within 1e-11 when unscreened, and the same bits on every
+    build (the property atomics do not have)."""
+    import torch
+    from felizjueves_b200 import _lib
+    w = configs.by_name(wname)
+    eng = FockEngine(w.basis)
+    eng.plan(w.D, tau, w.n_mag)
+    D = torch.tensor(w.D, device=cuda)
+    ref = [t.clone() for t in eng.build(D)]
+    runs = [[t.clone() for t in eng.build(D, precision=_lib.FJB_FP64_SCATTER)] for _ in range(3)]
+    torch.cuda.synchronize()
+    for r in runs[1:]:
+        for a, b in zip(r, runs[0]):
+            assert torch.equal(a, b)  # bit-identical
+    for a, b in zip(runs[0], ref):
+        assert float((a - b).abs().max()) <= 1e-12
+    if tau == 0.0:
+        Jo, Ko = oracle_lib.jk(oracle_lib.OracleBasis.of(w.basis), w.D)
+        J, K, G = (t.cpu().numpy() for t in runs[0])
+        assert np.abs(J - Jo).max() <= FP64_ABS
+        assert np.abs(K - Ko).max() <= FP64_ABS
+    # graph replay of the same mode
+    out = [torch.empty_like(D) for _ in range(3)]
+    eng.build(D, J=out[0], K=out[1], G=out[2], precision=_lib.FJB_FP64_SCATTER, graph=True)
+    torch.cuda.synchronize()
+    for a, b in zip(out, runs[0]):
+        assert torch.equal(a, b)
