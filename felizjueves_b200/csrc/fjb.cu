@@ -367,10 +367,10 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                     __syncthreads();
                     for (int lv = 0; lv < C.n_levels; ++lv) {
                         const int o0 = __ldg(C.level_off + lv), o1 = __ldg(C.level_off + lv + 1);
-                        for (int oi = o0 + tid; oi < o1; oi += nt) {
-                            const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(C.ops) + oi);
-                            VOp op;
-                            memcpy(&op, &raw, sizeof(op));
+                        // Two ops of the level per thread per pass: a level's
+                        // ops read only earlier levels, so both ops' loads
+                        // are issued before either store (ILP across ops).
+                        auto eval = [&](const VOp &op) -> R {
                             const int d = op.d;
                             R a, b, c, dd;
                             if (op.kind) {
@@ -387,7 +387,18 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                             R v = a * V[op.s0] + b * V[op.s1];
                             v += (R)op.c2 * (c * V[op.s2] - dd * V[op.s3]);
                             v += (R)op.c4 * e2 * V[op.s4];
-                            V[op.dst] = v;
+                            return v;
+                        };
+                        for (int oi = o0 + tid; oi < o1; oi += 2 * nt) {
+                            const int oj = oi + nt < o1 ? oi + nt : oi;
+                            const uint4 ra = __ldg(reinterpret_cast<const uint4 *>(C.ops) + oi);
+                            const uint4 rb = __ldg(reinterpret_cast<const uint4 *>(C.ops) + oj);
+                            VOp opa, opb;
+                            memcpy(&opa, &ra, sizeof(opa));
+                            memcpy(&opb, &rb, sizeof(opb));
+                            const R va = eval(opa), vb = eval(opb);
+                            V[opa.dst] = va;
+                            if (oj != oi) V[opb.dst] = vb;
                         }
                         __syncthreads();
                     }
@@ -436,10 +447,10 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                     for (int lv = 0; lv < C.n_levels; ++lv) {
                         const int o0 = __ldg(C.level_off + lv), o1 = __ldg(C.level_off + lv + 1);
                         const int items = (o1 - o0) * ns;
-                        for (int it = tid; it < items; it += nt) {
+                        // two (op, slot) items per thread per pass, as above
+                        auto eval = [&](int it, VOp &op) -> R {
                             const int oi = o0 + it / ns, s = it - (it / ns) * ns;
                             const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(C.ops) + oi);
-                            VOp op;
                             memcpy(&op, &raw, sizeof(op));
                             const R *Ss = S + s;
                             const int base = op.kind * 8;
@@ -451,7 +462,14 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                             R v = a * V[(size_t)op.s0 * slots + s] + b * V[(size_t)op.s1 * slots + s];
                             v += (R)op.c2 * (c * V[(size_t)op.s2 * slots + s] - dd * V[(size_t)op.s3 * slots + s]);
                             v += (R)op.c4 * e * V[(size_t)op.s4 * slots + s];
-                            V[(size_t)op.dst * slots + s] = v;
+                            return v;
+                        };
+                        for (int it = tid; it < items; it += 2 * nt) {
+                            const int jt = it + nt < items ? it + nt : it;
+                            VOp opa, opb;
+                            const R va = eval(it, opa), vb = eval(jt, opb);
+                            V[(size_t)opa.dst * slots + (it - (it / ns) * ns)] = va;
+                            if (jt != it) V[(size_t)opb.dst * slots + (jt - (jt / ns) * ns)] = vb;
                         }
                         __syncthreads();
                     }
