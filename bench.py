@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--workload", default="c1")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--path", default="fock", choices=["fock", "coulomb", "df"],
+                    help="fock: the G build (the headline); coulomb: the MMD J-engine; "
+                         "df: DF-J/K (FP64 and split-BF16 tensor-core GEMMs)")
     return ap.parse_args()
 
 
@@ -183,6 +186,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         return reference_arm(a, rank, world)
+    if a.path != "fock":
+        return side_path(a, local)
 
     import torch
     from felizjueves_b200 import _lib, configs, cost
@@ -316,6 +321,53 @@ def ctypes_probe(_lib, fp32: int) -> float:
     v = C.c_double()
     _lib.check(_lib.load().fjb_fma_probe(fp32, 5, C.byref(v)))
     return float(v.value)
+
+
+def side_path(a, local):
+    """One GPU: the J-engine (`--path coulomb`: fjb_coulomb at the workload's
+    tau) or DF-J/K (`--path df`: the (mn|P) L^-T factors once, then J and K
+    per step in FP64 and as split-BF16 tensor-core GEMMs), W untimed and K
+    timed steps with CUDA events on the current stream."""
+    import torch
+    from felizjueves_b200 import configs
+    w = configs.by_name(a.workload)
+    torch.cuda.set_device(local)
+    D = torch.tensor(w.D, device=f"cuda:{local}")
+    st = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(a.steps):
+            out = fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / a.steps, out
+
+    line = {"n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "higher_is_better": False,
+            "data": "synthetic", "dtype": "f64", "config": {"workload": a.workload, "n_ao": w.n_ao}}
+    if a.path == "coulomb":
+        from felizjueves_b200.fock import FockEngine
+        eng = FockEngine(w.basis, device=local)
+        J = torch.empty_like(D)
+        ms, _ = timed(lambda: eng.coulomb(D, tau=w.tau, J=J))
+        line.update(metric="J-engine J build ms/iter", value=round(ms, 3), unit="ms/iter",
+                    gpu_launches=eng.j_launches())
+    else:
+        from felizjueves_b200.df import DFEngine
+        aux = configs.aux_basis(w)
+        eng = DFEngine(w.basis, aux, device=local)
+        B = eng.factors()
+        ms64, (J64, K64) = timed(lambda: eng.jk(D, "fp64", B=B))
+        ms16, (J16, K16) = timed(lambda: eng.jk(D, "bf16x3", B=B))
+        line.update(metric="DF-J/K ms/iter", value=round(ms16, 3), unit="ms/iter", dtype="bf16x3 -> f32",
+                    fp64_ms=round(ms64, 3), n_aux=aux.n_ao,
+                    max_abs_dJ_bf16x3_vs_fp64=float((J16 - J64).abs().max()),
+                    max_abs_dK_bf16x3_vs_fp64=float((K16 - K64).abs().max()))
+    print(json.dumps(line))
 
 
 def reference_arm(a, rank, world):

@@ -247,7 +247,7 @@ constexpr int kSmallL = 6;
 
 template <int LP, int LQ>
 __global__ void __launch_bounds__(128) j_pq_small_kernel(const JRec *__restrict__ recs, int bra0, int nbra,
-                                                         int ket0, int nket, const int *__restrict__ order,
+                                                         int ket0, int nket, const double4 *__restrict__ kst, const int *__restrict__ kdq,
                                                          const double *__restrict__ skey,
                                                          const double *__restrict__ Dq, double *__restrict__ Jp,
                                                          double tau, const double *__restrict__ boys_tab) {
@@ -264,10 +264,11 @@ __global__ void __launch_bounds__(128) j_pq_small_kernel(const JRec *__restrict_
             const int k = k0 + lane;
             const bool on = k < nket && !(B.G * skey[ket0 + k] < tau);
             if (on) {
-                const JRec K = recs[order[ket0 + k]];
-                const double p = B.zeta, q = K.zeta;
+                const double4 KP = kst[ket0 + k];  // (P, eta) of the k-th ket in key order
+                const int kdo = kdq[ket0 + k];
+                const double p = B.zeta, q = KP.w;
                 const double rho = p * q / (p + q);
-                const double X = B.P[0] - K.P[0], Y = B.P[1] - K.P[1], Z = B.P[2] - K.P[2];
+                const double X = B.P[0] - KP.x, Y = B.P[1] - KP.y, Z = B.P[2] - KP.z;
                 const double T = rho * (X * X + Y * Y + Z * Z);
                 double F[L + 1];
                 boys_t<L>(T, F, boys_tab);
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(128) j_pq_small_kernel(const JRec *__restrict_
                 R[0] = f[L];
                 RLevels<L, L - 1>::run(R, f, X, Y, Z);
                 double d[NQ];
-                signed_dq(d, Dq + K.dq_off, std::make_integer_sequence<int, NQ>{});
+                signed_dq(d, Dq + kdo, std::make_integer_sequence<int, NQ>{});
                 contract<NQ>(jp, R, d, std::make_integer_sequence<int, NP * NQ>{});
             }
             const unsigned bal = __ballot_sync(0xffffffffu, on);
@@ -302,7 +303,7 @@ __global__ void __launch_bounds__(128) j_pq_small_kernel(const JRec *__restrict_
 // One (bra L, ket L) class at total order L = lp + lq (runtime lp, lq).
 template <int L>
 __global__ void __launch_bounds__(128) j_pq_kernel(const JRec *__restrict__ recs, int lp, int lq, int bra0, int nbra,
-                                                   int ket0, int nket, const int *__restrict__ order,
+                                                   int ket0, int nket, const double4 *__restrict__ kst, const int *__restrict__ kdq,
                                                    const double *__restrict__ skey, const double *__restrict__ Dq,
                                                    double *__restrict__ Jp, double tau,
                                                    const double *__restrict__ boys_tab) {
@@ -319,10 +320,11 @@ __global__ void __launch_bounds__(128) j_pq_kernel(const JRec *__restrict__ recs
             const int k = k0 + lane;
             const bool on = k < nket && !(B.G * skey[ket0 + k] < tau);
             if (on) {
-                const JRec K = recs[order[ket0 + k]];
-                const double p = B.zeta, q = K.zeta;
+                const double4 KP = kst[ket0 + k];  // (P, eta) of the k-th ket in key order
+                const int kdo = kdq[ket0 + k];
+                const double p = B.zeta, q = KP.w;
                 const double rho = p * q / (p + q);
-                const double X = B.P[0] - K.P[0], Y = B.P[1] - K.P[1], Z = B.P[2] - K.P[2];
+                const double X = B.P[0] - KP.x, Y = B.P[1] - KP.y, Z = B.P[2] - KP.z;
                 const double T = rho * (X * X + Y * Y + Z * Z);
                 double F[L + 1];
                 boys_t<L>(T, F, boys_tab);
@@ -359,7 +361,7 @@ __global__ void __launch_bounds__(128) j_pq_kernel(const JRec *__restrict__ recs
                     }
                     R[0] = f[m];
                 }
-                const double *dq = Dq + K.dq_off;
+                const double *dq = Dq + kdo;
                 for (int qi = 0; qi < NQ; ++qi) {
                     const int tq = kHermR[qi][0], uq = kHermR[qi][1], vq = kHermR[qi][2];
                     const double d = (((tq + uq + vq) & 1) ? -1.0 : 1.0) * __ldg(dq + qi);
@@ -376,6 +378,17 @@ __global__ void __launch_bounds__(128) j_pq_kernel(const JRec *__restrict__ recs
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) Jp[B.dq_off + pi] += v;
         }
+    }
+}
+
+// The kets of every L in key order as a contiguous stream: (P, eta) and the
+// D_q offset of the k-th sorted ket, so the walk's loads are coalesced.
+__global__ void j_gather_kernel(const JRec *__restrict__ recs, const int *__restrict__ order, int n,
+                                double4 *__restrict__ kst, int *__restrict__ kdq) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const JRec R = recs[order[k]];
+        kst[k] = make_double4(R.P[0], R.P[1], R.P[2], R.zeta);
+        kdq[k] = R.dq_off;
     }
 }
 
@@ -419,13 +432,14 @@ __global__ void j_jab_kernel(const JRec *__restrict__ recs, const int *__restric
     }
 }
 
-using PqLaunch = void (*)(int grid, cudaStream_t st, const JRec *, int, int, int, int, int, int, const int *,
-                          const double *, const double *, double *, double, const double *);
+using PqLaunch = void (*)(int grid, cudaStream_t st, const JRec *, int, int, int, int, int, int, const double4 *,
+                          const int *, const double *, const double *, double *, double, const double *);
 
 template <int L>
 void pq_launch(int grid, cudaStream_t st, const JRec *recs, int lp, int lq, int bra0, int nbra, int ket0, int nket,
-               const int *order, const double *skey, const double *Dq, double *Jp, double tau, const double *boys) {
-    j_pq_kernel<L><<<grid, 128, 0, st>>>(recs, lp, lq, bra0, nbra, ket0, nket, order, skey, Dq, Jp, tau, boys);
+               const double4 *kst, const int *kdq, const double *skey, const double *Dq, double *Jp, double tau,
+               const double *boys) {
+    j_pq_kernel<L><<<grid, 128, 0, st>>>(recs, lp, lq, bra0, nbra, ket0, nket, kst, kdq, skey, Dq, Jp, tau, boys);
 }
 
 template <int... L>
@@ -434,16 +448,16 @@ constexpr std::array<PqLaunch, sizeof...(L)> pq_table(std::integer_sequence<int,
 }
 const auto kPqTable = pq_table(std::make_integer_sequence<int, 2 * kJMaxL + 1>{});
 
-using PqSmallLaunch = void (*)(int grid, cudaStream_t st, const JRec *, int, int, int, int, const int *,
-                               const double *, const double *, double *, double, const double *);
+using PqSmallLaunch = void (*)(int grid, cudaStream_t st, const JRec *, int, int, int, int, const double4 *,
+                               const int *, const double *, const double *, double *, double, const double *);
 
 template <int LP, int LQ>
 void pq_small_launch(int grid, cudaStream_t st, const JRec *recs, int bra0, int nbra, int ket0, int nket,
-                     const int *order, const double *skey, const double *Dq, double *Jp, double tau,
+                     const double4 *kst, const int *kdq, const double *skey, const double *Dq, double *Jp, double tau,
                      const double *boys) {
     if constexpr (LP + LQ <= kSmallL)
-        j_pq_small_kernel<LP, LQ><<<grid, 128, 0, st>>>(recs, bra0, nbra, ket0, nket, order, skey, Dq, Jp, tau,
-                                                        boys);
+        j_pq_small_kernel<LP, LQ><<<grid, 128, 0, st>>>(recs, bra0, nbra, ket0, nket, kst, kdq, skey, Dq, Jp,
+                                                        tau, boys);
 }
 
 template <int LP, int... LQ>
@@ -516,7 +530,8 @@ struct JEngine {
     int n_rec = 0, n_pairs = 0;
     std::vector<int> L_off;       // [kJMaxL + 2] record groups by L
     DBuf<JRec> recs;
-    DBuf<int> pair_rec0, pair_nrec, seg_off, iota, order;
+    DBuf<int> pair_rec0, pair_nrec, seg_off, iota, order, kdq;
+    DBuf<double4> kst;
     DBuf<double> Dq, Jp, key, skey;
     DBuf<unsigned char> sort_tmp;
     size_t sort_bytes = 0;
@@ -580,6 +595,8 @@ JEngine *jengine_create(const HostBasis &basis, int device, std::string *err) {
     if (ce == cudaSuccess) ce = e->seg_off.upload(e->L_off);
     if (ce == cudaSuccess) ce = e->iota.upload(io);
     if (ce == cudaSuccess) ce = e->order.alloc(e->n_rec);
+    if (ce == cudaSuccess) ce = e->kdq.alloc(std::max(e->n_rec, 1));
+    if (ce == cudaSuccess) ce = e->kst.alloc(std::max(e->n_rec, 1));
     if (ce == cudaSuccess) ce = e->Dq.alloc(std::max(dq, 1));
     if (ce == cudaSuccess) ce = e->Jp.alloc(std::max(dq, 1));
     if (ce == cudaSuccess) ce = e->key.alloc(std::max(e->n_rec, 1));
@@ -621,6 +638,9 @@ int jengine_build(JEngine *e, const double *D_dev, double *J_dev, double tau, co
                "segmented sort"))
         return -2;
     ++nl;
+    j_gather_kernel<<<rec_grid, 128, 0, st>>>(e->recs.p, e->order.p, e->n_rec, e->kst.p, e->kdq.p);
+    ++nl;
+    if (!check(cudaGetLastError(), "j_gather_kernel")) return -2;
     if (!check(cudaMemsetAsync(e->Jp.p, 0, e->Jp.n * sizeof(double), st), "memset")) return -2;
     for (int lp = 0; lp <= kJMaxL; ++lp) {
         const int b0 = e->L_off[lp], nb = e->L_off[lp + 1] - b0;
@@ -630,10 +650,10 @@ int jengine_build(JEngine *e, const double *D_dev, double *J_dev, double tau, co
             const int k0 = e->L_off[lq], nk = e->L_off[lq + 1] - k0;
             if (nk == 0) continue;
             if (lp + lq <= kSmallL)
-                kPqSmall[lp][lq](grid, st, e->recs.p, b0, nb, k0, nk, e->order.p, e->skey.p, e->Dq.p, e->Jp.p, tau,
+                kPqSmall[lp][lq](grid, st, e->recs.p, b0, nb, k0, nk, e->kst.p, e->kdq.p, e->skey.p, e->Dq.p, e->Jp.p, tau,
                                  boys_tab);
             else
-                kPqTable[lp + lq](grid, st, e->recs.p, lp, lq, b0, nb, k0, nk, e->order.p, e->skey.p, e->Dq.p,
+                kPqTable[lp + lq](grid, st, e->recs.p, lp, lq, b0, nb, k0, nk, e->kst.p, e->kdq.p, e->skey.p, e->Dq.p,
                                   e->Jp.p, tau, boys_tab);
             ++nl;
             if (!check(cudaGetLastError(), "j_pq_kernel")) return -2;

@@ -158,7 +158,7 @@ class DFEngine:
             B2 = B.reshape(nx, n * n)
             gamma = _mm3(B2, D.reshape(n * n, 1)).reshape(nx)
             J = _mm3(B2.T.contiguous(), gamma.reshape(nx, 1)).reshape(n, n)
-            X = torch.stack([_mm3(B[q], D) for q in range(nx)])      # (nx, n, n)
+            X = _mm3(B.reshape(nx * n, n), D).reshape(nx, n, n)   # X_q = B_q D, one GEMM
             K = _mm3(X.permute(1, 0, 2).reshape(n, nx * n).contiguous(),
                      B.permute(0, 2, 1).reshape(nx * n, n).contiguous())
             return J, K
