@@ -53,9 +53,11 @@ def parse():
     ap.add_argument("--workload", default="c1")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--path", default="fock", choices=["fock", "coulomb", "df"],
+    ap.add_argument("--path", default="fock", choices=["fock", "coulomb", "df", "batch"],
                     help="fock: the G build (the headline); coulomb: the MMD J-engine; "
-                         "df: DF-J/K (FP64 and split-BF16 tensor-core GEMMs)")
+                         "df: DF-J/K (FP64 and split-BF16 tensor-core GEMMs); batch: the "
+                         "uneven molecule batch (c4) as one captured graph")
+    ap.add_argument("--molecules", type=int, default=64, help="batch path: the first N c4 molecules")
     return ap.parse_args()
 
 
@@ -349,6 +351,8 @@ def side_path(a, local):
 
     line = {"n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "higher_is_better": False,
             "data": "synthetic", "dtype": "f64", "config": {"workload": a.workload, "n_ao": w.n_ao}}
+    if a.path == "batch":
+        return batch_path(a, local)
     if a.path == "coulomb":
         from felizjueves_b200.fock import FockEngine
         eng = FockEngine(w.basis, device=local)
@@ -368,6 +372,61 @@ def side_path(a, local):
                     max_abs_dJ_bf16x3_vs_fp64=float((J16 - J64).abs().max()),
                     max_abs_dK_bf16x3_vs_fp64=float((K16 - K64).abs().max()))
     print(json.dumps(line))
+
+
+def batch_path(a, local):
+    """The c4 batch (its first --molecules molecules): the plain FP64
+    per-molecule loop, the batch as one captured graph in FP64, and in the
+    routed mode with the learned router (trained here on seeded 4-10 atom
+    clusters, calibrated, installed on every molecule); total ms per batch,
+    per-molecule device ms (p50, p99) and max|dG| against FP64."""
+    import torch
+    from felizjueves_b200 import _lib, configs, router
+    from felizjueves_b200.batch import BatchBuilder
+    torch.cuda.set_device(local)
+    ws = configs.c4(a.molecules)
+    bb = BatchBuilder(ws, device=local)
+    st = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(a.steps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / a.steps
+
+    loop_ms = timed(lambda: bb.build_loop(_lib.FJB_FP64))
+    bb.capture("fp64", _lib.FJB_FP64)
+    g64_ms = timed(lambda: bb.replay("fp64"))
+    G64 = [g.clone() for g in bb.G()]
+    X, y = router.training_set([configs.cluster(n, 100 + n) for n in (4, 5, 6, 7, 8, 10)], n_per=12000, seed=1)
+    perm = np.random.default_rng(2).permutation(len(X))
+    tr, va = perm[: int(0.8 * len(X))], perm[int(0.8 * len(X)):]
+    mlp = router.MLP(router.init_params(X[tr], y[tr], seed=0))
+    mlp.train(X[tr], y[tr])
+    margin = router.calibrate(mlp, X[va], y[va], 0.999)
+    for eng in bb.engines:
+        router.install(eng, mlp, threshold=1e-9, margin=margin)
+    bb.capture("routed", _lib.FJB_ROUTED, 1e-9)
+    gr_ms = timed(lambda: bb.replay("routed"))
+    per = bb.device_ms()
+    dG = max(float((g - h).abs().max()) for g, h in zip(bb.G(), G64))
+    sizes = [len(w.coords) for w in ws]
+    print(json.dumps({
+        "metric": "uneven batch G builds ms/batch (one graph, routed + learned router)", "value": round(gr_ms, 3),
+        "unit": "ms/batch", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "higher_is_better": False,
+        "data": "synthetic", "dtype": "f64 (routed units FP32)",
+        "config": {"workload": f"c4: first {len(ws)} of 512 molecules, {min(sizes)}-{max(sizes)} atoms "
+                               f"({sum(sizes)} atoms, {sum(w.n_ao for w in ws)} AO in all)"},
+        "fp64_loop_ms": round(loop_ms, 3), "fp64_graph_ms": round(g64_ms, 3),
+        "per_molecule_device_ms": {"p50": round(float(np.percentile(per, 50)), 3),
+                                   "p99": round(float(np.percentile(per, 99)), 3)},
+        "max_abs_dG_vs_fp64": dG, "router_margin": round(margin, 3)}))
 
 
 def reference_arm(a, rank, world):

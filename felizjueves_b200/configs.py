@@ -159,6 +159,17 @@ def sub_workload(w: Workload, atoms: int) -> Workload:
                     w.coords[:atoms], w.seed, w.n_occ)
 
 
+def c4(n_molecules: int = 512) -> list[Workload]:
+    """The uneven batch: molecules of 3-40 atoms (uniform size draw from
+    seed 4), each a cluster of the c1 shell recipe at c1's density with its
+    own seeded geometry and density (n_occ = 2 x atoms).  The first
+    `n_molecules` of the 512."""
+    rng = np.random.default_rng(4)
+    sizes = rng.integers(3, 41, size=512)
+    return [cluster(int(n), 4000 + i, name=f"c4_{i}_{int(n)}at")
+            for i, n in enumerate(sizes[:n_molecules])]
+
+
 WORKLOADS = {"c0": c0, "c1": c1}
 
 
