@@ -58,6 +58,9 @@ def parse():
                          "df: DF-J/K (FP64 and split-BF16 tensor-core GEMMs); batch: the "
                          "uneven molecule batch (c4) as one captured graph")
     ap.add_argument("--molecules", type=int, default=64, help="batch path: the first N c4 molecules")
+    ap.add_argument("--router", default="bound", choices=["learned", "bound"],
+                    help="routed builds: the learned router (trained and calibrated before the "
+                         "timed region) or the Schwarz x density bound alone")
     return ap.parse_args()
 
 
@@ -249,8 +252,13 @@ def main():
         return ms_, ck_, eng.last_build_stats()[1], eng.class_stats(), eng.launch_stats(), G.clone()
 
     ms64, ck64, nl64, cs, ls, G64 = timed(_lib.FJB_FP64)
+    router_info = None
+    if a.precision == "routed" and a.router == "learned":
+        router_info = install_learned_router(eng)
     if a.precision == "routed":
         ms, ck, nl, cs_r, ls_r, Gr = timed(_lib.FJB_ROUTED)
+        n32, n64 = route_counts(eng)
+        router_info = dict(router_info or {"kind": "bound"}, fp32_units=n32, fp64_units=n64)
         dG = float((Gr - G64).abs().max())
         prec = _lib.FJB_ROUTED
     else:
@@ -299,6 +307,7 @@ def main():
         "speedup_routed_vs_fp64": round(ms64 / ms, 4) if a.precision == "routed" else None,
         "max_abs_dG_vs_fp64": dG if a.precision == "routed" else None,
         "route_threshold": 1e-9 if a.precision == "routed" else None,
+        "router": router_info,
         "config": {"workload": WORKLOAD, "n_ao": n, "shells": len(w.basis.shells),
                    "tau": w.tau, "quartets_launched": launched, "quartets_computed": computed,
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
@@ -323,6 +332,33 @@ def ctypes_probe(_lib, fp32: int) -> float:
     v = C.c_double()
     _lib.check(_lib.load().fjb_fma_probe(fp32, 5, C.byref(v)))
     return float(v.value)
+
+
+def train_router():
+    """The learned precision router: trained on the GPU with the library's
+    kernels on quartets the FP64 method computes for six seeded 4-10 atom
+    clusters (not a benchmarked system), calibrated on held-out quartets
+    (0.999 residual quantile).  Returns (network, margin, training size)."""
+    from felizjueves_b200 import configs, router
+    X, y = router.training_set([configs.cluster(n, 100 + n) for n in (4, 5, 6, 7, 8, 10)], n_per=12000, seed=1)
+    perm = np.random.default_rng(2).permutation(len(X))
+    tr, va = perm[: int(0.8 * len(X))], perm[int(0.8 * len(X)):]
+    mlp = router.MLP(router.init_params(X[tr], y[tr], seed=0))
+    mlp.train(X[tr], y[tr])
+    return mlp, router.calibrate(mlp, X[va], y[va], 0.999), int(len(tr))
+
+
+def install_learned_router(eng) -> dict:
+    """train_router(), installed on `eng` at the 1e-9 threshold."""
+    from felizjueves_b200 import router
+    mlp, margin, n_tr = train_router()
+    router.install(eng, mlp, threshold=1e-9, margin=margin)
+    return {"kind": "learned", "training_quartets": n_tr, "margin_log10": round(margin, 3)}
+
+
+def route_counts(eng):
+    from felizjueves_b200 import router
+    return router.route_stats(eng)
 
 
 def side_path(a, local):
@@ -404,12 +440,7 @@ def batch_path(a, local):
     bb.capture("fp64", _lib.FJB_FP64)
     g64_ms = timed(lambda: bb.replay("fp64"))
     G64 = [g.clone() for g in bb.G()]
-    X, y = router.training_set([configs.cluster(n, 100 + n) for n in (4, 5, 6, 7, 8, 10)], n_per=12000, seed=1)
-    perm = np.random.default_rng(2).permutation(len(X))
-    tr, va = perm[: int(0.8 * len(X))], perm[int(0.8 * len(X)):]
-    mlp = router.MLP(router.init_params(X[tr], y[tr], seed=0))
-    mlp.train(X[tr], y[tr])
-    margin = router.calibrate(mlp, X[va], y[va], 0.999)
+    mlp, margin, _ = train_router()
     for eng in bb.engines:
         router.install(eng, mlp, threshold=1e-9, margin=margin)
     bb.capture("routed", _lib.FJB_ROUTED, 1e-9)

@@ -178,10 +178,18 @@ __global__ void route_units_kernel(const Unit *units, int unit0, int n_units, co
     }
 }
 
+// The largest gap (decades) below the Schwarz x density bound the router's
+// network may use: the range of gaps it is trained on (4.2 observed).
+constexpr double kRouterMaxGap = 5.0;
+constexpr double kRouterReach = 1e5;  // 10^kRouterMaxGap
+
 // The learned router's unit split: as route_units_kernel, but a quartet the
 // rigorous bound calls high may still go to FP32 when the network predicts
-// its deposit under 10^log_thr.  Screening is untouched (the bound decides
-// what is skipped).
+// its deposit under 10^log_thr -- provided its bound is within
+// kRouterMaxGap decades of the threshold; a unit with a quartet beyond that
+// stays FP64 without running the network.  Screening is untouched (the
+// bound decides what is skipped).
+
 __global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units, const LaunchRec *launches,
                                        const PairRec *pairs, const PrimRec *prims, const double *Dsh, int n_sh,
                                        double tau, double thresh, const float *params, float log_thr, int la,
@@ -197,19 +205,30 @@ __global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units
         const LaunchRec L = launches[U.launch];
         const PairRec bra = pairs[L.bra_pair0 + U.ib];
         const int ik = U.k0 + lane;
-        bool active = false, low = true;
+        bool active = false, need = false, reach = true;
+        PairRec ket{};
+        double dmax = 0.0;
         if (ik < U.k1) {
-            const PairRec ket = pairs[L.ket_pair0 + ik];
-            const double dmax = six_block_dmax(Dsh, n_sh, bra.a, bra.b, ket.a, ket.b);
+            ket = pairs[L.ket_pair0 + ik];
+            dmax = six_block_dmax(Dsh, n_sh, bra.a, bra.b, ket.a, ket.b);
             const double b = __dmul_rn(bra.G, __dmul_rn(ket.G, dmax));
             active = !(b < tau);
-            if (active && !(b < thresh)) {
-                float f[kFeat];
-                quartet_features(bra, ket, prims, la, lb, lc, ld, dmax, f);
-                low = mlp_forward(sp, f, nullptr, nullptr) < log_thr;
-            }
+            need = active && !(b < thresh);
+            // the network learned gaps below the bound of up to kRouterMaxGap
+            // decades: a quartet further above the threshold cannot go FP32
+            reach = !need || b < thresh * kRouterReach;
         }
         const bool any = __any_sync(0xffffffffu, active);
+        bool low = true;
+        // a unit goes FP32 only if all its quartets do: if one is out of the
+        // network's reach the unit stays FP64 and the network is not run
+        if (__all_sync(0xffffffffu, reach) && need) {
+            float f[kFeat];
+            quartet_features(bra, ket, prims, la, lb, lc, ld, dmax, f);
+            low = mlp_forward(sp, f, nullptr, nullptr) < log_thr;
+        } else if (need) {
+            low = false;
+        }
         const bool all_low = __all_sync(0xffffffffu, low);
         if (lane == 0 && any) {
             if (all_low)
