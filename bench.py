@@ -58,6 +58,12 @@ def parse():
                          "df: DF-J/K (FP64 and split-BF16 tensor-core GEMMs); batch: the "
                          "uneven molecule batch (c4) as one captured graph")
     ap.add_argument("--molecules", type=int, default=64, help="batch path: the first N c4 molecules")
+    ap.add_argument("--threshold", type=float, default=1e-9,
+                    help="routed builds: the Schwarz x density bound under which a unit runs FP32 "
+                         "(config c2's rule: 1e-9)")
+    ap.add_argument("--budget-threshold", type=float, default=1e-7,
+                    help="a second routed measurement at this threshold, reported with its "
+                         "max|dG| against the 1e-8 budget (0: skip)")
     ap.add_argument("--router", default="bound", choices=["learned", "bound"],
                     help="routed builds: the learned router (trained and calibrated before the "
                          "timed region) or the Schwarz x density bound alone")
@@ -217,7 +223,7 @@ def main():
     G = torch.empty_like(J)
     stream = torch.cuda.current_stream()
 
-    def timed(prec):
+    def timed(prec, thr=0.0):
         """W untimed builds, then K builds between two events on the build
         stream (each step: the in-place update of the working density, then
         the build replayed as its captured CUDA graph), bracketed by barrier + synchronize; nvidia-smi sampled over
@@ -226,7 +232,7 @@ def main():
         last build and a copy of its G."""
         for i in range(a.warmup):
             Dw.copy_(Ds[i % n_d])  # the SCF loop's in-place density update
-            eng.build(Dw, J=J, K=K, G=G, precision=prec, graph=True)
+            eng.build(Dw, J=J, K=K, G=G, precision=prec, threshold=thr, graph=True)
         torch.cuda.synchronize()
         clocks = Clocks(local)
         clocks.start()
@@ -238,7 +244,7 @@ def main():
         e0.record(stream)
         for i in range(a.steps):
             Dw.copy_(Ds[i % n_d])  # the SCF loop's in-place density update
-            eng.build(Dw, J=J, K=K, G=G, precision=prec, graph=True)
+            eng.build(Dw, J=J, K=K, G=G, precision=prec, threshold=thr, graph=True)
         e1.record(stream)
         torch.cuda.synchronize()
         if dist:
@@ -255,10 +261,17 @@ def main():
     router_info = None
     if a.precision == "routed" and a.router == "learned":
         router_info = install_learned_router(eng)
+    budget = None
     if a.precision == "routed":
-        ms, ck, nl, cs_r, ls_r, Gr = timed(_lib.FJB_ROUTED)
+        ms, ck, nl, cs_r, ls_r, Gr = timed(_lib.FJB_ROUTED, a.threshold)
         n32, n64 = route_counts(eng)
         router_info = dict(router_info or {"kind": "bound"}, fp32_units=n32, fp64_units=n64)
+        if a.budget_threshold > 0:
+            msb, _, _, _, _, Gb = timed(_lib.FJB_ROUTED, a.budget_threshold)
+            budget = {"threshold": a.budget_threshold, "ms_per_step": round(msb, 3),
+                      "speedup_vs_fp64": round(ms64 / msb, 4),
+                      "max_abs_dG_vs_fp64": float((Gb - G64).abs().max()),
+                      "fp32_units": route_counts(eng)[0]}
         dG = float((Gr - G64).abs().max())
         prec = _lib.FJB_ROUTED
     else:
@@ -279,11 +292,11 @@ def main():
     e2e = None
     if not a.no_e2e and rank == 0:
         Dh = [configs.perturbed_density(w.D, i) for i in range(3)]
-        eng.build_host(Dh[0], precision=prec)  # warm
+        eng.build_host(Dh[0], precision=prec, threshold=a.threshold)  # warm
         k2 = min(a.steps, 3)
         t0 = time.perf_counter()
         for i in range(k2):
-            eng.build_host(Dh[i % 3], precision=prec)
+            eng.build_host(Dh[i % 3], precision=prec, threshold=a.threshold)
         e2e_ms = (time.perf_counter() - t0) * 1e3 / k2
         e2e = {"value": round(e2e_ms, 3), "unit": "ms/iter", "h2d_bytes_per_step": n * n * 8,
                "d2h_bytes_per_step": 3 * n * n * 8,
@@ -306,7 +319,8 @@ def main():
         "fp64": {"ms_per_step": round(ms64, 3), "clocks": ck64},
         "speedup_routed_vs_fp64": round(ms64 / ms, 4) if a.precision == "routed" else None,
         "max_abs_dG_vs_fp64": dG if a.precision == "routed" else None,
-        "route_threshold": 1e-9 if a.precision == "routed" else None,
+        "route_threshold": a.threshold if a.precision == "routed" else None,
+        "routed_at_budget_threshold": budget,
         "router": router_info,
         "config": {"workload": WORKLOAD, "n_ao": n, "shells": len(w.basis.shells),
                    "tau": w.tau, "quartets_launched": launched, "quartets_computed": computed,

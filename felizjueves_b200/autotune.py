@@ -59,6 +59,53 @@ def autotune(eng, D, candidates=CANDIDATES, reps: int = 1, precision: int = 0) -
                    for c, t in times.items()}}
 
 
+CANDIDATES32 = ((32, 0), (64, 0), (128, 0), (256, 0), (512, 0), (64, 1), (128, 1), (128, 2), (256, 4))
+
+
+def autotune32(eng, D, candidates=CANDIDATES32, reps: int = 1) -> dict:
+    """The routed path's FP32 interpreter, per class: every unit sent to FP32
+    (a routing threshold above every bound), one build timed per candidate
+    (threads, slots), the fastest kept per class (classes with an FP32
+    register body run it whatever this sets)."""
+    import torch
+    from . import _lib
+    everything = 1e300
+    times: dict[tuple, dict[tuple, float]] = {}
+    for cand in candidates:
+        classes = [(r["la"], r["lb"], r["lc"], r["ld"]) for r in eng.class_stats()] if times else None
+        if classes is None:
+            eng.build(D, precision=_lib.FJB_ROUTED, threshold=everything)
+            torch.cuda.synchronize()
+            classes = [(r["la"], r["lb"], r["lc"], r["ld"]) for r in eng.class_stats()]
+            times = {c: {} for c in classes}
+        ok = []
+        for c in classes:
+            try:
+                eng.set_class_config32(c, *cand)
+                ok.append(c)
+            except ValueError:
+                pass
+        samples: dict[tuple, list[float]] = {c: [] for c in ok}
+        for _ in range(reps):
+            eng.build(D, precision=_lib.FJB_ROUTED, threshold=everything)
+            torch.cuda.synchronize()
+            for r in eng.class_stats():
+                c = (r["la"], r["lb"], r["lc"], r["ld"])
+                if c in samples:
+                    samples[c].append(r["ms"])
+        for c, v in samples.items():
+            if v:
+                times[c][cand] = float(np.median(v))
+    choice = {}
+    for c, t in times.items():
+        if t:
+            choice[c] = min(t, key=t.get)
+            eng.set_class_config32(c, *choice[c])
+    return {"choice32": {",".join(map(str, c)): list(v) for c, v in choice.items()},
+            "ms32": {",".join(map(str, c)): {f"{k[0]}x{k[1]}": v for k, v in t.items()}
+                     for c, t in times.items()}}
+
+
 def _has_build(eng) -> bool:
     try:
         eng.class_stats()
@@ -71,6 +118,11 @@ def apply(eng, table: dict) -> None:
     for key, (threads, slots) in table["choice"].items():
         try:
             eng.set_class_config(tuple(int(x) for x in key.split(",")), threads, slots)
+        except ValueError:
+            pass
+    for key, (threads, slots) in table.get("choice32", {}).items():
+        try:
+            eng.set_class_config32(tuple(int(x) for x in key.split(",")), threads, slots)
         except ValueError:
             pass
 

@@ -810,7 +810,8 @@ struct fjb_handle {
     int j_launches = 0;            // kernel launches of the last J-engine build
     std::string err;
     std::map<std::tuple<int, int, int, int>, std::unique_ptr<ClassEntry>> classes;
-    std::map<std::tuple<int, int, int, int>, std::pair<int, int>> cfg;  // (threads, slots) overrides
+    std::map<std::tuple<int, int, int, int>, std::pair<int, int>> cfg;    // (threads, slots) overrides
+    std::map<std::tuple<int, int, int, int>, std::pair<int, int>> cfg32;  // the FP32 interpreter's
     DevBuf<double> boys;
     DevBuf<int> sh_off, sh_nc;
     // plan
@@ -1272,6 +1273,9 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
             run.dev32 = ov == h->cfg.end() || th == 1
                             ? ce.dev(deg.first, deg.second, 0, 0, 4)
                             : ce.dev(deg.first, deg.second, th, ov->second.second, 4);
+            auto ov32 = h->cfg32.find(kv.first);
+            if (ov32 != h->cfg32.end())
+                run.dev32 = ce.dev(deg.first, deg.second, ov32->second.first, ov32->second.second, 4);
             run.compiled = compiled_available(la, lb, lc, ld, false) && (th == 0 || th == 1);
             run.has32 = compiled_available(la, lb, lc, ld, true);
             run.unit0 = (int)units.size();
@@ -1941,9 +1945,44 @@ int fjb_set_class_config(fjb_handle *h, int la, int lb, int lc, int ld, int thre
             ClassDev d = threads == 1 ? ce.dev(r.max_kab, r.max_kcd) : ce.dev(r.max_kab, r.max_kcd, threads, slots);
             r.dev32 = threads == 1 ? ce.dev(r.max_kab, r.max_kcd, 0, 0, 4)
                                    : ce.dev(r.max_kab, r.max_kcd, threads, slots, 4);
+            auto ov32 = h->cfg32.find(key);
+            if (ov32 != h->cfg32.end())
+                r.dev32 = ce.dev(r.max_kab, r.max_kcd, ov32->second.first, ov32->second.second, 4);
             r.dev = d;
             r.compiled = compiled_available(la, lb, lc, ld, false) && (threads == 0 || threads == 1);
             r.grid = run_grid(r);
+            r.grid32 = run_grid32(r);
+        } catch (const std::length_error &e) {
+            return fail(h, FJB_E_LIMIT, e.what());
+        }
+    }
+    return FJB_OK;
+}
+
+int fjb_set_class_config32(fjb_handle *h, int la, int lb, int lc, int ld, int threads, int slots) {
+    if (!h) return fail(h, FJB_E_ARG, "null handle");
+    if (threads != 0 && threads != 32 && threads != 64 && threads != 128 && threads != 256 && threads != 512)
+        return fail(h, FJB_E_ARG, "threads must be 0, 32, 64, 128, 256 or 512");
+    if (slots < 0 || slots > kMaxThreads) return fail(h, FJB_E_ARG, "slots out of range");
+    auto key = std::make_tuple(la, lb, lc, ld);
+    h->drop_graph();
+    if (threads == 0 && slots == 0)
+        h->cfg32.erase(key);
+    else
+        h->cfg32[key] = {threads, slots};
+    if (h->device < 0 || !h->planned) return FJB_OK;
+    for (auto &r : h->runs) {
+        if (std::make_tuple(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld) != key) continue;
+        try {
+            ClassEntry &ce = h->cls(la, lb, lc, ld);
+            if (threads == 0 && slots == 0) {  // back to the FP64 configuration's FP32 twin
+                auto ov = h->cfg.find(key);
+                const int th = ov == h->cfg.end() ? 0 : ov->second.first;
+                r.dev32 = ov == h->cfg.end() || th == 1 ? ce.dev(r.max_kab, r.max_kcd, 0, 0, 4)
+                                                         : ce.dev(r.max_kab, r.max_kcd, th, ov->second.second, 4);
+            } else {
+                r.dev32 = ce.dev(r.max_kab, r.max_kcd, threads, slots, 4);
+            }
             r.grid32 = run_grid32(r);
         } catch (const std::length_error &e) {
             return fail(h, FJB_E_LIMIT, e.what());

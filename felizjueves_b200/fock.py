@@ -345,6 +345,12 @@ class FockEngine:
         _lib.check(self._L.fjb_set_class_config(self._h, *map(int, cls), int(threads),
                                                 int(slots)), self._h)
 
+    def set_class_config32(self, cls, threads: int = 0, slots: int = 0) -> None:
+        """The same for the routed path's FP32 interpreter kernel of a class
+        (0, 0 = the FP64 configuration's FP32 twin)."""
+        _lib.check(self._L.fjb_set_class_config32(self._h, *map(int, cls), int(threads),
+                                                  int(slots)), self._h)
+
     def launch_stats(self) -> list[dict]:
         """Per launch: class, degrees, quartets met and computed by the last
         build."""

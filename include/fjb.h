@@ -294,6 +294,10 @@ int fjb_class_stats(const fjb_handle *h, fjb_class_stat *out, int64_t n, int64_t
  * reference's performance/dispatch.py:1-45 picks a batch count from measured
  * medians.  FJB_E_LIMIT if the class does not fit that configuration. */
 int fjb_set_class_config(fjb_handle *h, int la, int lb, int lc, int ld, int threads, int slots);
+/* The same for the routed path's FP32 interpreter kernel of a class (used
+ * for its FP32 units when the class has no FP32 register body); threads 0
+ * and slots 0 restore the FP64 configuration's FP32 twin. */
+int fjb_set_class_config32(fjb_handle *h, int la, int lb, int lc, int ld, int threads, int slots);
 
 /* fjb_fock_build without any device allocation (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc while they run the
