@@ -16,7 +16,10 @@ import os
 
 import numpy as np
 
-CANDIDATES = ((1, 0), (32, 0), (64, 0), (128, 0), (256, 0), (512, 0))  # (1, 0): register kernel
+# (threads, slots): (1, 0) the register kernel; slots 0 the layout's default
+# chunk, 1 the single-slot path forced
+CANDIDATES = ((1, 0), (32, 0), (64, 0), (128, 0), (256, 0), (512, 0), (32, 1), (64, 1), (128, 1), (256, 1),
+              (512, 1))
 
 
 def autotune(eng, D, candidates=CANDIDATES, reps: int = 1, precision: int = 0) -> dict:
@@ -59,7 +62,8 @@ def autotune(eng, D, candidates=CANDIDATES, reps: int = 1, precision: int = 0) -
                    for c, t in times.items()}}
 
 
-CANDIDATES32 = ((32, 0), (64, 0), (128, 0), (256, 0), (512, 0), (64, 1), (128, 1), (128, 2), (256, 4))
+CANDIDATES32 = ((32, 0), (64, 0), (128, 0), (256, 0), (512, 0), (32, 1), (64, 1), (128, 1), (256, 1), (512, 1),
+                (128, 2))
 
 
 def autotune32(eng, D, candidates=CANDIDATES32, reps: int = 1) -> dict:
