@@ -562,84 +562,61 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                     __syncthreads();
                     continue;
                 }
-                // the six-block digest
+                // the six-block digest (kernel_f.py:94-131): per output
+                // element its contraction with one density block, then the
+                // bra block into Jab (shared), the five ket blocks by FP64
+                // atomics -- or, in the atomics-free build, into the
+                // quartet's own slots (this order, n2..n6, is BLOCKS[1:]'s)
                 {
                     const int oa = bra.ao_a, ob = bra.ao_b, oc = ket.ao_a, od = ket.ao_b;
                     const int n1 = nab, n2 = n1 + ncd, n3 = n2 + na * nc, n4 = n3 + na * nd,
                               n5 = n4 + nb * nc, n6 = n5 + nb * nd;
                     const double w2 = 2.0 * deg;
-                    // the atomics-free build: the five ket blocks (this
-                    // order, n2..n6) into the quartet's own slots
                     double *wq = A.W ? ket_slots(A, U.launch, LR.n_ket, U.ib, ik, nab, n6 - n1) : nullptr;
                     for (int o = tid; o < n6; o += nt) {
-                        double acc = 0.0;
-                        if (o >= n1 && wq) {
-                            const int e = o - n1;
-                            if (o < n2) {
-                                const int kl = o - n1;
-                                for (int ij = 0; ij < nab; ++ij) acc += Dab[ij] * Y[(size_t)ij * ncd + kl];
-                                acc *= w2;
-                            } else if (o < n3) {
-                                const int r = o - n2, i = r / nc, k = r % nc;
-                                for (int j = 0; j < nb; ++j)
-                                    for (int l = 0; l < nd; ++l)
-                                        acc += Dbd[j * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                                acc *= deg;
-                            } else if (o < n4) {
-                                const int r = o - n3, i = r / nd, l = r % nd;
-                                for (int j = 0; j < nb; ++j)
-                                    for (int k = 0; k < nc; ++k)
-                                        acc += Dbc[j * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                                acc *= deg;
-                            } else if (o < n5) {
-                                const int r = o - n4, j = r / nc, k = r % nc;
-                                for (int i = 0; i < na; ++i)
-                                    for (int l = 0; l < nd; ++l)
-                                        acc += Dad[i * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                                acc *= deg;
-                            } else {
-                                const int r = o - n5, j = r / nd, l = r % nd;
-                                for (int i = 0; i < na; ++i)
-                                    for (int k = 0; k < nc; ++k)
-                                        acc += Dac[i * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                                acc *= deg;
-                            }
-                            wq[(size_t)e * LR.n_ket] = acc;
-                            continue;
-                        }
+                        double acc = 0.0, w = deg;
+                        size_t x = 0;  // the J' or K' element of an atomic add
+                        double *M = A.Kp;
                         if (o < n1) {
                             const R *y = Y + (size_t)o * ncd;
                             for (int kl = 0; kl < ncd; ++kl) acc += Dcd[kl] * y[kl];
                             Jab[o] += w2 * acc;
+                            continue;
                         } else if (o < n2) {
                             const int kl = o - n1;
                             for (int ij = 0; ij < nab; ++ij) acc += Dab[ij] * Y[(size_t)ij * ncd + kl];
-                            atomicAdd(A.Jp + (size_t)(oc + kl / nd) * n_ao + od + kl % nd, w2 * acc);
+                            w = w2;
+                            M = A.Jp;
+                            x = (size_t)(oc + kl / nd) * n_ao + od + kl % nd;
                         } else if (o < n3) {
                             const int r = o - n2, i = r / nc, k = r % nc;
                             for (int j = 0; j < nb; ++j)
                                 for (int l = 0; l < nd; ++l)
                                     acc += Dbd[j * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                            atomicAdd(A.Kp + (size_t)(oa + i) * n_ao + oc + k, deg * acc);
+                            x = (size_t)(oa + i) * n_ao + oc + k;
                         } else if (o < n4) {
                             const int r = o - n3, i = r / nd, l = r % nd;
                             for (int j = 0; j < nb; ++j)
                                 for (int k = 0; k < nc; ++k)
                                     acc += Dbc[j * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                            atomicAdd(A.Kp + (size_t)(oa + i) * n_ao + od + l, deg * acc);
+                            x = (size_t)(oa + i) * n_ao + od + l;
                         } else if (o < n5) {
                             const int r = o - n4, j = r / nc, k = r % nc;
                             for (int i = 0; i < na; ++i)
                                 for (int l = 0; l < nd; ++l)
                                     acc += Dad[i * nd + l] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                            atomicAdd(A.Kp + (size_t)(ob + j) * n_ao + oc + k, deg * acc);
+                            x = (size_t)(ob + j) * n_ao + oc + k;
                         } else {
                             const int r = o - n5, j = r / nd, l = r % nd;
                             for (int i = 0; i < na; ++i)
                                 for (int k = 0; k < nc; ++k)
                                     acc += Dac[i * nc + k] * Y[(size_t)(i * nb + j) * ncd + k * nd + l];
-                            atomicAdd(A.Kp + (size_t)(ob + j) * n_ao + od + l, deg * acc);
+                            x = (size_t)(ob + j) * n_ao + od + l;
                         }
+                        if (wq)
+                            wq[(size_t)(o - n1) * LR.n_ket] = w * acc;
+                        else
+                            atomicAdd(M + x, w * acc);
                     }
                 }
                 __syncthreads();
