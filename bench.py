@@ -139,11 +139,14 @@ def _time_quartets(args):
     return out
 
 
-def cpu_sample(w, lstats, plan, cores: int, budget_s: float = 20.0, seed: int = 0):
+def cpu_sample(w, lstats, plan, cores: int, budget_s: float = 15.0, seed: int = 0):
     """Estimated ms of the whole build on the oracle: per (class, K_AB, K_CD)
     launch key, time the oracle's ERI block on sampled computed-class
     quartets of that key; weight by the computed counts of the last GPU
-    build.  Returns (ms_estimate, description, cpu_seconds_spent)."""
+    build.  A pilot of 2 quartets per key sets how many more each key gets
+    so that the sampled CPU work comes to about `budget_s` seconds (at most
+    200 per key).  Returns (ms_estimate, description, cpu_seconds_spent,
+    wall_seconds)."""
     import multiprocessing as mp
     rng = np.random.default_rng(seed)
     keys = {}
@@ -153,27 +156,42 @@ def cpu_sample(w, lstats, plan, cores: int, budget_s: float = 20.0, seed: int = 
         k = (s["la"], s["lb"], s["lc"], s["ld"], s["kab"], s["kcd"])
         keys.setdefault(k, []).append(li)
     batches = plan.batches
-    samples, owners = [], []
-    for k, lis in sorted(keys.items()):
-        L = plan.launches[lis[int(rng.integers(len(lis)))]]
-        for _ in range(2):
-            bp = batches[L.bra].pairs[int(rng.integers(len(batches[L.bra].pairs)))]
-            kp = batches[L.ket].pairs[int(rng.integers(len(batches[L.ket].pairs)))]
-            samples.append((bp.a, bp.b, kp.a, kp.b))
-            owners.append(k)
     f = w.basis.flat()
     flat = (f["l"], f["centre"], f["prim0"], f["nprim"], f["exps"], f["coefs"])
-    chunks = [samples[i::cores] for i in range(cores)]
+
+    def draw(n_per):
+        samples, owners = [], []
+        for k, lis in sorted(keys.items()):
+            for _ in range(n_per):
+                L = plan.launches[lis[int(rng.integers(len(lis)))]]
+                bp = batches[L.bra].pairs[int(rng.integers(len(batches[L.bra].pairs)))]
+                kp = batches[L.ket].pairs[int(rng.integers(len(batches[L.ket].pairs)))]
+                samples.append((bp.a, bp.b, kp.a, kp.b))
+                owners.append(k)
+        return samples, owners
+
+    def run(samples, owners, per):
+        chunks = [samples[i::cores] for i in range(cores)]
+        with mp.get_context("spawn").Pool(cores) as pool:
+            res = pool.map(_time_quartets, [(flat, c) for c in chunks])
+        spent = 0.0
+        for i in range(cores):
+            for idx, t in zip(range(i, len(samples), cores), res[i]):
+                per.setdefault(owners[idx], []).append(t)
+                spent += t
+        return spent
+
+    per: dict = {}
     t0 = time.perf_counter()
-    with mp.get_context("spawn").Pool(cores) as pool:
-        res = pool.map(_time_quartets, [(flat, c) for c in chunks])
+    pilot = draw(2)
+    spent = run(*pilot, per)
+    n_more = int(min(200, max(0, 2 * (budget_s / max(spent, 1e-9) - 1))))
+    n_samples = len(pilot[0])
+    if n_more:
+        more = draw(n_more)
+        spent += run(*more, per)
+        n_samples += len(more[0])
     wall = time.perf_counter() - t0
-    per = {}
-    flat_times = []
-    for i in range(cores):
-        flat_times.extend(zip(range(i, len(samples), cores), res[i]))
-    for idx, t in flat_times:
-        per.setdefault(owners[idx], []).append(t)
     total_cpu_s = 0.0
     for k, lis in keys.items():
         # the oracle sums every primitive pair of the sampled shells (no
@@ -181,10 +199,10 @@ def cpu_sample(w, lstats, plan, cores: int, budget_s: float = 20.0, seed: int = 
         cnt = sum(lstats[li]["computed"] for li in lis)
         total_cpu_s += cnt * float(np.median(per[k]))
     ms = 1e3 * total_cpu_s / cores
-    spent = float(sum(t for _, t in flat_times))
-    desc = (f"oracle eri_block (MMD, FP64) on {len(samples)} sampled quartets, 2 per "
-            f"(class, K_AB, K_CD) key of the build's computed launches, median time per key "
-            f"x computed quartets, summed, / {cores} core(s); digest not timed")
+    desc = (f"oracle eri_block (MMD, FP64) on {n_samples} sampled quartets, {2 + n_more} per "
+            f"(class, K_AB, K_CD) key of the build's computed launches ({len(keys)} keys), median time "
+            f"per key x computed quartets, summed, / {cores} core(s); {spent:.1f} s of CPU sampled; "
+            f"digest not timed")
     return ms, desc, spent, wall
 
 
