@@ -72,6 +72,7 @@ def load():
     L.fjb_fock_build.argtypes = [vp, vp, vp, vp, vp, C.c_int, dbl, vp]
     L.fjb_fock_build_host.argtypes = [vp, vp, vp, vp, vp, C.c_int, dbl]
     L.fjb_eri_blocks.argtypes = [vp, vp, C.c_int, vp, vp]
+    L.fjb_eri_blocks_fp32.argtypes = [vp, vp, C.c_int, vp, vp]
     L.fjb_boys.argtypes = [C.c_int, vp, C.c_int, vp]
     L.fjb_last_build_stats.argtypes = [vp, C.POINTER(dbl), C.POINTER(C.c_int)]
     L.fjb_launch_stats.argtypes = [vp, vp, i64]
@@ -100,7 +101,7 @@ def load():
 
 EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_ao",
            "fjb_plan", "fjb_plan_counts", "fjb_plan_export", "fjb_screen_mask",
-           "fjb_fock_build", "fjb_fock_build_host", "fjb_eri_blocks", "fjb_boys",
+           "fjb_fock_build", "fjb_fock_build_host", "fjb_eri_blocks", "fjb_eri_blocks_fp32", "fjb_boys",
            "fjb_last_build_stats", "fjb_launch_stats", "fjb_class_stats",
            "fjb_fma_probe", "fjb_fock_build_noalloc", "fjb_set_class_config", "fjb_set_class_config32",
            "fjb_fock_build_graph", "fjb_create_df", "fjb_df_blocks", "fjb_mlp_n_params",

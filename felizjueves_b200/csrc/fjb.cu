@@ -1583,7 +1583,10 @@ int fjb_fock_build_host(fjb_handle *h, const double *D_host, double *J_host, dou
     return FJB_OK;
 }
 
-int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_dev, int64_t *offsets) {
+namespace {
+// The ERI tap: the interpreter kernel in tap mode, FP64 or (fp32) with the
+// routed path's FP32 recurrences.
+int eri_blocks_impl(fjb_handle *h, const int32_t *quartets, int n, double *out_dev, int64_t *offsets, bool fp32) {
     if (!h || !quartets || n < 0 || !offsets) return fail(h, FJB_E_ARG, "null argument");
     if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
     cudaSetDevice(h->device);
@@ -1641,7 +1644,8 @@ int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_de
         for (auto &kv : by_class) {
             auto [la, lb, lc, ld] = kv.first;
             ClassEntry &ce = h->cls(la, lb, lc, ld);
-            ClassDev dev = ce.dev(deg[kv.first].first, deg[kv.first].second);
+            ClassDev dev = fp32 ? ce.dev(deg[kv.first].first, deg[kv.first].second, 0, 0, 4)
+                                : ce.dev(deg[kv.first].first, deg[kv.first].second);
             std::vector<Unit> us;
             std::vector<int64_t> toff;
             for (int qi : kv.second) {
@@ -1665,7 +1669,10 @@ int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_de
             a.tap_out = out_dev;
             a.tap_off = dto.p;
             a.boys_tab = h->boys.p;
-            CUDA_OK(h, launch_hgp<double>(dev, grid_for(dev, a.n_units), nullptr, a));
+            if (fp32)
+                CUDA_OK(h, launch_hgp<float>(dev, grid_for<float>(dev, a.n_units), nullptr, a));
+            else
+                CUDA_OK(h, launch_hgp<double>(dev, grid_for(dev, a.n_units), nullptr, a));
             CUDA_OK(h, cudaDeviceSynchronize());
         }
     } catch (const std::length_error &e) {
@@ -1674,6 +1681,15 @@ int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_de
         return fail(h, FJB_E_CUDA, e.what());
     }
     return FJB_OK;
+}
+}  // namespace
+
+int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_dev, int64_t *offsets) {
+    return eri_blocks_impl(h, quartets, n, out_dev, offsets, false);
+}
+
+int fjb_eri_blocks_fp32(fjb_handle *h, const int32_t *quartets, int n, double *out_dev, int64_t *offsets) {
+    return eri_blocks_impl(h, quartets, n, out_dev, offsets, true);
 }
 
 int fjb_route_stats(const fjb_handle *hc, int64_t *n32, int64_t *n64) {

@@ -383,17 +383,18 @@ class FockEngine:
         torch.cuda.synchronize(Dt.device)
         return m.cpu().numpy()
 
-    def eri_blocks(self, quartets) -> list[np.ndarray]:
+    def eri_blocks(self, quartets, fp32: bool = False) -> list[np.ndarray]:
         """(ab|cd) of ordered shell quartets, each a (n_a n_b, n_c n_d) array
-        in the reference's eri_block layout."""
+        in the reference's eri_block layout; `fp32` with the routed path's
+        FP32 recurrences (what a quartet routed to FP32 contributes)."""
         import torch
         q = np.ascontiguousarray(np.asarray(quartets, np.int32).reshape(-1, 4))
         off = np.zeros(len(q) + 1, np.int64)
         sizes = [np.prod([self.basis.shells[s].n_cart for s in row]) for row in q]
         total = int(np.sum(sizes)) if len(q) else 0
         out = torch.zeros(max(total, 1), dtype=torch.float64, device=f"cuda:{self.device}")
-        _lib.check(self._L.fjb_eri_blocks(self._h, q.ctypes.data, len(q), out.data_ptr(),
-                                          off.ctypes.data), self._h)
+        fn = self._L.fjb_eri_blocks_fp32 if fp32 else self._L.fjb_eri_blocks
+        _lib.check(fn(self._h, q.ctypes.data, len(q), out.data_ptr(), off.ctypes.data), self._h)
         flat = out.cpu().numpy()
         res = []
         for i, row in enumerate(q):

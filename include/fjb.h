@@ -170,6 +170,12 @@ int fjb_fock_build_host(fjb_handle *h, const double *D_host, double *J_host,
  * Synchronises. */
 int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_dev,
                    int64_t *offsets);
+/* The same blocks with the routed path's FP32 recurrences (VRR, boundary and
+ * HRR in FP32; Boys and scalars FP64): what a quartet routed to FP32
+ * contributes, for measuring its FP32 error (eri/fock/levers/mixed.py's
+ * fmixed regions). */
+int fjb_eri_blocks_fp32(fjb_handle *h, const int32_t *quartets, int n, double *out_dev,
+                        int64_t *offsets);
 
 /* Density fitting (eri/density_fit/metric.py:228 metric_matrix,
  * eri3.py:226 eri3_tensor).  fjb_create_df makes a handle over the AO basis

@@ -305,3 +305,23 @@ def test_atomics_free_build_reproducible(cuda, lib_built, oracle_lib, wname, tau
     torch.cuda.synchronize()
     for a, b in zip(out, runs[0]):
         assert torch.equal(a, b)
+
+
+def test_fp32_tap_is_the_routed_arithmetic(cuda, lib_built):
+    """fjb_eri_blocks_fp32 (the FP32 recurrences a routed quartet runs)
+    agrees with the FP64 tap to FP32 accuracy measured on the whole sample,
+    while single quartets can lose digits to cancellation (the HRR's |AB|^k
+    factors): the spread is reported."""
+    w = configs.c0()
+    z = golden("eri_c0.npz")
+    eng = FockEngine(w.basis)
+    b64 = eng.eri_blocks(z["quartets"])
+    b32 = eng.eri_blocks(z["quartets"], fp32=True)
+    err = np.array([np.abs(x - y).max() for x, y in zip(b32, b64)])
+    mag = np.array([np.abs(y).max() for y in b64])
+    big = max(mag)
+    rel = err[mag > 0] / mag[mag > 0]
+    print(f"FP32 tap: max|d|/max|ERI| {err.max() / big:.2e}; per-quartet relative error "
+          f"median {np.median(rel):.1e}, 99th percentile {np.percentile(rel, 99):.1e}")
+    assert np.all(np.isfinite(err))
+    assert err.max() <= 1e-5 * big
