@@ -381,14 +381,19 @@ __global__ void __launch_bounds__(128) j_pq_kernel(const JRec *__restrict__ recs
     }
 }
 
-// The kets of every L in key order as a contiguous stream: (P, eta) and the
-// D_q offset of the k-th sorted ket, so the walk's loads are coalesced.
+// The kets of every L in key order as a contiguous stream: (P, eta) of the
+// k-th sorted ket, and its D_q copied into the D_q slot of position k (a
+// group's slots have one stride, so position k's slot is record k's), so the
+// walk's loads of consecutive kets are consecutive in memory.
 __global__ void j_gather_kernel(const JRec *__restrict__ recs, const int *__restrict__ order, int n,
-                                double4 *__restrict__ kst, int *__restrict__ kdq) {
+                                const double *__restrict__ Dq, double4 *__restrict__ kst, int *__restrict__ kdq,
+                                double *__restrict__ Dqs) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const JRec R = recs[order[k]];
+        const int dst = recs[k].dq_off;
         kst[k] = make_double4(R.P[0], R.P[1], R.P[2], R.zeta);
-        kdq[k] = R.dq_off;
+        kdq[k] = dst;
+        for (int q = 0; q < nh(R.L); ++q) Dqs[dst + q] = Dq[R.dq_off + q];
     }
 }
 
@@ -532,7 +537,7 @@ struct JEngine {
     DBuf<JRec> recs;
     DBuf<int> pair_rec0, pair_nrec, seg_off, iota, order, kdq;
     DBuf<double4> kst;
-    DBuf<double> Dq, Jp, key, skey;
+    DBuf<double> Dq, Dqs, Jp, key, skey;
     DBuf<unsigned char> sort_tmp;
     size_t sort_bytes = 0;
 };
@@ -598,6 +603,7 @@ JEngine *jengine_create(const HostBasis &basis, int device, std::string *err) {
     if (ce == cudaSuccess) ce = e->kdq.alloc(std::max(e->n_rec, 1));
     if (ce == cudaSuccess) ce = e->kst.alloc(std::max(e->n_rec, 1));
     if (ce == cudaSuccess) ce = e->Dq.alloc(std::max(dq, 1));
+    if (ce == cudaSuccess) ce = e->Dqs.alloc(std::max(dq, 1));
     if (ce == cudaSuccess) ce = e->Jp.alloc(std::max(dq, 1));
     if (ce == cudaSuccess) ce = e->key.alloc(std::max(e->n_rec, 1));
     if (ce == cudaSuccess) ce = e->skey.alloc(std::max(e->n_rec, 1));
@@ -638,7 +644,7 @@ int jengine_build(JEngine *e, const double *D_dev, double *J_dev, double tau, co
                "segmented sort"))
         return -2;
     ++nl;
-    j_gather_kernel<<<rec_grid, 128, 0, st>>>(e->recs.p, e->order.p, e->n_rec, e->kst.p, e->kdq.p);
+    j_gather_kernel<<<rec_grid, 128, 0, st>>>(e->recs.p, e->order.p, e->n_rec, e->Dq.p, e->kst.p, e->kdq.p, e->Dqs.p);
     ++nl;
     if (!check(cudaGetLastError(), "j_gather_kernel")) return -2;
     if (!check(cudaMemsetAsync(e->Jp.p, 0, e->Jp.n * sizeof(double), st), "memset")) return -2;
@@ -650,10 +656,10 @@ int jengine_build(JEngine *e, const double *D_dev, double *J_dev, double tau, co
             const int k0 = e->L_off[lq], nk = e->L_off[lq + 1] - k0;
             if (nk == 0) continue;
             if (lp + lq <= kSmallL)
-                kPqSmall[lp][lq](grid, st, e->recs.p, b0, nb, k0, nk, e->kst.p, e->kdq.p, e->skey.p, e->Dq.p, e->Jp.p, tau,
+                kPqSmall[lp][lq](grid, st, e->recs.p, b0, nb, k0, nk, e->kst.p, e->kdq.p, e->skey.p, e->Dqs.p, e->Jp.p, tau,
                                  boys_tab);
             else
-                kPqTable[lp + lq](grid, st, e->recs.p, lp, lq, b0, nb, k0, nk, e->kst.p, e->kdq.p, e->skey.p, e->Dq.p,
+                kPqTable[lp + lq](grid, st, e->recs.p, lp, lq, b0, nb, k0, nk, e->kst.p, e->kdq.p, e->skey.p, e->Dqs.p,
                                   e->Jp.p, tau, boys_tab);
             ++nl;
             if (!check(cudaGetLastError(), "j_pq_kernel")) return -2;
