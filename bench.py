@@ -219,15 +219,11 @@ def main():
         return side_path(a, local)
 
     import torch
-    from felizjueves_b200 import _lib, configs, cost
+    from felizjueves_b200 import _lib, configs, cost, replicas
     from felizjueves_b200.fock import FockEngine
 
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dist = replicas.init(world, "nccl")
     w = configs.by_name(a.workload)
     eng = FockEngine(w.basis, device=local)
     P = eng.plan(w.D, w.tau, w.n_mag)
@@ -254,8 +250,7 @@ def main():
         torch.cuda.synchronize()
         clocks = Clocks(local)
         clocks.start()
-        if dist:
-            dist.barrier()
+        replicas.barrier(dist)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -265,14 +260,9 @@ def main():
             eng.build(Dw, J=J, K=K, G=G, precision=prec, threshold=thr, graph=True)
         e1.record(stream)
         torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        ms_ = e0.elapsed_time(e1) / a.steps
+        replicas.barrier(dist)
         ck_ = clocks.stop()
-        if dist:
-            t = torch.tensor([ms_], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_ = float(t.item())
+        ms_ = replicas.max_over_ranks(dist, e0.elapsed_time(e1) / a.steps, f"cuda:{local}")
         return ms_, ck_, eng.last_build_stats()[1], eng.class_stats(), eng.launch_stats(), G.clone()
 
     ms64, ck64, nl64, cs, ls, G64 = timed(_lib.FJB_FP64)
@@ -355,8 +345,7 @@ def main():
     }
     if rank == 0:
         print(json.dumps(out))
-    if dist:
-        dist.destroy_process_group()
+    replicas.finish(dist)
 
 
 def ctypes_probe(_lib, fp32: int) -> float:
