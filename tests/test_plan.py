@@ -104,3 +104,17 @@ def test_l_above_limit_refused(lib_built):
     B = Basis((Shell(4, (0.0, 0.0, 0.0), [1.0], [1.0]),))
     with pytest.raises(ValueError, match="above the compiled maximum"):
         FockEngine(B, device=-1)
+
+
+def test_pair_degree_limit(lib_built):
+    """A shell pair of more than MAX_PRIM_PAIRS = 128 primitive pairs is
+    refused (the interpreter stages a pair's primitives in shared memory,
+    kernel_f.py:196-203); 11 x 11 = 121 is planned whole."""
+    from felizjueves_b200.shell import Basis, Shell
+    ex = list(np.geomspace(0.1, 50.0, 12))
+    B = Basis((Shell(0, (0.0, 0.0, 0.0), ex, [1.0] * 12),))
+    with pytest.raises(ValueError, match="MAX_PRIM_PAIRS"):
+        FockEngine(B, device=-1).plan(np.ones((1, 1)), 0.0, 4)
+    B = Basis((Shell(0, (0.0, 0.0, 0.0), ex[:11], [1.0] * 11),))
+    P = FockEngine(B, device=-1).plan(np.ones((1, 1)), 0.0, 4)
+    assert [b.degree for b in P.batches] == [121]
