@@ -352,7 +352,8 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
             if (slots == 1) {
                 // One primitive quartet at a time (ng == 1): every thread
                 // holds its scalars in registers; the Boys leaves of all K
-                // primitive quartets are evaluated first, one thread each.
+                // primitive quartets are evaluated first, one thread each
+                // (layouts give one slot only when those leaves fit).
                 double *Fq = sm + C.sm_F;
                 for (int t = tid; t < K; t += nt) {
                     const int ikcd = t / kab, ikab = t - ikcd * kab;

@@ -265,8 +265,14 @@ void default_config(const ClassHost &c, int budget, int *threads, int *target) {
     }
 }
 
-bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, int threads, int target,
-                  int force_slots, ClassDev *o, int rsize) {
+namespace {
+
+// One carve-up attempt.  stage_leaves: room for the single-slot path's Boys
+// leaves of every primitive quartet of a quartet (one slot allowed);
+// without it the class keeps at least two slots (the slot path, which
+// evaluates its leaves slot by slot).
+bool layout_try(const ClassHost &c, int max_kab, int max_kcd, int budget, int threads, int target,
+                int force_slots, ClassDev *o, int rsize, bool stage_leaves) {
     *o = ClassDev{};
     o->la = c.la;
     o->lb = c.lb;
@@ -292,13 +298,13 @@ bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, int 
     auto dd = [&](long n) { return (int)((n + 1) & ~1L); };
     const int hr = c.nab * c.nbf + c.nab * c.ncd;
     const int dblk = c.nab + c.ncd + c.na * c.nc + c.na * c.nd + c.nb * c.nc + c.nb * c.nd;
-    // the single-slot path's Boys leaves of every primitive quartet of a quartet
-    const int fleaves = max_kab * max_kcd * (c.L + 1);
+    const int min_slots = stage_leaves ? 1 : 2;
+    const int fleaves = stage_leaves ? max_kab * max_kcd * (c.L + 1) : 0;
     const int fixed = dd(kPrimWords * max_kab) + rd(o->n_cb) + rd(o->n_ck) + dd(dblk) + dd(c.nab) + dd(fleaves);
     // Slots span (ket, primitive quartet) pairs: up to one per thread, and
     // no more than a full unit of kets needs.
-    int want = std::max(1, std::min(threads, kKetChunk * max_kab * max_kcd));
-    int slots = force_slots > 0 ? std::min(force_slots, threads) : want;
+    int want = std::max(min_slots, std::min(threads, kKetChunk * max_kab * max_kcd));
+    int slots = force_slots > 0 ? std::max(min_slots, std::min(force_slots, threads)) : want;
     auto group = [&](int s) { return std::max(1, std::min(kKetChunk, s)); };
     // per ket of a group: its boundary and its staged primitive pairs
     auto total = [&](int s) {
@@ -308,8 +314,8 @@ bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, int 
     // Occupancy first: shrink the chunk until the CTA fits its target,
     // unless one slot already needs more; then stay inside the hard budget.
     if (force_slots <= 0)
-        while (slots > 1 && total(slots) > target) --slots;
-    while (slots > 1 && total(slots) > budget) --slots;
+        while (slots > min_slots && total(slots) > target) --slots;
+    while (slots > min_slots && total(slots) > budget) --slots;
     o->threads = threads;
     if (total(slots) > budget) return false;
     o->slots = slots;
@@ -333,6 +339,17 @@ bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, int 
     o->sm_F = take(dd(fleaves));
     o->sm_total = off;
     return off <= budget;
+}
+
+}  // namespace
+
+bool layout_class(const ClassHost &c, int max_kab, int max_kcd, int budget, int threads, int target,
+                  int force_slots, ClassDev *o, int rsize) {
+    // The single-slot path's staged leaves first (every layout of the
+    // degrees the kernels were tuned on); a class whose leaves do not fit
+    // beside its values (high contraction degrees) runs on two or more slots.
+    return layout_try(c, max_kab, max_kcd, budget, threads, target, force_slots, o, rsize, true) ||
+           layout_try(c, max_kab, max_kcd, budget, threads, target, force_slots, o, rsize, false);
 }
 
 }  // namespace fjb
