@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--workload", default="c1")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--path", default="fock", choices=["fock", "coulomb", "df", "batch"],
+    ap.add_argument("--path", default="fock", choices=["fock", "coulomb", "df", "batch", "onee"],
                     help="fock: the G build (the headline); coulomb: the MMD J-engine; "
                          "df: DF-J/K (FP64 and split-BF16 tensor-core GEMMs); batch: the "
                          "uneven molecule batch (c4) as one captured graph")
@@ -417,6 +417,37 @@ def side_path(a, local):
         ms, _ = timed(lambda: eng.coulomb(D, tau=w.tau, J=J))
         line.update(metric="J-engine J build ms/iter", value=round(ms, 3), unit="ms/iter",
                     gpu_launches=eng.j_launches())
+    elif a.path == "onee":
+        # S, T, V and H = T + V; one nucleus of charge 1 + (k mod 9) per atom
+        from felizjueves_b200.fock import FockEngine
+        centres = []
+        for s_ in w.basis.shells:
+            if s_.centre not in centres:
+                centres.append(s_.centre)
+        nuclei = [(float(1 + k % 9), c) for k, c in enumerate(centres)]
+        eng = FockEngine(w.basis, device=local)
+        outs = eng.one_electron(nuclei)
+        ms, _ = timed(lambda: eng.one_electron(nuclei, S=outs[0], T=outs[1], V=outs[2], H=outs[3]))
+        line.update(metric="one-electron S, T, V, H ms/iter", value=round(ms, 3), unit="ms/iter",
+                    n_nuclei=len(nuclei), shell_pairs=len(w.basis.shells) * (len(w.basis.shells) + 1) // 2,
+                    gpu_launches=10)
+        if not a.no_cpu:
+            # the oracle on a bounded sample of shell pairs, scaled by the pair count
+            import random
+            import time as _t
+            from oracle import one_electron as _o
+            rng = random.Random(0)
+            sh = w.basis.shells
+            pairs = [(i, j) for i in range(len(sh)) for j in range(i, len(sh))]
+            sample = rng.sample(pairs, min(300, len(pairs)))
+            t0 = _t.perf_counter()
+            for i, j in sample:
+                _o.blocks(sh[i], sh[j], nuclei)
+            spent = _t.perf_counter() - t0
+            line["cpu_baseline"] = {"value": round(spent / len(sample) * len(pairs) * 1e3, 1), "unit": "ms/iter",
+                                    "cores": 1, "kind": "port",
+                                    "sample": f"oracle one_electron.blocks on {len(sample)} random shell pairs "
+                                              f"of {len(pairs)}, {spent:.1f} s, scaled by the pair count"}
     else:
         from felizjueves_b200.df import DFEngine
         aux = configs.aux_basis(w)

@@ -95,6 +95,7 @@ def load():
     L.fjb_j_last_launches.argtypes = [vp]
     L.fjb_j_plan_lists.argtypes = [vp, vp, C.POINTER(JLists_t), C.POINTER(i64)]
     L.fjb_scatter_map.argtypes = [vp, C.c_int, vp, vp, vp, C.POINTER(i64), C.POINTER(i64)]
+    L.fjb_one_electron.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp, vp, vp]
     _lib = L
     return L
 
@@ -107,7 +108,7 @@ EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_
            "fjb_fock_build_graph", "fjb_create_df", "fjb_df_blocks", "fjb_mlp_n_params",
            "fjb_router_set", "fjb_router_features", "fjb_mlp_forward", "fjb_mlp_gradient",
            "fjb_mlp_adam", "fjb_route_stats", "fjb_coulomb", "fjb_j_last_launches",
-           "fjb_j_plan_lists", "fjb_scatter_map")
+           "fjb_j_plan_lists", "fjb_scatter_map", "fjb_one_electron")
 
 
 class LaunchStat_t(C.Structure):

@@ -25,6 +25,7 @@
 #include "fock_kernels.cuh"
 #include "hgp_tables.h"
 #include "jengine.h"
+#include "onee.h"
 #include "plan.h"
 #include "scatter.h"
 #include "router.cuh"
@@ -785,6 +786,7 @@ struct fjb_handle {
     int device = 0;
     HostBasis basis;
     fjb::JEngine *jeng = nullptr;  // the J-engine, built on first use
+    fjb::OneElectron *onee = nullptr;  // the one-electron shell pairs, built on first use
     int j_launches = 0;            // kernel launches of the last J-engine build
     std::string err;
     std::map<std::tuple<int, int, int, int>, std::unique_ptr<ClassEntry>> classes;
@@ -1154,6 +1156,7 @@ int fjb_create_df(fjb_handle **out, const fjb_basis *ao, const fjb_basis *aux, i
 void fjb_destroy(fjb_handle *h) {
     if (!h) return;
     if (h->jeng) jengine_destroy(h->jeng);
+    if (h->onee) onee_destroy(h->onee);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     delete h;
@@ -1836,6 +1839,29 @@ int fjb_coulomb(fjb_handle *h, const double *D_dev, double *J_dev, double tau, v
     if (jengine_build(h->jeng, D_dev, J_dev, tau, h->boys.p, (cudaStream_t)stream, &err, &nl))
         return fail(h, FJB_E_CUDA, err);
     h->j_launches = nl;
+    return FJB_OK;
+}
+
+int fjb_one_electron(fjb_handle *h, const double *charges, const double *coords, int n_nuc, double *S_dev,
+                     double *T_dev, double *V_dev, double *H_dev, void *stream) {
+    if (!h) return fail(h, FJB_E_ARG, "null argument");
+    if (n_nuc < 0 || (n_nuc > 0 && (!charges || !coords))) return fail(h, FJB_E_ARG, "nuclei: null or n_nuc < 0");
+    for (int q = 0; q < n_nuc; ++q)
+        if (!std::isfinite(charges[q]) || !std::isfinite(coords[3 * q]) || !std::isfinite(coords[3 * q + 1]) ||
+            !std::isfinite(coords[3 * q + 2]))
+            return fail(h, FJB_E_ARG, "nucleus " + std::to_string(q) + " has a non-finite charge or coordinate");
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    if (h->df) return fail(h, FJB_E_STATE, "a density-fitting handle has no one-electron matrices");
+    CUDA_OK(h, cudaSetDevice(h->device));
+    std::string err;
+    if (!h->onee) {
+        h->onee = onee_create(h->basis, h->device, &err);
+        if (!h->onee) return fail(h, FJB_E_CUDA, err);
+    }
+    int nl = 0;
+    if (onee_build(h->onee, charges, coords, n_nuc, S_dev, T_dev, V_dev, H_dev, h->boys.p, (cudaStream_t)stream,
+                   &err, &nl))
+        return fail(h, FJB_E_CUDA, err);
     return FJB_OK;
 }
 

@@ -13,6 +13,10 @@ Mirrors (paths within the reference project):
 * `eri_block(basis, a, b, c, d)`  eri/eri.py:145 -> the (ab|cd) block.
 * `FockEngine`  the reusable form: plan once per (basis, tau, n), then build
   for any symmetric D, on device tensors (torch) or host arrays (numpy).
+* `overlap_matrix`, `kinetic_matrix`, `potential_matrix`,
+  `core_hamiltonian`, `FockEngine.one_electron`  the one-electron matrices
+  the G build's caller needs (one_electron/overlap.py:67, kinetic.py:114,
+  potential.py:101; H = T + V).
 
 Refusals are the reference's: an asymmetric or non-finite D, a bad tau, an
 l or a contraction degree above the compiled limits raise ValueError.  There
@@ -315,6 +319,36 @@ class FockEngine:
         _lib.check(self._L.fjb_coulomb(self._h, D.data_ptr(), J.data_ptr(), tau, C.c_void_p(st)), self._h)
         return J
 
+    # -- the one-electron matrices (one_electron/) ---------------------------
+    def one_electron(self, nuclei, *, S=None, T=None, V=None, H=None, want=("S", "T", "V", "H")):
+        """(S, T, V, H) of the basis as device tensors (H = T + V, the core
+        Hamiltonian), for nuclei [(Z, (x, y, z)), ...] in Bohr
+        (one_electron/overlap.py, kinetic.py, potential.py; potential.py's
+        Nucleus).  Matrices not in `want` are not computed into and come
+        back None; given tensors are written in full.  Needs no plan."""
+        import torch
+        nuc = _checked_nuclei(nuclei)
+        charges = np.ascontiguousarray([z for z, _ in nuc], np.float64)
+        coords = np.ascontiguousarray([c for _, c in nuc], np.float64).reshape(-1)
+        n = self.n_ao
+        dev = torch.device(f"cuda:{self.device}")
+        out = []
+        for name, M in (("S", S), ("T", T), ("V", V), ("H", H)):
+            if name not in want:
+                out.append(None)
+                continue
+            if M is None:
+                M = torch.empty((n, n), dtype=torch.float64, device=dev)
+            elif not (M.is_cuda and M.dtype == torch.float64 and tuple(M.shape) == (n, n) and M.is_contiguous()):
+                raise ValueError(f"{name} must be a contiguous cuda float64 ({n}, {n}) tensor")
+            out.append(M)
+        st = torch.cuda.current_stream(dev).cuda_stream
+        ptr = [None if M is None else M.data_ptr() for M in out]
+        _lib.check(self._L.fjb_one_electron(self._h, charges.ctypes.data if len(nuc) else None,
+                                            coords.ctypes.data if len(nuc) else None, len(nuc), *ptr,
+                                            C.c_void_p(st)), self._h)
+        return tuple(out)
+
     def j_launches(self) -> int:
         """Kernel launches of the last `coulomb` call."""
         return int(self._L.fjb_j_last_launches(self._h))
@@ -406,6 +440,43 @@ class FockEngine:
 def f_launches(basis: Basis, D, *, tau: float, n: int, device: int = 0) -> FPlan:
     eng = FockEngine(basis, device)
     return eng.plan(D, tau, n)
+
+
+def _checked_nuclei(nuclei) -> list[tuple[float, tuple[float, float, float]]]:
+    """Nuclei as [(Z, (x, y, z))], refused as the reference's _check_nuclei
+    does (one_electron/potential.py:67-76)."""
+    out = []
+    for nu in nuclei:
+        if len(nu) != 2:
+            raise ValueError(f"nucleus {nu!r} is not (Z, centre)")
+        Z, c = nu
+        if len(c) != 3:
+            raise ValueError(f"nucleus centre {c!r} is not three coordinates")
+        nz = (float(Z), (float(c[0]), float(c[1]), float(c[2])))
+        if not all(np.isfinite([nz[0], *nz[1]])):
+            raise ValueError(f"nucleus {nu!r} has a non-finite charge or coordinate")
+        out.append(nz)
+    return out
+
+
+def overlap_matrix(basis: Basis, *, device: int = 0) -> np.ndarray:
+    """S (one_electron/overlap.py:67), on the GPU."""
+    return FockEngine(basis, device).one_electron([], want=("S",))[0].cpu().numpy()
+
+
+def kinetic_matrix(basis: Basis, *, device: int = 0) -> np.ndarray:
+    """T (one_electron/kinetic.py:114), on the GPU."""
+    return FockEngine(basis, device).one_electron([], want=("T",))[1].cpu().numpy()
+
+
+def potential_matrix(basis: Basis, nuclei, *, device: int = 0) -> np.ndarray:
+    """V = -sum_C Z_C <a|1/r_C|b> (one_electron/potential.py:101), on the GPU."""
+    return FockEngine(basis, device).one_electron(nuclei, want=("V",))[2].cpu().numpy()
+
+
+def core_hamiltonian(basis: Basis, nuclei, *, device: int = 0) -> np.ndarray:
+    """H = T + V, on the GPU."""
+    return FockEngine(basis, device).one_electron(nuclei, want=("H",))[3].cpu().numpy()
 
 
 def coulomb_exchange(basis: Basis, D, *, tau: float = 0.0, n: int = 4, device: int = 0):

@@ -44,6 +44,13 @@
  *   fjb_j_plan_lists  eri/j_coulomb/launch.py:274-327 launches(): the
  *                                            records, bounds, keys and the
  *                                            sorted ket order
+ *   fjb_one_electron  one_electron/overlap.py:67 overlap_matrix,
+ *                     one_electron/kinetic.py:114 kinetic_matrix,
+ *                     one_electron/potential.py:101 potential_matrix (nuclei
+ *                                            (Z, centre)), assembled as
+ *                                            one_electron/one_electron.py:57
+ *                                            matrix; H = T + V the core
+ *                                            Hamiltonian
  *   fjb_last_error,
  *   fjb_destroy       the reference raises ValueError with a message
  *
@@ -254,6 +261,16 @@ int fjb_scatter_map(const fjb_handle *h, int launch, int32_t *el, int32_t *ptr, 
 
 /* Kernel launches of the last fjb_coulomb. */
 int fjb_j_last_launches(const fjb_handle *h);
+
+/* The one-electron matrices of the handle's basis: overlap S, kinetic
+ * energy T, nuclear attraction V = -sum_C Z_C <a|1/r_C|b> over n_nuc nuclei
+ * (charges[k], coords[3k..3k+2], HOST, Bohr; charges finite, n_nuc >= 0) and
+ * H = T + V, each n_ao x n_ao row-major on the DEVICE; any of the four may be
+ * NULL (not written), every element of the others is written, each exactly
+ * symmetric.  Stream-ordered; the first call stages the shell pairs
+ * (allocates). */
+int fjb_one_electron(fjb_handle *h, const double *charges, const double *coords, int n_nuc, double *S_dev,
+                     double *T_dev, double *V_dev, double *H_dev, void *stream);
 
 /* The J-engine's plan on the host for density D_host: per record (sweep
  * order: shell pairs a >= b, a outer; primitive pairs i outer) its shell

@@ -9,7 +9,7 @@ files this script writes.
 
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
-parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost jplan_c0 scatter_c0
+parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost jplan_c0 scatter_c0 onee
 (default: all
 but plan_c1 and jk_small, which take minutes).
 """
@@ -106,6 +106,67 @@ def part_libcint():
                             int2e_diag=diag, **sh,
                             source=np.asarray(f"test/oracle/fixtures/{name}_schwarz.json"))
         print("libcint schwarz", name, n)
+
+
+# --- one-electron matrices: libcint int1e_* and the reference's own S, T, V ---
+
+ONEE = ["h2_sto3g_j", "h2o_sto3g_j", "h2o_631g_j", "h2o_ccpvdz_j", "h10_chain_ccpvdz_j",
+        "hf_ccpvtz", "prim_spd_f", "prim_spdf"]
+
+
+def _fixture_arrays(d, n, *keys):
+    return [np.asarray(d["arrays"][k]["values"]).reshape(n, n) for k in keys]
+
+
+def part_onee():
+    fx = os.path.join(REF, "test", "oracle", "fixtures")
+    todo = [(name, [name]) for name in ONEE] + [("co_ccpvtz", ["co_ccpvtz_j_st", "co_ccpvtz_j_vh"])]
+    for name, files in todo:
+        ds = [json.load(open(os.path.join(fx, f + ".json"))) for f in files]
+        for d in ds:
+            assert d["provenance"]["cart"] is True and d["provenance"]["mol"]["unit"] == "Bohr"
+        conv = ds[0]["converted"]["shells"]
+        n = ds[0]["nao"]
+        arr = {}
+        for d in ds:
+            arr.update({k: v for k, v in d["arrays"].items()})
+        dd = {"arrays": arr}
+        S, T, V, H = _fixture_arrays(dd, n, "int1e_ovlp", "int1e_kin", "int1e_nuc", "hcore")
+        atoms = ds[0]["atoms"]
+        sh = flat_shells([s["l"] for s in conv], [s["centre"] for s in conv],
+                         [s["exponents"] for s in conv],
+                         [s["coefficients"] for s in conv])
+        np.savez_compressed(os.path.join(HERE, f"onee_{name}.npz"), S=S, T=T, V=V, H=H,
+                            charges=np.asarray([a["charge"] for a in atoms], np.float64),
+                            coords=np.asarray([a["coord"] for a in atoms], np.float64), **sh,
+                            source=np.asarray(" + ".join(f"test/oracle/fixtures/{f}.json" for f in files)
+                                              + f" (PySCF {ds[0]['provenance']['pyscf']}, libcint "
+                                              f"{ds[0]['provenance']['libcint']})"))
+        print("onee", name, n)
+    # the reference's own S, T, V on the 3-atom seeded cluster (l to 3),
+    # nuclei of charges 3, 1, 2 on its atoms
+    from felizjueves.one_electron.kinetic import kinetic_matrix
+    from felizjueves.one_electron.overlap import overlap_matrix
+    from felizjueves.one_electron.potential import potential_matrix
+    from felizjueves.reference.pq import one_centre
+    from felizjueves_b200 import configs
+    w = configs.cluster(3, 5)
+    B = ref_basis(w.basis)
+    centres = []
+    for sh_ in w.basis.shells:
+        if sh_.centre not in centres:
+            centres.append(sh_.centre)
+    nuclei = [(float(z), c) for z, c in zip((3, 1, 2), centres)]
+    S = np.asarray(overlap_matrix(B))
+    T = np.asarray(kinetic_matrix(B))
+    V = np.asarray(potential_matrix(B, nuclei, one_centre=one_centre))
+    np.savez_compressed(os.path.join(HERE, "onee_ref_cluster3.npz"), S=S, T=T, V=V,
+                        charges=np.asarray([z for z, _ in nuclei]),
+                        coords=np.asarray([c for _, c in nuclei]),
+                        source=np.asarray("reference one_electron overlap_matrix, kinetic_matrix, "
+                                          "potential_matrix (one_centre from reference/pq.py) on "
+                                          "configs.cluster(3, 5)"))
+    print("onee reference cluster3", w.basis.n_ao)
 
 
 # --- density fitting: libcint (P|Q) rows and (mn|P) columns -------------------
@@ -482,7 +543,8 @@ def part_cost():
 PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_eri,
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "jk_small": part_jk_small,
-         "cost": part_cost, "jplan_c0": part_jplan_c0, "scatter_c0": part_scatter_c0}
+         "cost": part_cost, "jplan_c0": part_jplan_c0, "scatter_c0": part_scatter_c0,
+         "onee": part_onee}
 DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
 
 

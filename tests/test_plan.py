@@ -118,3 +118,16 @@ def test_pair_degree_limit(lib_built):
     B = Basis((Shell(0, (0.0, 0.0, 0.0), ex[:11], [1.0] * 11),))
     P = FockEngine(B, device=-1).plan(np.ones((1, 1)), 0.0, 4)
     assert [b.degree for b in P.batches] == [121]
+
+
+def test_one_electron_refusals(lib_built):
+    """Nuclei are checked before any device work, as the reference's
+    _check_nuclei (one_electron/potential.py:67-76) does."""
+    w = configs.c0()
+    e = FockEngine(w.basis, device=-1)
+    with pytest.raises(ValueError, match="not \\(Z, centre\\)"):
+        e.one_electron([(1.0,)])
+    with pytest.raises(ValueError, match="three coordinates"):
+        e.one_electron([(1.0, (0.0, 0.0))])
+    with pytest.raises(ValueError, match="non-finite"):
+        e.one_electron([(float("nan"), (0.0, 0.0, 0.0))])
