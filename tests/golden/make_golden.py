@@ -10,7 +10,7 @@ files this script writes.
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
 parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost jplan_c0 scatter_c0 onee
-(default: all
+scf (default: all
 but plan_c1 and jk_small, which take minutes).
 """
 
@@ -167,6 +167,35 @@ def part_onee():
                                           "potential_matrix (one_centre from reference/pq.py) on "
                                           "configs.cluster(3, 5)"))
     print("onee reference cluster3", w.basis.n_ao)
+
+
+# --- converged closed-shell SCF: PySCF's RHF density and orbital energies ----
+
+SCF = ["h2o_sto3g_grad", "h2o_631g_grad", "h2o_ccpvdz_grad", "nh2f_631g_grad"]
+
+
+def part_scf():
+    fx = os.path.join(REF, "test", "oracle", "fixtures")
+    for name in SCF:
+        d = json.load(open(os.path.join(fx, name + ".json")))
+        assert d["provenance"]["cart"] is True and d["provenance"]["mol"]["unit"] == "Bohr"
+        assert d["provenance"]["mol"]["charge"] == 0 and d["provenance"]["mol"]["spin"] == 0
+        conv = d["converted"]["shells"]
+        n = d["nao"]
+        sh = flat_shells([s["l"] for s in conv], [s["centre"] for s in conv],
+                         [s["exponents"] for s in conv],
+                         [s["coefficients"] for s in conv])
+        atoms = d["atoms"]
+        np.savez_compressed(os.path.join(HERE, f"scf_{name.replace('_grad', '')}.npz"),
+                            D=np.asarray(d["arrays"]["density"]["values"]).reshape(n, n),
+                            mo_energy=np.asarray(d["arrays"]["mo_energy"]["values"]),
+                            mo_occ=np.asarray(d["arrays"]["mo_occ"]["values"]),
+                            charges=np.asarray([a["charge"] for a in atoms], np.float64),
+                            coords=np.asarray([a["coord"] for a in atoms], np.float64), **sh,
+                            source=np.asarray(f"test/oracle/fixtures/{name}.json ({d['density_recipe']}; "
+                                              f"PySCF {d['provenance']['pyscf']}, libcint "
+                                              f"{d['provenance']['libcint']})"))
+        print("scf", name, n)
 
 
 # --- density fitting: libcint (P|Q) rows and (mn|P) columns -------------------
@@ -544,7 +573,7 @@ PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "jk_small": part_jk_small,
          "cost": part_cost, "jplan_c0": part_jplan_c0, "scatter_c0": part_scatter_c0,
-         "onee": part_onee}
+         "onee": part_onee, "scf": part_scf}
 DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
 
 
