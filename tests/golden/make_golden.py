@@ -10,7 +10,7 @@ files this script writes.
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
 parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost jplan_c0 scatter_c0 onee
-scf (default: all
+scf bse (default: all
 but plan_c1 and jk_small, which take minutes).
 """
 
@@ -196,6 +196,51 @@ def part_scf():
                                               f"PySCF {d['provenance']['pyscf']}, libcint "
                                               f"{d['provenance']['libcint']})"))
         print("scf", name, n)
+
+
+# --- Basis Set Exchange documents: the elements the fixtures use -------------
+
+BSE_SETS = ["sto-3g.json", "6-31g.json", "cc-pVDZ.json", "cc-pVTZ.json"]
+BSE_ELEMENTS = ["1", "6", "7", "8", "9"]
+BSE_CASES = [("h2_sto3g_j", "sto-3g.json", False), ("h2o_631g_j", "6-31g.json", False),
+             ("h2o_ccpvdz_j", "cc-pVDZ.json", True), ("h2o_ccpvdz_j", "cc-pVDZ.json", False),
+             ("co_ccpvtz_j", "cc-pVTZ.json", True)]
+
+
+def part_bse():
+    """The reference's data/basis documents (BSE JSON, molssi_bse_schema),
+    cut to H, C, N, O, F and their electron shells, values verbatim."""
+    out = {}
+    for f in BSE_SETS:
+        d = json.load(open(os.path.join(REF, "data", "basis", f)))
+        out[f] = {"molssi_bse_schema": d["molssi_bse_schema"], "name": d["name"],
+                  "function_types": d["function_types"],
+                  "elements": {z: {"electron_shells": d["elements"][z]["electron_shells"]}
+                               for z in BSE_ELEMENTS}}
+    # the reference's own mapping (test/oracle/basis.py from_bse) of these
+    # documents onto shells, for the atoms of the one-electron fixtures
+    sys.path.insert(0, os.path.join(REF, "test"))
+    from felizjueves.ao import bse as ref_bse
+    from oracle.basis import from_bse as ref_from_bse
+    fx = os.path.join(REF, "test", "oracle", "fixtures")
+    for case, f, reduce in BSE_CASES:
+        d = json.load(open(os.path.join(fx, case + ".json")))
+        atoms = [(a["charge"], tuple(a["coord"])) for a in d["atoms"]]
+        B = ref_from_bse(ref_bse.load(os.path.join(REF, "data", "basis", f)), atoms, reduce=reduce)
+        sh = flat_shells([s_.l for s_ in B.shells], [s_.centre for s_ in B.shells],
+                         [s_.exponents for s_ in B.shells], [s_.coefficients for s_ in B.shells])
+        np.savez_compressed(os.path.join(HERE, f"bse_{case}{'_reduced' if reduce else ''}.npz"), **sh,
+                            source=np.asarray(f"reference test/oracle/basis.py from_bse(data/basis/{f}, "
+                                              f"atoms of {case}, reduce={reduce})"))
+        print("bse mapped", case)
+    sys.path.remove(os.path.join(REF, "test"))
+    for m in [m for m in sys.modules if m == "oracle" or m.startswith("oracle.")]:
+        del sys.modules[m]  # the reference's test oracle, not this repository's
+    with open(os.path.join(HERE, "bse_subset.json"), "w") as fh:
+        json.dump({"source": "reference data/basis/{" + ",".join(BSE_SETS) + "} (Basis Set Exchange "
+                             "JSON, via FreeBreakfast data/basis), elements " + " ".join(BSE_ELEMENTS),
+                   "sets": out}, fh, indent=0)
+    print("bse", len(out))
 
 
 # --- density fitting: libcint (P|Q) rows and (mn|P) columns -------------------
@@ -573,7 +618,7 @@ PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "jk_small": part_jk_small,
          "cost": part_cost, "jplan_c0": part_jplan_c0, "scatter_c0": part_scatter_c0,
-         "onee": part_onee, "scf": part_scf}
+         "onee": part_onee, "scf": part_scf, "bse": part_bse}
 DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
 
 

@@ -70,3 +70,25 @@ def test_one_electron_subsets_and_no_nuclei(cuda, lib_built):
     S, T, V, H = eng.one_electron([])
     assert int((V != 0).sum()) == 0 and bool((H == T).all())
     assert _rel(overlap_matrix(B), g["S"]) <= 1e-12
+
+
+def test_bse_document_to_libcint_jk(cuda, lib_built):
+    """A molecule read from its Basis Set Exchange document (basis_io) runs
+    through the C ABI to libcint's J and K: H2O in cc-pVDZ (reduced form)."""
+    import json
+    import os
+
+    from conftest import GOLDEN
+    from felizjueves_b200 import basis_io
+    from felizjueves_b200.fock import FockEngine
+    with open(os.path.join(GOLDEN, "bse_subset.json")) as fh:
+        dz = basis_io.parse(json.load(fh)["sets"]["cc-pVDZ.json"])
+    g1 = golden("onee_h2o_ccpvdz_j.npz")
+    g2 = golden("libcint_h2o_ccpvdz.npz")
+    B = basis_io.from_bse(dz, nuclei_of(g1), reduce=True)
+    eng = FockEngine(B)
+    eng.plan(g2["D"], 0.0, 4)
+    J, K, G = eng.build_host(g2["D"])
+    assert _rel(J, g2["vj"]) <= 1e-12 and _rel(K, g2["vk"]) <= 1e-12
+    S, T, V, H = [M.cpu().numpy() for M in eng.one_electron(nuclei_of(g1))]
+    assert _rel(H, g1["H"]) <= 1e-12
