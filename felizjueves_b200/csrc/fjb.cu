@@ -787,6 +787,7 @@ struct fjb_handle {
     HostBasis basis;
     fjb::JEngine *jeng = nullptr;  // the J-engine, built on first use
     fjb::OneElectron *onee = nullptr;  // the one-electron shell pairs, built on first use
+    std::vector<fjb::PairBounds> pair_bounds;  // the plan's D-independent pair bounds, computed once
     int j_launches = 0;            // kernel launches of the last J-engine build
     std::string err;
     std::map<std::tuple<int, int, int, int>, std::unique_ptr<ClassEntry>> classes;
@@ -1173,7 +1174,7 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     h->drop_graph();
     try {
         unsigned nt = std::max(1u, std::thread::hardware_concurrency());
-        h->plan = f_launches(h->basis, D_host, tau, n_mag, (int)nt);
+        h->plan = f_launches(h->basis, D_host, tau, n_mag, (int)nt, &h->pair_bounds);
     } catch (const std::invalid_argument &e) {
         return fail(h, FJB_E_ARG, e.what());
     } catch (const std::exception &e) {

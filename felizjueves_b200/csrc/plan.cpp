@@ -208,7 +208,8 @@ int magnitude_index(double G, const std::vector<double> &mags) {
 
 }  // namespace
 
-Plan f_launches(const HostBasis &basis, const double *D, double tau, int n, int threads) {
+Plan f_launches(const HostBasis &basis, const double *D, double tau, int n, int threads,
+                std::vector<PairBounds> *bounds) {
     if (!(std::isfinite(tau) && tau >= 0.0)) throw std::invalid_argument("tau is not a finite float >= 0");
     if (n < 1) throw std::invalid_argument("n is not an int >= 1 (the number of eq. 29 magnitudes)");
     const int nsh = (int)basis.shells.size(), nao = basis.n_ao;
@@ -224,38 +225,38 @@ Plan f_launches(const HostBasis &basis, const double *D, double tau, int n, int 
     plan.n = n;
     for (int i = 0; i < n; ++i) plan.mags.push_back(std::pow(tau, (double)i / (double)n));
 
-    struct Raw {
-        int a, b;
-        std::vector<double> g;
-        double G;
-    };
-    std::vector<std::pair<int, int>> canon;
-    for (int i = 0; i < nsh; ++i)
-        for (int j = i; j < nsh; ++j) {
-            bool keep = std::make_pair(basis.shells[i].l, i) <= std::make_pair(basis.shells[j].l, j);
-            canon.emplace_back(keep ? i : j, keep ? j : i);
-        }
-    std::vector<Raw> raw(canon.size());
-    int nt = std::max(1, threads);
-    std::vector<std::thread> pool;
-    std::vector<std::string> errs(nt);
-    for (int t = 0; t < nt; ++t)
-        pool.emplace_back([&, t]() {
-            try {
-                for (size_t k = t; k < canon.size(); k += nt) {
-                    auto [a, b] = canon[k];
-                    raw[k].a = a;
-                    raw[k].b = b;
-                    raw[k].g = primitive_schwarz_bounds(basis.shells[a], basis.shells[b]);
-                    raw[k].G = fsum(raw[k].g.data(), raw[k].g.size());
-                }
-            } catch (const std::exception &e) {
-                errs[t] = e.what();
+    std::vector<PairBounds> local;
+    std::vector<PairBounds> &raw = bounds ? *bounds : local;
+    if (raw.empty()) {
+        std::vector<std::pair<int, int>> canon;
+        for (int i = 0; i < nsh; ++i)
+            for (int j = i; j < nsh; ++j) {
+                bool keep = std::make_pair(basis.shells[i].l, i) <= std::make_pair(basis.shells[j].l, j);
+                canon.emplace_back(keep ? i : j, keep ? j : i);
             }
-        });
-    for (auto &th : pool) th.join();
-    for (auto &e : errs)
-        if (!e.empty()) throw std::runtime_error(e);
+        std::vector<PairBounds> fresh(canon.size());
+        int nt = std::max(1, threads);
+        std::vector<std::thread> pool;
+        std::vector<std::string> errs(nt);
+        for (int t = 0; t < nt; ++t)
+            pool.emplace_back([&, t]() {
+                try {
+                    for (size_t k = t; k < canon.size(); k += nt) {
+                        auto [a, b] = canon[k];
+                        fresh[k].a = a;
+                        fresh[k].b = b;
+                        fresh[k].g = primitive_schwarz_bounds(basis.shells[a], basis.shells[b]);
+                        fresh[k].G = fsum(fresh[k].g.data(), fresh[k].g.size());
+                    }
+                } catch (const std::exception &e) {
+                    errs[t] = e.what();
+                }
+            });
+        for (auto &th : pool) th.join();
+        for (auto &e : errs)
+            if (!e.empty()) throw std::runtime_error(e);
+        raw = std::move(fresh);
+    }
 
     double g_max = 0.0;
     for (auto &r : raw) g_max = std::max(g_max, r.G);

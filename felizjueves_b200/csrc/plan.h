@@ -66,8 +66,20 @@ void hermite_bounds(double zeta, int L, const std::vector<Cart3> &hs, double *I)
 // primitive_pairs order (i outer).
 std::vector<double> primitive_schwarz_bounds(const HostShell &sa, const HostShell &sb);
 
+// The bounds of one canonical shell pair: G_[ab] per primitive pair and
+// their fsum G.  They depend on the basis alone, not on D or tau.
+struct PairBounds {
+    int a = 0, b = 0;
+    std::vector<double> g;
+    double G = 0.0;
+};
+
 // The pair stream (launch_f.py:390-466).  Throws std::invalid_argument /
-// std::runtime_error with the reference's refusals.
-Plan f_launches(const HostBasis &basis, const double *D, double tau, int n, int threads);
+// std::runtime_error with the reference's refusals.  With `bounds` non-null
+// the canonical pairs' bounds are taken from it when it is filled, and
+// computed into it when it is empty, so plans of one basis for successive
+// densities (an SCF loop) compute them once.
+Plan f_launches(const HostBasis &basis, const double *D, double tau, int n, int threads,
+                std::vector<PairBounds> *bounds = nullptr);
 
 }  // namespace fjb

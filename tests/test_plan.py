@@ -131,3 +131,18 @@ def test_one_electron_refusals(lib_built):
         e.one_electron([(1.0, (0.0, 0.0))])
     with pytest.raises(ValueError, match="non-finite"):
         e.one_electron([(float("nan"), (0.0, 0.0, 0.0))])
+
+
+def test_replan_reuses_bounds_with_identical_lists(lib_built):
+    """A handle computes the D-independent pair bounds once and reuses them
+    for later densities: each plan equals a fresh handle's plan."""
+    w = configs.c0()
+    e = FockEngine(w.basis, device=-1)
+    for it in range(3):
+        D = configs.perturbed_density(w.D, it)
+        P = e.plan(D, w.tau, w.n_mag)
+        Q = FockEngine(w.basis, device=-1).plan(D, w.tau, w.n_mag)
+        assert P.launches == Q.launches and P.screened == Q.screened and P.deleted == Q.deleted
+        assert [(b.la, b.lb, b.degree, b.mag) for b in P.batches] == [(b.la, b.lb, b.degree, b.mag) for b in Q.batches]
+        assert [[(p.a, p.b, p.prims, p.G, p.key) for p in b.pairs] for b in P.batches] == \
+               [[(p.a, p.b, p.prims, p.G, p.key) for p in b.pairs] for b in Q.batches]
