@@ -10,7 +10,7 @@ files this script writes.
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
 parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost jplan_c0 scatter_c0 onee
-scf bse (default: all
+scf bse harmonics (default: all
 but plan_c1 and jk_small, which take minutes).
 """
 
@@ -196,6 +196,19 @@ def part_scf():
                                               f"PySCF {d['provenance']['pyscf']}, libcint "
                                               f"{d['provenance']['libcint']})"))
         print("scf", name, n)
+
+
+# --- real solid harmonics over Cartesians: the reference's convention ---------
+
+def part_harmonics():
+    """The reference's aux_harmonics(l), l = 0..6 (eri/density_fit/
+    kernel_eri3.py: columns m = -l..l over cartesians(l))."""
+    from felizjueves.eri.density_fit.kernel_eri3 import aux_harmonics
+    out = {f"l{l}": np.asarray(aux_harmonics(l)) for l in range(7)}
+    np.savez_compressed(os.path.join(HERE, "harmonics.npz"), **out,
+                        source=np.asarray("reference eri/density_fit/kernel_eri3.py aux_harmonics(l), "
+                                          "l = 0..6, rows m = -l..l"))
+    print("harmonics", len(out))
 
 
 # --- Basis Set Exchange documents: the elements the fixtures use -------------
@@ -618,7 +631,8 @@ PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "jk_small": part_jk_small,
          "cost": part_cost, "jplan_c0": part_jplan_c0, "scatter_c0": part_scatter_c0,
-         "onee": part_onee, "scf": part_scf, "bse": part_bse}
+         "onee": part_onee, "scf": part_scf, "bse": part_bse,
+         "harmonics": part_harmonics}
 DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
 
 

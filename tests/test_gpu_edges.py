@@ -110,3 +110,24 @@ def test_plan_without_launches(cuda, lib_built):
     assert all(int(torch.count_nonzero(X)) == 0 for X in out)
     Jh, Kh, Gh = eng.build_host(w.D)
     assert not Jh.any() and not Kh.any() and not Gh.any()
+
+
+def test_spherical_build_matches_oracle(cuda, lib_built, oracle_lib):
+    """A spherical density through SphericalFock: J, K, G in real solid
+    harmonics against T^T (oracle's Cartesian J, K) T."""
+    import torch
+    from felizjueves_b200 import configs
+    from felizjueves_b200.spherical import SphericalFock, transform
+    w = configs.cluster(3, 5)
+    T = transform(w.basis)
+    ns = T.shape[1]
+    Ds = _sym(ns, 9)
+    sf = SphericalFock(w.basis)
+    sf.plan(Ds, 0.0, 4)
+    J, K, G = (M.cpu().numpy() for M in sf.build(torch.tensor(Ds, device=cuda)))
+    Dc = T @ Ds @ T.T
+    Dc = 0.5 * (Dc + Dc.T)
+    Jo, Ko = oracle_lib.jk(oracle_lib.OracleBasis.of(w.basis), Dc)
+    assert np.abs(J - T.T @ Jo @ T).max() <= FP64_ABS
+    assert np.abs(K - T.T @ Ko @ T).max() <= FP64_ABS
+    assert np.abs(G - T.T @ (Jo - 0.5 * Ko) @ T).max() <= FP64_ABS
