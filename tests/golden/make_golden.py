@@ -10,7 +10,7 @@ files this script writes.
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
 parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost jplan_c0 scatter_c0 onee
-scf bse harmonics (default: all
+scf bse harmonics grad (default: all
 but plan_c1 and jk_small, which take minutes).
 """
 
@@ -196,6 +196,27 @@ def part_scf():
                                               f"PySCF {d['provenance']['pyscf']}, libcint "
                                               f"{d['provenance']['libcint']})"))
         print("scf", name, n)
+
+
+# --- nuclear-gradient J/K terms: libcint int2e_ip1 contracted by PySCF --------
+
+def part_grad():
+    fx = os.path.join(REF, "test", "oracle", "fixtures")
+    for name in SCF:
+        d = json.load(open(os.path.join(fx, name + ".json")))
+        n = d["nao"]
+        arr = d["arrays"]
+        g = {k.replace(":", "_"): np.asarray(arr[k]["values"]).reshape(arr[k]["shape"])
+             for k in ("vj1", "vk1", "grad:j", "grad:k", "density")}
+        ao_atom = [int(lbl.split()[0]) for lbl in d["ao_labels"]]
+        np.savez_compressed(os.path.join(HERE, f"grad_{name.replace('_grad', '')}.npz"), **g,
+                            ao_atom=np.asarray(ao_atom, np.int32),
+                            source=np.asarray(f"test/oracle/fixtures/{name}.json vj1, vk1 (PySCF "
+                                              f"grad.rhf.get_jk over int2e_ip1), grad:j, grad:k, "
+                                              f"density; PySCF {d['provenance']['pyscf']}, libcint "
+                                              f"{d['provenance']['libcint']}"))
+        assert g["vj1"].shape == (3, n, n)
+        print("grad", name, n)
 
 
 # --- real solid harmonics over Cartesians: the reference's convention ---------
@@ -632,7 +653,7 @@ PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_
          "screen_c0": part_screen_c0, "jk_small": part_jk_small,
          "cost": part_cost, "jplan_c0": part_jplan_c0, "scatter_c0": part_scatter_c0,
          "onee": part_onee, "scf": part_scf, "bse": part_bse,
-         "harmonics": part_harmonics}
+         "harmonics": part_harmonics, "grad": part_grad}
 DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
 
 
