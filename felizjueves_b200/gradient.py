@@ -77,28 +77,100 @@ def jk_derivatives(basis: Basis, D, *, tau: float = 0.0, device: int = 0, jk=Non
     Dx = np.zeros((m, m))
     Dx[:n, :n] = D
     J, K = (jk or _gpu_jk(tau, device))(B, Dx)
-    vj1 = np.zeros((3, n, n))
-    vk1 = np.zeros((3, n, n))
+    vj1 = -_shift_rows(basis, B, up, dn, J)
+    vk1 = -_shift_rows(basis, B, up, dn, K)
+    return vj1, vk1
+
+
+def _shift_rows(basis: Basis, B: Basis, up, dn, M: np.ndarray) -> np.ndarray:
+    """out[x, i, :] = M[i+1_x, :n] + i_x M[i-1_x, :n] over the original AOs
+    i: the electron-coordinate derivative of the bra function, as rows of a
+    matrix over the extended basis."""
+    n = basis.n_ao
+    out = np.zeros((3, n, n))
     for s, shell in enumerate(basis.shells):
-        comps = cartesians(shell.l)
         iu = {c: B.offsets[up[s]] + k for k, c in enumerate(cartesians(shell.l + 1))}
         idn = ({c: B.offsets[dn[s]] + k for k, c in enumerate(cartesians(shell.l - 1))}
                if dn[s] is not None else {})
-        for r, comp in enumerate(comps):
+        for r, comp in enumerate(cartesians(shell.l)):
             i = basis.offsets[s] + r
             for x in range(3):
                 cp = list(comp)
                 cp[x] += 1
-                vj = J[iu[tuple(cp)], :n].copy()
-                vk = K[iu[tuple(cp)], :n].copy()
+                v = M[iu[tuple(cp)], :n].copy()
                 if comp[x] > 0:
                     cm = list(comp)
                     cm[x] -= 1
-                    vj += comp[x] * J[idn[tuple(cm)], :n]
-                    vk += comp[x] * K[idn[tuple(cm)], :n]
-                vj1[x, i] = -vj
-                vk1[x, i] = -vk
-    return vj1, vk1
+                    v += comp[x] * M[idn[tuple(cm)], :n]
+                out[x, i] = v
+    return out
+
+
+def _gpu_onee(device: int):
+    def onee(B, nuclei):
+        eng = FockEngine(B, device)
+        S, T, V, _ = eng.one_electron(nuclei, want=("S", "T", "V"))
+        return S.cpu().numpy(), T.cpu().numpy(), V.cpu().numpy()
+    return onee
+
+
+def one_electron_derivatives(basis: Basis, nuclei, *, device: int = 0, onee=None):
+    """libcint's int1e_ipovlp, int1e_ipkin, int1e_ipnuc (3 x n x n) and
+    int1e_iprinv at each nucleus (n_atoms x 3 x n x n): <d_x i|O|j> with d_x
+    on the electron coordinate of i, from the one-electron matrices of the
+    shift-extended basis (rinv at nucleus C: V of one charge -1 there)."""
+    nuc = _checked_nuclei(nuclei)
+    B, up, dn = extended_basis(basis)
+    ev = onee or _gpu_onee(device)
+    S, T, V = ev(B, nuc)
+    ipovlp = _shift_rows(basis, B, up, dn, S)
+    ipkin = _shift_rows(basis, B, up, dn, T)
+    ipnuc = _shift_rows(basis, B, up, dn, V)
+    iprinv = np.stack([_shift_rows(basis, B, up, dn, ev(B, [(-1.0, c)])[2]) for _, c in nuc])
+    return ipovlp, ipkin, ipnuc, iprinv
+
+
+def nuclear_repulsion_gradient(nuclei) -> np.ndarray:
+    """d V_nn / d R_A = -sum_B Z_A Z_B (R_A - R_B) / |R_A - R_B|^3."""
+    nuc = _checked_nuclei(nuclei)
+    g = np.zeros((len(nuc), 3))
+    for a, (za, ca) in enumerate(nuc):
+        for b, (zb, cb) in enumerate(nuc):
+            if a != b:
+                d = np.subtract(ca, cb)
+                g[a] -= za * zb * d / np.linalg.norm(d) ** 3
+    return g
+
+
+def rhf_gradient(basis: Basis, nuclei, D, W, *, tau: float = 0.0, device: int = 0, jk=None,
+                 onee=None) -> dict:
+    """The closed-shell SCF nuclear gradient of density D and energy-
+    weighted density W = 2 sum_occ e_i C_i C_i^T, per term (PySCF's
+    grad.rhf.grad_elec + grad_nuc, which the reference's fixtures record):
+
+        h[A]   = sum_ij dh^A_ij D_ij,  dh^A = v + v^T,
+                 v = -Z_A rinv'_A, rows of A's AOs plus -(ipkin + ipnuc)
+        s[A]   = 2 sum_(i on A) sum_j ipovlp[:, i, j] W_ij
+        j[A], k[A]  as gradient_jk
+        nuc[A] the nuclear repulsion's
+    and their sum `total` (n_atoms x 3 each)."""
+    nuc = _checked_nuclei(nuclei)
+    D = _checked_density(basis, D)
+    W = np.asarray(W, np.float64)
+    atoms = ao_atoms(basis, nuc)
+    ipovlp, ipkin, ipnuc, iprinv = one_electron_derivatives(basis, nuc, device=device, onee=onee)
+    h1 = -(ipkin + ipnuc)
+    gh = np.zeros((len(nuc), 3))
+    gs = np.zeros((len(nuc), 3))
+    for a, (za, _) in enumerate(nuc):
+        v = -za * iprinv[a]
+        rows = atoms == a
+        v[:, rows] += h1[:, rows]
+        gh[a] = np.einsum("xij,ij->x", v + v.transpose(0, 2, 1), D)
+        gs[a] = 2.0 * np.einsum("xij,ij->x", ipovlp[:, rows], W[rows])
+    gj, gk = gradient_jk(basis, D, nuc, tau=tau, device=device, jk=jk)
+    gn = nuclear_repulsion_gradient(nuc)
+    return {"h": gh, "s": gs, "j": gj, "k": gk, "nuc": gn, "total": gh + gs + gj + gk + gn}
 
 
 def ao_atoms(basis: Basis, nuclei) -> np.ndarray:

@@ -207,13 +207,15 @@ def part_grad():
         n = d["nao"]
         arr = d["arrays"]
         g = {k.replace(":", "_"): np.asarray(arr[k]["values"]).reshape(arr[k]["shape"])
-             for k in ("vj1", "vk1", "grad:j", "grad:k", "density")}
+             for k in ("vj1", "vk1", "grad:j", "grad:k", "density", "dme", "int1e_ipovlp", "int1e_ipkin",
+                       "int1e_ipnuc", "int1e_iprinv", "grad:h", "grad:s", "grad:nuc", "grad:total")}
         ao_atom = [int(lbl.split()[0]) for lbl in d["ao_labels"]]
         np.savez_compressed(os.path.join(HERE, f"grad_{name.replace('_grad', '')}.npz"), **g,
                             ao_atom=np.asarray(ao_atom, np.int32),
                             source=np.asarray(f"test/oracle/fixtures/{name}.json vj1, vk1 (PySCF "
-                                              f"grad.rhf.get_jk over int2e_ip1), grad:j, grad:k, "
-                                              f"density; PySCF {d['provenance']['pyscf']}, libcint "
+                                              f"grad.rhf.get_jk over int2e_ip1), int1e_ip*, the RHF "
+                                              f"gradient's terms, density, dme; PySCF "
+                                              f"{d['provenance']['pyscf']}, libcint "
                                               f"{d['provenance']['libcint']}"))
         assert g["vj1"].shape == (3, n, n)
         print("grad", name, n)

@@ -56,3 +56,31 @@ def test_extended_basis_refuses_f():
     from felizjueves_b200.shell import Basis, Shell
     with pytest.raises(ValueError, match="l = 2"):
         gradient.extended_basis(Basis((Shell(3, (0.0, 0.0, 0.0), [1.0], [1.0]),)))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_rhf_gradient_assembly_with_oracle(oracle_lib, name):
+    """The product's whole RHF gradient (felizjueves_b200/gradient.py
+    rhf_gradient) with the oracle's one-electron matrices and J/K injected:
+    libcint's int1e_ipovlp / ipkin / ipnuc / iprinv (1e-13 of the largest
+    element) and PySCF's per-atom h, S, J, K, nuclear terms and total
+    (1e-11)."""
+    from felizjueves_b200 import gradient
+    from oracle import one_electron, oracle
+    s = golden(f"scf_{name}.npz")
+    g = golden(f"grad_{name}.npz")
+    B = basis_of(s)
+    nuclei = [(float(z), tuple(c)) for z, c in zip(s["charges"], s["coords"])]
+
+    def onee(Bx, nuc):
+        return one_electron.matrices(Bx, nuc)
+
+    def jk(Bx, Dx):
+        return oracle.jk(oracle.OracleBasis.of(Bx), Dx)
+
+    ip = gradient.one_electron_derivatives(B, nuclei, onee=onee)
+    for got, key in zip(ip, ("int1e_ipovlp", "int1e_ipkin", "int1e_ipnuc", "int1e_iprinv")):
+        assert np.abs(got - g[key]).max() <= 1e-13 * np.abs(g[key]).max(), key
+    r = gradient.rhf_gradient(B, nuclei, g["density"], g["dme"], jk=jk, onee=onee)
+    for term in ("h", "s", "j", "k", "nuc", "total"):
+        assert np.abs(r[term] - g[f"grad_{term}"]).max() <= 1e-11, term
