@@ -28,7 +28,7 @@ class BatchBuilder:
         self.engines, self.D, self.out = [], [], []
         for w in self.workloads:
             eng = FockEngine(w.basis, device=self.device)
-            eng.plan(w.D, w.tau, w.n_mag)
+            eng.plan(w.D, w.tau, w.n_mag, export=False)
             self.engines.append(eng)
             D = torch.tensor(w.D, device=dev)
             self.D.append(D)

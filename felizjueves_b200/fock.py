@@ -163,7 +163,8 @@ class FockEngine:
         h = C.c_void_p()
         _lib.check(self._L.fjb_create(C.byref(h), C.byref(bt), self.device))
         self._h = h
-        self._plan = None
+        self._planned = False
+        self._plan_lists = None
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -181,20 +182,34 @@ class FockEngine:
         return self.basis.n_ao
 
     # -- the plan ----------------------------------------------------------
-    def plan(self, D, tau: float = 1e-12, n: int = 4) -> FPlan:
+    def plan(self, D, tau: float = 1e-12, n: int = 4, *, export: bool = True) -> FPlan | None:
+        """Plan the builds of density D: the pair stream on the host, staged
+        on the device.  Returns the lists as an FPlan, or None with
+        `export=False` (an SCF loop that only builds: the lists are then
+        exported on first use)."""
         A = _checked_density(self.basis, D)
         tau = _checked_tau(tau)
         if type(n) is not int or n < 1:
             raise ValueError(f"n = {n!r} is not an int >= 1 (the number of eq. 29 magnitudes)")
+        self._planned = False
+        self._plan_lists = None
         _lib.check(self._L.fjb_plan(self._h, A.ctypes.data, tau, n), self._h)
-        self._tau = tau
-        self._plan = self._export(n)
+        self._tau, self._n_mag, self._planned = tau, n, True
         if self.tuned and self.device >= 0:
             from . import autotune
             table = autotune.load_default()
             if table:
                 autotune.apply(self, table)
-        return self._plan
+        return self._plan if export else None
+
+    @property
+    def _plan(self) -> FPlan | None:
+        """The current plan's lists (exported from the handle once)."""
+        if not self._planned:
+            return None
+        if self._plan_lists is None:
+            self._plan_lists = self._export(self._n_mag)
+        return self._plan_lists
 
     def counts_raw(self) -> dict[str, int]:
         c = _lib.PlanCounts_t()
@@ -245,7 +260,7 @@ class FockEngine:
 
     # -- builds --------------------------------------------------------------
     def _require_plan(self):
-        if self._plan is None:
+        if not self._planned:
             raise RuntimeError("no plan: call plan(D, tau, n) first")
 
     def build(self, D, *, J=None, K=None, G=None, precision: int = _lib.FJB_FP64,
@@ -482,7 +497,7 @@ def core_hamiltonian(basis: Basis, nuclei, *, device: int = 0) -> np.ndarray:
 def coulomb_exchange(basis: Basis, D, *, tau: float = 0.0, n: int = 4, device: int = 0):
     """(J, K) of the total density D (numpy arrays), on the GPU."""
     eng = FockEngine(basis, device)
-    eng.plan(D, tau, n)
+    eng.plan(D, tau, n, export=False)
     J, K, _ = eng.build_host(D)
     return J, K
 
@@ -490,7 +505,7 @@ def coulomb_exchange(basis: Basis, D, *, tau: float = 0.0, n: int = 4, device: i
 def fock_two_electron(basis: Basis, D, *, tau: float = 0.0, n: int = 4, device: int = 0):
     """G = J - K/2 of the total closed-shell density D, on the GPU."""
     eng = FockEngine(basis, device)
-    eng.plan(D, tau, n)
+    eng.plan(D, tau, n, export=False)
     return eng.build_host(D)[2]
 
 

@@ -63,7 +63,7 @@ def extended_basis(basis: Basis):
 def _gpu_jk(tau: float, device: int):
     def jk(B, D):
         eng = FockEngine(B, device)
-        eng.plan(D, tau, 4)
+        eng.plan(D, tau, 4, export=False)
         J, K, _ = eng.build_host(D)
         return J, K
     return jk

@@ -80,7 +80,7 @@ class GpuBuilders:
         return S, H
 
     def g(self, D):
-        self.eng.plan(D.cpu().numpy(), self.tau, self.n_mag)
+        self.eng.plan(D.cpu().numpy(), self.tau, self.n_mag, export=False)
         G = self.eng.build(D, precision=self.precision, threshold=self.threshold)[2]
         self.computed.append(sum(st["computed"] for st in self.eng.launch_stats()))
         return G
