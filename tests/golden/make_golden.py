@@ -10,7 +10,7 @@ files this script writes.
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
 parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost jplan_c0 scatter_c0 onee
-scf bse harmonics grad (default: all
+scf bse harmonics grad rys (default: all
 but plan_c1 and jk_small, which take minutes).
 """
 
@@ -219,6 +219,25 @@ def part_grad():
                                               f"{d['provenance']['libcint']}"))
         assert g["vj1"].shape == (3, n, n)
         print("grad", name, n)
+
+
+# --- the Rys rule: the reference's fp64 nodes and weights ---------------------
+
+def part_rys():
+    """rys/roots.py roots_weights(n, T), n = 1..5, on a T grid across its
+    switch (T = 80) and out to 1e4."""
+    from felizjueves.rys.roots import roots_weights
+    Ts = np.concatenate([[0.0, 1e-12, 1e-6], np.geomspace(1e-3, 1e4, 57), [79.9, 80.0, 80.1]])
+    x = np.zeros((5, len(Ts), 5))
+    w = np.zeros((5, len(Ts), 5))
+    for n in range(1, 6):
+        for k, T in enumerate(Ts):
+            xs, ws = roots_weights(n, float(T))
+            x[n - 1, k, :n] = xs
+            w[n - 1, k, :n] = ws
+    np.savez_compressed(os.path.join(HERE, "rys_roots.npz"), T=Ts, x=x, w=w,
+                        source=np.asarray("reference rys/roots.py roots_weights(n, T), n = 1..5"))
+    print("rys", len(Ts))
 
 
 # --- real solid harmonics over Cartesians: the reference's convention ---------
@@ -655,7 +674,7 @@ PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_
          "screen_c0": part_screen_c0, "jk_small": part_jk_small,
          "cost": part_cost, "jplan_c0": part_jplan_c0, "scatter_c0": part_scatter_c0,
          "onee": part_onee, "scf": part_scf, "bse": part_bse,
-         "harmonics": part_harmonics, "grad": part_grad}
+         "harmonics": part_harmonics, "grad": part_grad, "rys": part_rys}
 DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
 
 
