@@ -325,8 +325,13 @@ int onee_build(OneElectron *e, const double *charges, const double *coords, int 
     std::vector<double4> nuc(n_nuc);
     for (int q = 0; q < n_nuc; ++q)
         nuc[q] = make_double4(coords[3 * q], coords[3 * q + 1], coords[3 * q + 2], charges[q]);
+    // ordered on the build's stream: a later call with other nuclei cannot
+    // overwrite them under this call's kernels (pageable source: the call
+    // returns once the bytes are staged)
     cudaError_t ce = cudaSuccess;
-    if (n_nuc > 0) ce = e->nuc.upload(nuc);
+    if (n_nuc > 0) ce = e->nuc.alloc(nuc.size());
+    if (ce == cudaSuccess && n_nuc > 0)
+        ce = cudaMemcpyAsync(e->nuc.p, nuc.data(), nuc.size() * sizeof(double4), cudaMemcpyHostToDevice, st);
     if (ce != cudaSuccess) {
         *err = std::string("one-electron nuclei: ") + cudaGetErrorString(ce);
         return 1;
