@@ -133,7 +133,9 @@ void fjb_destroy(fjb_handle *h);
 /* Build the pair stream for density D (HOST pointer, n_ao^2) at threshold
  * tau with n_mag eq.29 magnitudes, and stage it on the device.  The plan's
  * sort inside a batch reads D; the builds that follow take any symmetric D
- * (the in-kernel six-block screen reads the density each build is given). */
+ * (the in-kernel six-block screen reads the density each build is given).
+ * The basis's primitive-pair bounds do not depend on D: the first plan of a
+ * handle computes them and later plans reuse them. */
 int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag);
 int fjb_plan_counts(const fjb_handle *h, fjb_plan_counts_t *out);
 int fjb_plan_export(const fjb_handle *h, fjb_plan_lists *out);
