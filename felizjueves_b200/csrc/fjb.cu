@@ -643,7 +643,6 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
 
 namespace {
 
-constexpr int kSmemBudgetDoubles = 27648;  // 216 KiB of the 227 KiB a CTA may hold
 
 template <typename T>
 struct DevBuf {

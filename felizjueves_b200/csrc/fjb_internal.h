@@ -16,6 +16,7 @@ constexpr int kBoysRow = kBoysMaxM + 2;  // F_0 .. F_kBoysMaxM, then exp(-T_i)
 constexpr int kThreads = 128;       // widest CTA of the HGP kernel's default choice
 constexpr int kMaxThreads = 512;    // widest CTA the kernel is instantiated for
 constexpr int kKetChunk = 32;       // ket pairs per work unit (one per lane of a warp)
+constexpr int kSmemBudgetDoubles = 27648;  // the HGP kernel's shared memory: 216 KiB of the 227 KiB a CTA may hold
 constexpr int kNumScalars = 17;     // per-primitive-quartet VRR scalars
 
 // One VRR node update, 16 bytes.  value(dst) =
