@@ -1198,8 +1198,9 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     }
     // launches and work units, grouped by class
     std::vector<LaunchRec> lr;
-    std::map<std::tuple<int, int, int, int>, std::vector<Unit>> by_class;
+    std::map<std::tuple<int, int, int, int>, std::vector<int>> class_launches;  // launch indices, plan order
     std::map<std::tuple<int, int, int, int>, std::pair<int, int>> class_deg;
+    size_t n_units_total = 0;
     int64_t qbase = 0;
     for (auto &L : P.launches) {
         const PlanBatch &br = P.batches[L.first], &kt = P.batches[L.second];
@@ -1219,28 +1220,46 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
         auto &cd = class_deg[key];
         cd.first = std::max(cd.first, br.degree);
         cd.second = std::max(cd.second, kt.degree);
-        auto &us = by_class[key];
+        class_launches[key].push_back(li);
         for (int ib = 0; ib < r.n_bra; ++ib) {
             const int k_begin = r.diag ? ib : 0;
-            for (int k0 = k_begin; k0 < r.n_ket; k0 += kKetChunk)
-                us.push_back(Unit{li, ib, k0, std::min(r.n_ket, k0 + kKetChunk)});
+            if (r.n_ket > k_begin) n_units_total += (size_t)((r.n_ket - k_begin + kKetChunk - 1) / kKetChunk);
         }
     }
+    // the work units, class by class (the map's order), each class's
+    // launches in plan order: written once into one array
     std::vector<Unit> units;
+    std::map<std::tuple<int, int, int, int>, std::pair<int, int>> class_units;  // (first unit, count)
+    try {
+        units.reserve(n_units_total);
+        for (auto &kv : class_launches) {
+            const int u0 = (int)units.size();
+            for (int li : kv.second) {
+                const LaunchRec &r = lr[li];
+                for (int ib = 0; ib < r.n_bra; ++ib) {
+                    const int k_begin = r.diag ? ib : 0;
+                    for (int k0 = k_begin; k0 < r.n_ket; k0 += kKetChunk)
+                        units.push_back(Unit{li, ib, k0, std::min(r.n_ket, k0 + kKetChunk)});
+                }
+            }
+            class_units[kv.first] = {u0, (int)units.size() - u0};
+        }
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_LIMIT, std::string("work units: ") + e.what());
+    }
     h->runs.clear();
     h->scatter_ready = false;
     h->lr_host = lr;
     h->pr_host = pr;
     if (h->device < 0) {  // host-only: the lists are complete, nothing is staged
-        for (auto &kv : by_class) units.insert(units.end(), kv.second.begin(), kv.second.end());
-        h->units_host = units;
+        h->units_host = std::move(units);
         h->quartets_launched = qbase;
-        h->n_units = (int)units.size();
+        h->n_units = (int)h->units_host.size();
         h->planned = true;
         return FJB_OK;
     }
     try {
-        for (auto &kv : by_class) {
+        for (auto &kv : class_units) {
             auto [la, lb, lc, ld] = kv.first;
             ClassEntry &ce = h->cls(la, lb, lc, ld);
             ClassRun run;
@@ -1259,16 +1278,15 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
                 run.dev32 = ce.dev(deg.first, deg.second, ov32->second.first, ov32->second.second, 4);
             run.compiled = compiled_available(la, lb, lc, ld, false) && (th == 0 || th == 1);
             run.has32 = compiled_available(la, lb, lc, ld, true);
-            run.unit0 = (int)units.size();
-            run.n_units = (int)kv.second.size();
-            units.insert(units.end(), kv.second.begin(), kv.second.end());
+            run.unit0 = kv.second.first;
+            run.n_units = kv.second.second;
             h->runs.push_back(run);
         }
         h->pairs.upload(pr);
         h->prims.upload(pm);
         h->launches.upload(lr);
         h->units.upload(units);
-        h->units_host = units;
+        h->units_host = std::move(units);
         const size_t nn = (size_t)h->basis.n_ao * h->basis.n_ao;
         const size_t ns = h->basis.shells.size();
         h->Dsh.alloc(ns * ns);
@@ -1301,14 +1319,14 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
             lc.push_back(s.ld);
         }
         h->launch_cls.upload(lc);
-        h->route_list.alloc(std::max<size_t>(1, 2 * units.size()));
+        h->route_list.alloc(std::max<size_t>(1, 2 * h->units_host.size()));
         h->route_counts.alloc(std::max<size_t>(1, 2 * h->runs.size()));
     } catch (const std::exception &e) {
         return fail(h, FJB_E_CUDA, e.what());
     }
     h->built = false;
     h->quartets_launched = qbase;
-    h->n_units = (int)units.size();
+    h->n_units = (int)h->units_host.size();
     h->planned = true;
     return FJB_OK;
 }
