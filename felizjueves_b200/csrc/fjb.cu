@@ -1230,6 +1230,8 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     // launches in plan order: written once into one array
     std::vector<Unit> units;
     std::map<std::tuple<int, int, int, int>, std::pair<int, int>> class_units;  // (first unit, count)
+    if (n_units_total > (size_t)INT32_MAX)
+        return fail(h, FJB_E_LIMIT, "more than 2^31 work units: the unit indices are 32-bit");
     try {
         units.reserve(n_units_total);
         for (auto &kv : class_launches) {
