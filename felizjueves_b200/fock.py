@@ -9,7 +9,9 @@ Mirrors (paths within the reference project):
   C++; it is not injectable here.
 * `fock_two_electron(basis, D, *, tau, n)`  eri/fock/fock.py:166
   fock_two_electron_reference -> G = J - K/2, and
-  `coulomb_exchange(basis, D, ...)`  eri/fock/fock.py:126 -> (J, K).
+  `coulomb_exchange(basis, D, ...)`  eri/fock/fock.py:126 -> (J, K);
+  `coulomb_matrix` (the J-engine, eri/j_coulomb/j.py:436) and
+  `exchange_matrix` (eri/k_exchange/k.py:482) -> J or K alone.
 * `eri_block(basis, a, b, c, d)`  eri/eri.py:145 -> the (ab|cd) block.
 * `FockEngine`  the reusable form: plan once per (basis, tau, n), then build
   for any symmetric D, on device tensors (torch) or host arrays (numpy).
@@ -519,6 +521,16 @@ def coulomb_matrix(basis: Basis, D, *, tau: float = 0.0, device: int = 0) -> np.
     J = eng.coulomb(Dt, tau=tau)
     torch.cuda.synchronize(Dt.device)
     return J.cpu().numpy()
+
+
+def exchange_matrix(basis: Basis, D, *, tau: float = 0.0, n: int = 4, device: int = 0) -> np.ndarray:
+    """K_ab = sum_cd D_cd (ac|bd) of the symmetric density D (numpy), on the
+    GPU: the reference's exchange_matrix (eri/k_exchange/k.py:482; its
+    staged MMD sweep) computed by the fused build, whose K is the same sum
+    over the 8-fold orbits (unscreened at tau = 0)."""
+    eng = FockEngine(basis, device)
+    eng.plan(D, tau, n, export=False)
+    return eng.build_host(D)[1]
 
 
 def eri_block(basis: Basis, a: int, b: int, c: int, d: int, device: int = 0) -> np.ndarray:

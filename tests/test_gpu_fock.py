@@ -120,6 +120,14 @@ def test_jk_matches_libcint(cuda, lib_built, name):
     assert np.abs(G - (g["vj"] - 0.5 * g["vk"])).max() <= 1e-12 * np.abs(g["vj"]).max()
 
 
+def test_exchange_matrix_matches_libcint(cuda, lib_built):
+    """The reference-shaped K driver (eri/k_exchange/k.py:482) on libcint."""
+    from felizjueves_b200.fock import exchange_matrix
+    g = golden("libcint_co_ccpvtz.npz")
+    K = exchange_matrix(_basis_from_npz(g), g["D"])
+    assert np.abs(K - g["vk"]).max() <= 1e-12 * np.abs(g["vk"]).max()
+
+
 @pytest.mark.parametrize("name,atoms,wfn", [("c0_1at", 1, "c0"), ("c0_2at", 2, "c0"),
                                             ("c1_1at", 1, "c1")])
 def test_jk_matches_reference_host_path(cuda, lib_built, name, atoms, wfn):
