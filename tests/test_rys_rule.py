@@ -64,3 +64,46 @@ def test_matches_reference_and_oracle(harness):
         xo, wo = rys.roots_weights(n, T)
         assert np.abs(x - xo).max() <= 1e-12 * np.abs(xo).max()
         assert np.abs(w - wo).max() <= 1e-12 * np.abs(wo).max()
+
+
+def test_rys_boundary_with_hgp_hrr_matches_oracle(oracle_lib, tmp_path):
+    """The Rys boundary (csrc/rys_vrr.h) fed to the HGP class's own HRR
+    tables gives the oracle's ERI blocks (26 canonical quartets of a cluster
+    with shells to l = 3, (ff|ff) among them): 1e-11 of the block's largest
+    element (the HRR's |AB|^k cancellation leaves ~1e-12)."""
+    if shutil.which("g++") is None:
+        pytest.skip("needs g++")
+    from felizjueves_b200 import configs
+    from oracle import oracle
+    exe = tmp_path / "rys_q"
+    c = os.path.join(REPO, "felizjueves_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", c, "-I", os.path.join(REPO, "include"),
+                    os.path.join(REPO, "tests", "rys_quartet_harness.cpp"), os.path.join(c, "rys_table.cpp"),
+                    os.path.join(c, "hgp_tables.cpp"), "-o", str(exe)], check=True)
+    B = configs.cluster(3, 5).basis
+    ob = oracle.OracleBasis.of(B)
+    sh = B.shells
+
+    def canon(q):
+        a, b, cc, d = q
+        if sh[a].l > sh[b].l:
+            a, b = b, a
+        if sh[cc].l > sh[d].l:
+            cc, d = d, cc
+        if (sh[a].l, sh[b].l) > (sh[cc].l, sh[d].l):
+            a, b, cc, d = cc, d, a, b
+        return [a, b, cc, d]
+
+    rng = np.random.default_rng(1)
+    qs = [canon([int(v) for v in rng.integers(0, len(sh), 4)]) for _ in range(25)]
+    fs = [i for i, s in enumerate(sh) if s.l == 3][:2]
+    qs.append([fs[0], fs[1], fs[0], fs[1]])
+    for q in qs:
+        inp = "".join(f"{sh[i].l} {float(sh[i].centre[0])!r} {float(sh[i].centre[1])!r} "
+                      f"{float(sh[i].centre[2])!r} {sh[i].n_prim} "
+                      + " ".join(repr(float(x)) for x in sh[i].exponents) + " "
+                      + " ".join(repr(float(x)) for x in sh[i].coefficients) + "\n" for i in q)
+        out = subprocess.run([str(exe)], input=inp, capture_output=True, text=True, check=True)
+        r = np.array([float(v) for v in out.stdout.split()])
+        m = oracle.eri_block(ob, *q)
+        assert np.abs(r - m).max() <= 1e-11 * np.abs(m).max(), q
