@@ -125,85 +125,133 @@ class Clocks:
 
 # --- CPU baseline: the oracle on a bounded sample ---------------------------
 
-def _time_quartets(args):
-    """Worker (spawned): oracle eri_block + digest-free timing of quartets."""
-    flat, quartets = args
-    sys.path.insert(0, HERE)
+def reference_plan(workload: str):
+    """The reference's own plan of the workload (its f_launches output,
+    eri/fock/launch_f.py:390, recorded by tests/golden/make_golden.py from
+    the reference itself): pairs with their bounds G and kept primitive
+    pairs, batches and launches.  None for a workload with no record."""
+    path = os.path.join(HERE, "tests", "golden", f"plan_{workload}.npz")
+    if not os.path.exists(path):
+        return None
+    z = np.load(path)
+    pb = z["pair_batch"]
+    n_b = len(z["batch_npairs"])
+    first = np.searchsorted(pb, np.arange(n_b))
+    return {"ab": z["pair_ab"], "G": z["pair_G"], "prims": z["prims"], "prim_off": z["prim_off"],
+            "batch_key": z["batch_key"], "batch_first": first, "batch_n": z["batch_npairs"],
+            "launches": z["launches"], "tau": float(z["tau"])}
+
+
+def density_blocks(D, basis):
+    """max |D| over each shell block (kernel_f.py:608-617), n_sh x n_sh."""
+    off = basis.offsets
+    nc = [s.n_cart for s in basis.shells]
+    n = len(nc)
+    A = np.abs(D)
+    rows = np.stack([A[off[i]:off[i] + nc[i]].max(axis=0) for i in range(n)])
+    return np.stack([rows[:, off[j]:off[j] + nc[j]].max(axis=1) for j in range(n)], axis=1)
+
+
+def cpu_estimate(w, plan, D, cores: int, budget_s: float = 6.0, seed: int = 0):
+    """ms of one whole build on `cores` host cores by the oracle (the
+    reference's per-quartet work: ERI block over the plan's kept primitive
+    pairs + the six-block digest), estimated from a timed sample.
+
+    Per (class, K_AB, K_CD) launch key: 256 launched quartets drawn (launch
+    by its quartet count, then bra and ket uniformly) and put through the
+    reference's six-block screen with the plan's G (walk_f.py:344-351) give
+    the key's computed fraction; computed quartets drawn the same way are
+    timed (a pilot of 2 per key, then as many more as fill about `budget_s`
+    s of CPU).  Estimate = sum over keys of launched x computed fraction x
+    mean time per computed quartet, / cores (the sample ran on `cores`
+    threads at once).  Returns (ms, description, cpu_seconds_timed)."""
     from oracle import oracle as O
-    ob = O.OracleBasis(*flat)
-    out = []
-    for q in quartets:
-        t = time.perf_counter()
-        O.eri_block(ob, *q)
-        out.append(time.perf_counter() - t)
-    return out
-
-
-def cpu_sample(w, lstats, plan, cores: int, budget_s: float = 15.0, seed: int = 0):
-    """Estimated ms of the whole build on the oracle: per (class, K_AB, K_CD)
-    launch key, time the oracle's ERI block on sampled computed-class
-    quartets of that key; weight by the computed counts of the last GPU
-    build.  A pilot of 2 quartets per key sets how many more each key gets
-    so that the sampled CPU work comes to about `budget_s` seconds (at most
-    200 per key).  Returns (ms_estimate, description, cpu_seconds_spent,
-    wall_seconds)."""
-    import multiprocessing as mp
     rng = np.random.default_rng(seed)
+    ab, G, bk = plan["ab"], plan["G"], plan["batch_key"]
+    first, nb = plan["batch_first"], plan["batch_n"]
+    tau = plan["tau"]
+    Dsh = density_blocks(D, w.basis)
+    LI = plan["launches"][:, 0].astype(np.int64)
+    LJ = plan["launches"][:, 1].astype(np.int64)
+    nI, nJ = nb[LI].astype(np.int64), nb[LJ].astype(np.int64)
+    diag = LI == LJ
+    nq = np.where(diag, nI * (nI + 1) // 2, nI * nJ)
     keys = {}
-    for li, s in enumerate(lstats):
-        if s["computed"] == 0:
-            continue
-        k = (s["la"], s["lb"], s["lc"], s["ld"], s["kab"], s["kcd"])
+    for li in range(len(LI)):
+        k = (int(bk[LI[li]][0]), int(bk[LI[li]][1]), int(bk[LJ[li]][0]), int(bk[LJ[li]][1]),
+             int(bk[LI[li]][2]), int(bk[LJ[li]][2]))
         keys.setdefault(k, []).append(li)
-    batches = plan.batches
-    f = w.basis.flat()
-    flat = (f["l"], f["centre"], f["prim0"], f["nprim"], f["exps"], f["coefs"])
+    keys = {k: np.asarray(v, np.int64) for k, v in sorted(keys.items())}
 
-    def draw(n_per):
-        samples, owners = [], []
-        for k, lis in sorted(keys.items()):
-            for _ in range(n_per):
-                L = plan.launches[lis[int(rng.integers(len(lis)))]]
-                bp = batches[L.bra].pairs[int(rng.integers(len(batches[L.bra].pairs)))]
-                kp = batches[L.ket].pairs[int(rng.integers(len(batches[L.ket].pairs)))]
-                samples.append((bp.a, bp.b, kp.a, kp.b))
-                owners.append(k)
-        return samples, owners
+    def draw(k, m):
+        ls = keys[k]
+        wts = nq[ls].astype(np.float64)
+        li = ls[rng.choice(len(ls), size=m, p=wts / wts.sum())]
+        ib = (rng.random(m) * nI[li]).astype(np.int64)
+        lo = np.where(diag[li], ib, 0)
+        ik = lo + (rng.random(m) * (nJ[li] - lo)).astype(np.int64)
+        pi, pk = first[LI[li]] + ib, first[LJ[li]] + ik
+        a, b, c, d = ab[pi, 0], ab[pi, 1], ab[pk, 0], ab[pk, 1]
+        dmax = np.maximum.reduce([2.0 * Dsh[a, b], 2.0 * Dsh[c, d], 0.5 * Dsh[a, c],
+                                  0.5 * Dsh[a, d], 0.5 * Dsh[b, c], 0.5 * Dsh[b, d]])
+        on = ~(G[pi] * (G[pk] * dmax) < tau)
+        same = diag[li] & (ib == ik)
+        return pi, pk, same, on
 
-    def run(samples, owners, per):
-        chunks = [samples[i::cores] for i in range(cores)]
-        with mp.get_context("spawn").Pool(cores) as pool:
-            res = pool.map(_time_quartets, [(flat, c) for c in chunks])
-        spent = 0.0
-        for i in range(cores):
-            for idx, t in zip(range(i, len(samples), cores), res[i]):
-                per.setdefault(owners[idx], []).append(t)
-                spent += t
-        return spent
+    frac, cand = {}, {}
+    for k in keys:
+        pi, pk, same, on = draw(k, 256)
+        frac[k] = float(on.mean())
+        cand[k] = (pi[on], pk[on], same[on])
+    ob = O.OracleBasis.of(w.basis)
+    po, prims = plan["prim_off"], plan["prims"]
 
-    per: dict = {}
-    t0 = time.perf_counter()
-    pilot = draw(2)
-    spent = run(*pilot, per)
-    n_more = int(min(200, max(0, 2 * (budget_s / max(spent, 1e-9) - 1))))
-    n_samples = len(pilot[0])
+    def run(items):
+        qs, dg, kept, owner = [], [], [], []
+        for k, (pi, pk, same) in items:
+            for x, y, z in zip(pi, pk, same):
+                a, b = ab[x]
+                c, d = ab[y]
+                qs.append((a, b, c, d))
+                dg.append((0.5 if a == b else 1.0) * (0.5 if c == d else 1.0) * (0.5 if z else 1.0))
+                kept.append((prims[po[x]:po[x + 1]], prims[po[y]:po[y + 1]]))
+                owner.append(k)
+        if not qs:
+            return {}, 0.0
+        _, _, sec = O.fock_quartets(ob, D, qs, dg, kept, threads=cores)
+        per = {}
+        for k, t in zip(owner, sec):
+            per.setdefault(k, []).append(float(t))
+        return per, float(sec.sum())
+
+    def computed(k, m):
+        got = [[], [], []]
+        while len(got[0]) < m:
+            pi, pk, same, on = draw(k, max(64, int(2 * m / max(frac[k], 1e-3))))
+            for g, x in zip(got, (pi[on], pk[on], same[on])):
+                g.extend(x.tolist())
+        return tuple(np.asarray(g[:m]) for g in got)
+
+    live = [k for k in keys if frac[k] > 0.0]
+    per, spent = run([(k, tuple(x[:2] for x in cand[k])) for k in live])
+    n_more = int(min(100, max(0.0, budget_s / max(spent, 1e-9) - 1.0) * 2))
     if n_more:
-        more = draw(n_more)
-        spent += run(*more, per)
-        n_samples += len(more[0])
-    wall = time.perf_counter() - t0
-    total_cpu_s = 0.0
-    for k, lis in keys.items():
-        # the oracle sums every primitive pair of the sampled shells (no
-        # pruning), so the estimate is an upper bound on the pruned work
-        cnt = sum(lstats[li]["computed"] for li in lis)
-        total_cpu_s += cnt * float(np.median(per[k]))
-    ms = 1e3 * total_cpu_s / cores
-    desc = (f"oracle eri_block (MMD, FP64) on {n_samples} sampled quartets, {2 + n_more} per "
-            f"(class, K_AB, K_CD) key of the build's computed launches ({len(keys)} keys), median time "
-            f"per key x computed quartets, summed, / {cores} core(s); {spent:.1f} s of CPU sampled; "
-            f"digest not timed")
-    return ms, desc, spent, wall
+        more, s2 = run([(k, computed(k, n_more)) for k in live])
+        spent += s2
+        for k, v in more.items():
+            per.setdefault(k, []).extend(v)
+    n_timed = sum(len(v) for v in per.values())
+    total = 0.0
+    for k in live:
+        total += float(nq[keys[k]].sum()) * frac[k] * float(np.mean(per[k]))
+    ms = 1e3 * total / cores
+    desc = (f"oracle (the reference's eri_block over the plan's kept primitive pairs + the six-block "
+            f"digest) on {n_timed} sampled computed quartets of the reference's own plan of the "
+            f"workload ({len(keys)} (class, K_AB, K_CD) keys); computed fraction per key from 256 "
+            f"draws through the reference's six-block screen; mean time per key x launched x "
+            f"fraction, summed, / {cores} threads (the sample ran on {cores} threads); "
+            f"{spent:.1f} s of CPU timed")
+    return ms, desc, spent
 
 
 # --- the GPU arm --------------------------------------------------------------
@@ -298,24 +346,38 @@ def main():
     launched = sum(s["launched"] for s in ls)
 
     e2e = None
-    if not a.no_e2e and rank == 0:
-        Dh = [configs.perturbed_density(w.D, i) for i in range(3)]
-        eng.build_host(Dh[0], precision=prec, threshold=a.threshold)  # warm
-        k2 = min(a.steps, 3)
+    if not a.no_e2e:
+        # the same W + K sequence through the host-buffer C ABI: each step
+        # copies its density in from pinned host memory and J, K, G out
+        def pinned():
+            return torch.empty((n, n), dtype=torch.float64, pin_memory=True).numpy()
+        Dh = []
+        for i in range(n_d):
+            x = pinned()
+            x[...] = configs.perturbed_density(w.D, i)
+            Dh.append(x)
+        outs = (pinned(), pinned(), pinned())
+        for i in range(a.warmup):
+            eng.build_host(Dh[i % n_d], precision=prec, threshold=a.threshold, out=outs)
+        replicas.barrier(dist)
         t0 = time.perf_counter()
-        for i in range(k2):
-            eng.build_host(Dh[i % 3], precision=prec, threshold=a.threshold)
-        e2e_ms = (time.perf_counter() - t0) * 1e3 / k2
+        for i in range(a.steps):
+            eng.build_host(Dh[i % n_d], precision=prec, threshold=a.threshold, out=outs)
+        e2e_ms = replicas.max_over_ranks(dist, (time.perf_counter() - t0) * 1e3 / a.steps,
+                                         f"cuda:{local}")
         e2e = {"value": round(e2e_ms, 3), "unit": "ms/iter", "h2d_bytes_per_step": n * n * 8,
-               "d2h_bytes_per_step": 3 * n * n * 8,
-               "api": "fjb_fock_build_host (C ABI, host buffers; copies in the timed region)"}
+               "d2h_bytes_per_step": 3 * n * n * 8, "steps": a.steps, "warmup": a.warmup,
+               "api": "fjb_fock_build_host (C ABI; pinned host buffers; H2D of D, build, D2H of "
+                      "J, K, G inside the timed region, host clock, max over ranks)"}
 
     cpu = None
     if not a.no_cpu and rank == 0 and world == 1:
-        cores = 1
-        est, desc, spent, wall = cpu_sample(w, ls, P, cores)
-        cpu = {"value": round(est, 1), "unit": "ms/iter", "cores": cores, "kind": "port",
-               "sample": desc}
+        plan = reference_plan(a.workload)
+        if plan is not None:
+            cores = os.cpu_count() or 1
+            est, desc, spent = cpu_estimate(w, plan, configs.perturbed_density(w.D, 0), cores)
+            cpu = {"value": round(est, 1), "unit": "ms/iter", "cores": cores, "kind": "port",
+                   "estimate": "extrapolated from a timed sample", "sample": desc}
 
     out = {
         "metric": METRIC, "value": round(ms, 3), "unit": "ms/iter", "n_gpus": world,
@@ -513,33 +575,49 @@ def batch_path(a, local):
 
 
 def reference_arm(a, rank, world):
+    """The reference's CPU path on this host: the reference is pure Python
+    (its host path at the workload's size is infeasible: the 6-atom c0 takes
+    the times tests/golden/cpu_c0.npz records), so the arm runs its
+    restatement, the oracle (oracle/oracle.c: the reference's eri_block over
+    the plan's kept primitive pairs plus the six-block digest), on every host
+    thread.  The quartets are the reference's own plan of the workload
+    (tests/golden/plan_<workload>.npz, written by the reference's
+    f_launches), screened by the reference's six-block rule; this library is
+    not loaded.  Each of W + K steps is an independent timed sample (about
+    12 s of CPU) extrapolated to one whole build; the value is the median
+    over the K timed steps.  Rank 0 only."""
     if rank != 0:
         return
     from felizjueves_b200 import configs
-    from felizjueves_b200.fock import FockEngine
     w = configs.by_name(a.workload)
-    # the plan is host work (no GPU); its launch counts come from the plan
-    eng = FockEngine(w.basis, device=-1)
-    P = eng.plan(w.D, w.tau, w.n_mag)
-    ls = eng.launch_stats()
-    # without a GPU build, every launched quartet is counted as computed:
-    # the extrapolation is an upper bound on the CPU work of the screened
-    # build by the fraction the six-block screen skips
-    for s in ls:
-        s["computed"] = s["launched"]
+    plan = reference_plan(a.workload)
+    if plan is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          f"no recorded reference plan for workload {a.workload}"}))
+        return
     cores = os.cpu_count() or 1
-    times = []
-    for i in range(max(1, a.warmup) + a.steps if a.steps <= 3 else 1 + min(a.steps, 3)):
-        est, desc, spent, wall = cpu_sample(w, ls, P, cores, seed=i)
-        times.append(est)
-    v = float(np.median(times[1:] if len(times) > 1 else times))
+    t0 = time.perf_counter()
+    times, spent = [], 0.0
+    for i in range(a.warmup + a.steps):
+        est, desc, cpu_s = cpu_estimate(w, plan, configs.perturbed_density(w.D, i % 20), cores,
+                                        seed=i)
+        spent += cpu_s
+        if i >= a.warmup:
+            times.append(est)
+    wall = time.perf_counter() - t0
+    v = float(np.median(times))
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms/iter",
         "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(v, 1),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": WORKLOAD},
+        "data": "synthetic (seeded cluster, random symmetric densities)",
+        "config": {"workload": WORKLOAD, "n_ao": w.n_ao, "shells": len(w.basis.shells),
+                   "tau": w.tau},
+        "estimate": "extrapolated: each step times a sample of the build's computed quartets "
+                    "and scales it to the whole build; the build itself is not run",
+        "sample_wall_s": round(wall, 1), "sample_cpu_s": round(spent, 1),
         "cpu_baseline": {"value": round(v, 1), "unit": "ms/iter", "cores": cores, "kind": "port",
-                         "sample": desc + "; every launched quartet counted (no GPU screen)"},
+                         "sample": desc},
         "e2e": {"value": round(v, 1), "unit": "ms/iter", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}))
 

@@ -289,13 +289,21 @@ class FockEngine:
                       C.c_void_p(st.cuda_stream)), self._h)
         return tuple(out)
 
-    def build_host(self, D, *, precision: int = _lib.FJB_FP64, threshold: float = 0.0):
+    def build_host(self, D, *, precision: int = _lib.FJB_FP64, threshold: float = 0.0, out=None):
         """Host build through the C ABI's host-buffer entry point: numpy in,
-        (J, K, G) numpy out."""
+        (J, K, G) numpy out -- into `out`, three C-contiguous float64 n x n
+        arrays (e.g. views of pinned host memory), when given."""
         self._require_plan()
         A = _checked_density(self.basis, D)
         n = self.n_ao
-        J, K, G = (np.empty((n, n)) for _ in range(3))
+        if out is None:
+            J, K, G = (np.empty((n, n)) for _ in range(3))
+        else:
+            J, K, G = out
+            for M in out:
+                if not (isinstance(M, np.ndarray) and M.dtype == np.float64 and M.shape == (n, n)
+                        and M.flags.c_contiguous):
+                    raise ValueError(f"out: three C-contiguous float64 {n} x {n} arrays")
         _lib.check(self._L.fjb_fock_build_host(self._h, A.ctypes.data, J.ctypes.data,
                                                K.ctypes.data, G.ctypes.data,
                                                int(precision), float(threshold)), self._h)
@@ -420,9 +428,10 @@ class FockEngine:
         return [{k: getattr(arr[i], k) for k, _ in _lib.ClassStat_t._fields_}
                 for i in range(nc.value)]
 
-    def screen_mask(self, D) -> np.ndarray:
+    def screen_mask(self, D, at=None) -> np.ndarray:
         """Per launched quartet (launch, bra pair, ket pair order), 1 when
-        the six-block screen skips it (walk_f.py:344-380)."""
+        the six-block screen skips it (walk_f.py:344-380); only the entries
+        at positions `at` (gathered on the device) when given."""
         import torch
         self._require_plan()
         Dt = torch.as_tensor(_checked_density(self.basis, D if not hasattr(D, "cpu") else D.cpu().numpy()),
@@ -432,6 +441,8 @@ class FockEngine:
                                            C.c_void_p(torch.cuda.current_stream(Dt.device).cuda_stream)),
                    self._h)
         torch.cuda.synchronize(Dt.device)
+        if at is not None:
+            m = m[torch.as_tensor(np.asarray(at, np.int64), device=Dt.device)]
         return m.cpu().numpy()
 
     def eri_blocks(self, quartets, fp32: bool = False) -> list[np.ndarray]:

@@ -339,7 +339,13 @@ int fjb_set_class_config32(fjb_handle *h, int la, int lb, int lc, int ld, int th
  * a device looks up the array's device address (cudaGetSymbolAddress), so
  * make that first call before any stream capture.  Every call shares the
  * one array: calls that overlap on the GPU (two streams, two handles, two
- * threads) race and corrupt each other's results; serialise them. */
+ * threads) race and corrupt each other's results; serialise them.  The
+ * address is kept per device ordinal for the life of the process and
+ * belongs to the device's primary context (the runtime's): do not reset the
+ * device (cudaDeviceReset) or drive the call from another context while the
+ * library is loaded.  fjb_last_build_stats, fjb_launch_stats and
+ * fjb_class_stats describe the last fjb_fock_build only: this call records
+ * no statistics and leaves theirs as they were. */
 #define FJB_NOALLOC_MAX_AO 512
 #define FJB_NOALLOC_MAX_SHELLS 256
 #define FJB_NOALLOC_SCRATCH_DOUBLES                                              \

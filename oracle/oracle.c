@@ -36,6 +36,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -494,5 +495,123 @@ int or_jk_unique(const or_basis *B, const double *D, double *J, double *K,
     free_all(B, sp);
     free(pa);
     free(pb);
+    return 0;
+}
+
+/* The reference's per-quartet work of the fused build, timed: for each of n
+ * unique quartets (a, b | c, d) given with its degeneracy, the ERI block
+ * (eri/eri.py:86-145) and the six-block digest into J and K
+ * (eri/fock/kernel_f.py:94-131: Coulomb weight 2 on the ab and cd blocks,
+ * exchange 1 on ac, ad, bc, bd).  Pairs are made once per distinct (a, b)
+ * of the list, before the timed loop, as a sweep makes them once.  With
+ * `kept`, each pair keeps only the plan's primitive pairs (the reference's
+ * pruned pair, ao/pairs.py:545): the list of the pair in slot q (the bra of
+ * quartet q / 2 when q is even, its ket when odd) is
+ * kept[kept_off[q] .. kept_off[q + 1]), indices i * nprim_b + j, in the
+ * order they are summed.  The quartets run on nthreads OpenMP threads
+ * (dynamic schedule); sec receives each quartet's own wall time on its
+ * thread.  J and K come back as the unclosed sums (M, not M + M^T). */
+int or_fock_quartets(const or_basis *B, const double *D, int n, const int *quartets,
+                     const double *degs, const int *kept_off, const int *kept, double *J,
+                     double *K, int nthreads, double *sec) {
+    gl_init();
+    if (check_basis(B)) return -1;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    const int ns = B->n_sh, nao = B->n_ao;
+    /* distinct pairs of the list */
+    int *slot = (int *)malloc(sizeof(int) * (size_t)ns * ns);
+    for (size_t i = 0; i < (size_t)ns * ns; ++i) slot[i] = -1;
+    int np = 0;
+    for (int q = 0; q < 2 * n; ++q) {
+        const int a = quartets[2 * q], b = quartets[2 * q + 1];
+        if (slot[a * ns + b] < 0) slot[a * ns + b] = np++;
+    }
+    shell_pair *sp = (shell_pair *)calloc((size_t)(np ? np : 1), sizeof(shell_pair));
+    for (int q = 0; q < 2 * n; ++q) {
+        const int a = quartets[2 * q], b = quartets[2 * q + 1];
+        shell_pair *p = &sp[slot[a * ns + b]];
+        if (p->pp) continue;
+        make_pair(B, a, b, p);
+        if (kept) {
+            /* keep the plan's primitive pairs (index i * nprim_b + j), in order */
+            const int k0 = kept_off[q], k1 = kept_off[q + 1];
+            prim_pair *sel = (prim_pair *)calloc((size_t)(k1 - k0 ? k1 - k0 : 1), sizeof(prim_pair));
+            char *used = (char *)calloc((size_t)p->K, 1);
+            for (int k = k0; k < k1; ++k) {
+                sel[k - k0] = p->pp[kept[k]];
+                used[kept[k]] = 1;
+            }
+            for (int k = 0; k < p->K; ++k)
+                if (!used[k]) free(p->pp[k].E);
+            free(used);
+            free(p->pp);
+            p->pp = sel;
+            p->K = k1 - k0;
+        }
+    }
+    size_t nn = (size_t)nao * nao;
+    memset(J, 0, sizeof(double) * nn);
+    memset(K, 0, sizeof(double) * nn);
+#pragma omp parallel
+    {
+        double *blk = (double *)malloc(sizeof(double) * 28 * 28 * 28 * 28);
+#pragma omp for schedule(dynamic, 1)
+        for (int q = 0; q < n; ++q) {
+            struct timespec t0, t1;
+            clock_gettime(CLOCK_MONOTONIC, &t0);
+            const int a = quartets[4 * q], b = quartets[4 * q + 1], c = quartets[4 * q + 2],
+                      d = quartets[4 * q + 3];
+            eri_pairs(&sp[slot[a * ns + b]], &sp[slot[c * ns + d]], blk, NULL);
+            const int na = ncart(B->l[a]), nb = ncart(B->l[b]), nc = ncart(B->l[c]),
+                      nd = ncart(B->l[d]);
+            const int oa = B->ao_off[a], ob = B->ao_off[b], oc = B->ao_off[c], od = B->ao_off[d];
+            const double deg = degs[q];
+            /* the six blocks of this quartet, then one add per element */
+            double jab[28 * 28], jcd[28 * 28], kac[28 * 28], kad[28 * 28], kbc[28 * 28], kbd[28 * 28];
+            memset(jab, 0, sizeof(double) * na * nb);
+            memset(jcd, 0, sizeof(double) * nc * nd);
+            memset(kac, 0, sizeof(double) * na * nc);
+            memset(kad, 0, sizeof(double) * na * nd);
+            memset(kbc, 0, sizeof(double) * nb * nc);
+            memset(kbd, 0, sizeof(double) * nb * nd);
+#define DD(u, v) D[(size_t)(u) * nao + (v)]
+            for (int i = 0; i < na; ++i)
+                for (int j = 0; j < nb; ++j)
+                    for (int k = 0; k < nc; ++k)
+                        for (int l = 0; l < nd; ++l) {
+                            const double x = deg * blk[(size_t)(i * nb + j) * nc * nd + k * nd + l];
+                            jab[i * nb + j] += 2.0 * DD(oc + k, od + l) * x;
+                            jcd[k * nd + l] += 2.0 * DD(oa + i, ob + j) * x;
+                            kac[i * nc + k] += DD(ob + j, od + l) * x;
+                            kad[i * nd + l] += DD(ob + j, oc + k) * x;
+                            kbc[j * nc + k] += DD(oa + i, od + l) * x;
+                            kbd[j * nd + l] += DD(oa + i, oc + k) * x;
+                        }
+#undef DD
+#define ADD(M, r, c_, v) do { double *m_ = &M[(size_t)(r) * nao + (c_)]; const double v_ = (v); \
+                              _Pragma("omp atomic") *m_ += v_; } while (0)
+            for (int i = 0; i < na; ++i)
+                for (int j = 0; j < nb; ++j) ADD(J, oa + i, ob + j, jab[i * nb + j]);
+            for (int k = 0; k < nc; ++k)
+                for (int l = 0; l < nd; ++l) ADD(J, oc + k, od + l, jcd[k * nd + l]);
+            for (int i = 0; i < na; ++i) {
+                for (int k = 0; k < nc; ++k) ADD(K, oa + i, oc + k, kac[i * nc + k]);
+                for (int l = 0; l < nd; ++l) ADD(K, oa + i, od + l, kad[i * nd + l]);
+            }
+            for (int j = 0; j < nb; ++j) {
+                for (int k = 0; k < nc; ++k) ADD(K, ob + j, oc + k, kbc[j * nc + k]);
+                for (int l = 0; l < nd; ++l) ADD(K, ob + j, od + l, kbd[j * nd + l]);
+            }
+#undef ADD
+            clock_gettime(CLOCK_MONOTONIC, &t1);
+            if (sec) sec[q] = (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+        }
+        free(blk);
+    }
+    for (int i = 0; i < np; ++i) free_pair(&sp[i]);
+    free(sp);
+    free(slot);
     return 0;
 }

@@ -44,6 +44,9 @@ def lib():
         L.or_jk_ordered.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_int]
         L.or_jk_unique.argtypes = L.or_jk_ordered.argtypes
+        L.or_fock_quartets.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                       C.c_void_p]
         _lib = L
     return _lib
 
@@ -107,3 +110,33 @@ def jk(ob: OracleBasis, D, *, ordered=False, threads=0):
     if rc:
         raise ValueError(f"oracle jk refused: {rc}")
     return J, K
+
+
+def fock_quartets(ob: OracleBasis, D, quartets, degs, kept=None, threads=0):
+    """The reference's per-quartet work of the fused build (ERI block + the
+    six-block digest) on a list of unique quartets, timed per quartet on
+    `threads` OpenMP threads.  `kept`: per quartet a (bra, ket) pair of
+    kept-primitive index lists (the plan's pruned pairs), or None for every
+    primitive.  Returns (J, K, seconds per quartet); J, K unclosed."""
+    D = np.ascontiguousarray(D, np.float64)
+    q = np.ascontiguousarray(quartets, np.int32).reshape(-1, 4)
+    n = len(q)
+    dg = np.ascontiguousarray(degs, np.float64)
+    assert dg.shape == (n,)
+    koff = kidx = None
+    if kept is not None:
+        lists = [lst for pair in kept for lst in pair]
+        assert len(lists) == 2 * n
+        koff = np.ascontiguousarray(np.concatenate([[0], np.cumsum([len(x) for x in lists])]), np.int32)
+        kidx = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32) for x in lists])
+                                    if n else np.zeros(1, np.int32), np.int32)
+    J = np.zeros((ob.n_ao, ob.n_ao))
+    K = np.zeros_like(J)
+    sec = np.zeros(max(n, 1))
+    rc = lib().or_fock_quartets(C.byref(ob.s), D.ctypes.data, n, q.ctypes.data, dg.ctypes.data,
+                                koff.ctypes.data if koff is not None else None,
+                                kidx.ctypes.data if kidx is not None else None,
+                                J.ctypes.data, K.ctypes.data, int(threads), sec.ctypes.data)
+    if rc:
+        raise ValueError(f"oracle fock_quartets refused: {rc}")
+    return J, K, sec[:n]

@@ -9,7 +9,7 @@ files this script writes.
 
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
-parts: libcint boys eri plan_c0 plan_c1 jk_small screen_c0 cost jplan_c0 scatter_c0 onee
+parts: libcint boys eri plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 scatter_c0 onee
 scf bse harmonics grad rys (default: all
 but plan_c1 and jk_small, which take minutes).
 """
@@ -541,6 +541,68 @@ def part_screen_c0():
     print("screen_c0", len(rows), "quartets launched,", int(rows[:, 3].sum()), "skipped")
 
 
+def part_screen_c1():
+    """walk_f's six-block prediction (walk_f.py:344-351) on a sample of the
+    64-atom cluster's 1.34e9 launched quartets: for every (class, K_AB, K_CD)
+    key, the 12 candidates (of 400 drawn) whose bound G_ab (G_cd dmax) lies
+    nearest tau -- the decisions a rounding difference would flip -- and 8
+    drawn at random.  Rows (launch, ib, ik, skip) in the launch's
+    orientation, as screen_c0."""
+    _ref_imports()
+    from felizjueves.eri.fock import kernel_f as KF
+    from felizjueves_b200 import configs
+    w = configs.c1()
+    P = _plan(w, parallel_bounds=True)
+    rb = ref_basis(w.basis)
+    n_sh = len(rb.shells)
+    t = time.time()
+    Dsh = KF.density_blocks(w.D.tolist(), rb.offsets, [s.n_cart for s in rb.shells])
+    print("density_blocks", round(time.time() - t, 1), "s", flush=True)
+    wabs = [abs(KF.WEIGHTS.of(b)) for b in KF.BLOCKS]
+    tau = P.tau
+
+    def bound(br, kt):
+        s = (br.a, br.b, kt.a, kt.b)
+        dmax = wabs[0] * Dsh[s[0] * n_sh + s[1]]
+        for wv, (u, v) in zip(wabs[1:], KF.BLOCKS[1:]):
+            x = wv * Dsh[s[u] * n_sh + s[v]]
+            if dmax < x:
+                dmax = x
+        return br.G * (kt.G * dmax)
+
+    by_key = {}
+    for li, L in enumerate(P.launches):
+        B, K = P.batches[L.bra], P.batches[L.ket]
+        diag = L.bra == L.ket
+        nq = len(B.pairs) * len(K.pairs) if not diag else \
+            len(B.pairs) * (len(B.pairs) + 1) // 2
+        by_key.setdefault((B.la, B.lb, K.la, K.lb, B.degree, K.degree), []).append((li, nq))
+    rng = np.random.default_rng(11)
+    rows = []
+    for key in sorted(by_key):
+        ls = by_key[key]
+        wts = np.asarray([nq for _, nq in ls], np.float64)
+        cand = []
+        for _ in range(400):
+            li = ls[int(rng.choice(len(ls), p=wts / wts.sum()))][0]
+            L = P.launches[li]
+            bras, kets = P.batches[L.bra].pairs, P.batches[L.ket].pairs
+            ib = int(rng.integers(len(bras)))
+            ik = int(rng.integers(ib if L.bra == L.ket else 0, len(kets)))
+            cand.append((li, ib, ik, bound(bras[ib], kets[ik])))
+        cand = list({(c[0], c[1], c[2]): c for c in cand}.values())
+        near = sorted(cand, key=lambda c: abs(math.log(max(c[3], 1e-300) / tau)))[:12]
+        rest = [c for c in cand if c not in near]
+        pick = near + [rest[i] for i in rng.permutation(len(rest))[:8]]
+        for li, ib, ik, b in pick:
+            rows.append((li, ib, ik, int(b < tau)))
+    rows = np.asarray(sorted(rows), np.int32)
+    np.savez_compressed(os.path.join(HERE, "screen_c1_sample.npz"), rows=rows,
+                        n_launched=np.int64(sum(nq for v in by_key.values() for _, nq in v)))
+    print("screen_c1_sample", len(rows), "quartets from", len(by_key), "keys,",
+          int(rows[:, 3].sum()), "skipped")
+
+
 # --- J and K on small nested systems (reference host path) ------------------
 
 
@@ -557,6 +619,40 @@ def _jk(args):
     else:
         M = exchange_matrix(rb, w.D.tolist(), pq=pq)
     return which, np.asarray(M, np.float64), time.time() - t
+
+
+def _jk_screened(args):
+    which, w = args
+    _ref_imports()
+    from felizjueves.eri.j_coulomb.j import coulomb_matrix
+    from felizjueves.eri.k_exchange.k import exchange_matrix
+    from felizjueves.reference.pq import pq
+    rb = ref_basis(w.basis)
+    t = time.time()
+    f = coulomb_matrix if which == "J" else exchange_matrix
+    M = f(rb, w.D.tolist(), pq=pq, tau=w.tau)
+    return which, np.asarray(M, np.float64), time.time() - t
+
+
+def part_cpu_c0():
+    """The reference's own host path on the 6-atom workload at its tau
+    (1e-12): coulomb_matrix (j.py:436) and exchange_matrix (k.py:482), each
+    single-threaded in its own process, run side by side; G = J - K/2
+    (fock.py:106-108).  Records J, K and each one's wall time."""
+    from felizjueves_b200 import configs
+    w = configs.c0()
+    t = time.time()
+    with mp.get_context("spawn").Pool(2) as pool:
+        res = dict((r[0], r[1:]) for r in pool.map(_jk_screened, [(k, w) for k in ("J", "K")],
+                                                     chunksize=1))
+    (J, tj), (K, tk) = res["J"], res["K"]
+    import platform
+    np.savez_compressed(os.path.join(HERE, "cpu_c0.npz"), J=J, K=K, G=J - 0.5 * K, t_J=tj, t_K=tk,
+                        tau=w.tau, nproc=os.cpu_count(),
+                        cpu=np.asarray(platform.processor() or platform.machine()),
+                        source=np.asarray("reference coulomb_matrix + exchange_matrix, pq path, "
+                                          "tau 1e-12, one process (one core) each"))
+    print("cpu_c0 J", round(tj, 1), "s K", round(tk, 1), "s wall", round(time.time() - t, 1), "s")
 
 
 def part_jk_small():
@@ -671,7 +767,8 @@ def part_cost():
 
 PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_eri,
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
-         "screen_c0": part_screen_c0, "jk_small": part_jk_small,
+         "screen_c0": part_screen_c0, "screen_c1": part_screen_c1, "jk_small": part_jk_small,
+         "cpu_c0": part_cpu_c0,
          "cost": part_cost, "jplan_c0": part_jplan_c0, "scatter_c0": part_scatter_c0,
          "onee": part_onee, "scf": part_scf, "bse": part_bse,
          "harmonics": part_harmonics, "grad": part_grad, "rys": part_rys}

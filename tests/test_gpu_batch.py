@@ -11,6 +11,29 @@ from felizjueves_b200 import configs
 pytestmark = pytest.mark.gpu
 
 
+def test_batch_graph_matches_oracle(cuda, lib_built, oracle_lib):
+    """Each molecule of a captured batch against the oracle directly: the
+    FP64 graph within the screened build's bar (tau = 1e-12: every skipped
+    term is below tau by the proved bounds), the routed graph within the
+    1e-8 budget."""
+    import torch
+    from felizjueves_b200 import _lib
+    from felizjueves_b200.batch import BatchBuilder
+    ws = [configs.cluster(n, 4200 + n) for n in (3, 2, 4)]
+    bb = BatchBuilder(ws)
+    Go = []
+    for w in ws:
+        Jo, Ko = oracle_lib.jk(oracle_lib.OracleBasis.of(w.basis), w.D)
+        Go.append(Jo - 0.5 * Ko)
+    for name, prec, thr, bar in (("fp64", _lib.FJB_FP64, 0.0, 1e-9),
+                                 ("routed", _lib.FJB_ROUTED, 1e-9, 1e-8)):
+        bb.capture(name, prec, thr)
+        bb.replay(name)
+        torch.cuda.synchronize()
+        for g, go in zip(bb.G(), Go):
+            assert float(np.abs(g.cpu().numpy() - go).max()) <= bar, name
+
+
 def test_batch_graph_matches_per_molecule_builds(cuda, lib_built):
     import torch
     from felizjueves_b200 import _lib

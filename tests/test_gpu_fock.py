@@ -107,6 +107,31 @@ def test_c0_screen_mask_bit_exact(cuda, lib_built):
     assert np.array_equal(m, z["rows"][:, 3].astype(np.uint8))
 
 
+def test_c1_screen_mask_bit_exact_on_sample(cuda, lib_built):
+    """The 64-atom cluster's six-block mask (1.34e9 launched quartets) on the
+    reference's walk_f prediction for 16,800 sampled launched quartets: per
+    (class, K_AB, K_CD) key the 12 of 400 draws whose bound lies nearest tau
+    and 8 at random (tests/golden/make_golden.py part_screen_c1)."""
+    w = configs.c1()
+    z = golden("screen_c1_sample.npz")
+    eng = FockEngine(w.basis)
+    P = eng.plan(w.D, w.tau, w.n_mag)
+    assert P.quartets_launched == int(z["n_launched"])
+    qbase, q = [], 0
+    for L in P.launches:
+        nb, nk = len(P.batches[L.bra].pairs), len(P.batches[L.ket].pairs)
+        qbase.append(q)
+        q += nb * (nb + 1) // 2 if L.bra == L.ket else nb * nk
+    rows = z["rows"].astype(np.int64)
+    li, ib, ik = rows[:, 0], rows[:, 1], rows[:, 2]
+    n_ket = np.asarray([len(P.batches[P.launches[i].ket].pairs) for i in li], np.int64)
+    diag = np.asarray([P.launches[i].bra == P.launches[i].ket for i in li])
+    row = np.where(diag, ib * n_ket - ib * (ib - 1) // 2 - ib, ib * n_ket)
+    at = np.asarray(qbase, np.int64)[li] + row + ik
+    m = eng.screen_mask(w.D, at=at)
+    assert np.array_equal(m, rows[:, 3].astype(np.uint8)), int((m != rows[:, 3]).sum())
+
+
 LIBCINT = ["h2_sto3g", "h2o_sto3g", "h2o_631g", "h2o_ccpvdz", "h10_chain_ccpvdz", "co_ccpvtz"]
 
 

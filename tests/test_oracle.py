@@ -102,3 +102,24 @@ def test_df_integrals_match_libcint(oracle_lib, name):
     got = odf.metric(aux) if str(z["kind"]) == "metric" else odf.eri3(ao, aux)
     ref = z["value"]
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_fock_quartets_equals_unique_sweep(oracle_lib):
+    """The timed per-quartet sample function (ERI block + six-block digest)
+    over every unique quartet of c0, closed, equals the orbit sweep."""
+    from felizjueves_b200 import configs
+    w = configs.c0()
+    ob = oracle_lib.OracleBasis.of(w.basis)
+    n = len(w.basis.shells)
+    pairs = [(a, b) for a in range(n) for b in range(a, n)]
+    qs, dg = [], []
+    for P in range(len(pairs)):
+        for Q in range(P, len(pairs)):
+            (a, b), (c, d) = pairs[P], pairs[Q]
+            qs.append((a, b, c, d))
+            dg.append((0.5 if a == b else 1.0) * (0.5 if c == d else 1.0) * (0.5 if P == Q else 1.0))
+    J, K, sec = oracle_lib.fock_quartets(ob, w.D, qs, dg, threads=4)
+    Jo, Ko = oracle_lib.jk(ob, w.D)
+    assert np.abs(J + J.T - Jo).max() <= 1e-12
+    assert np.abs(K + K.T - Ko).max() <= 1e-12
+    assert sec.shape == (len(qs),) and np.all(sec > 0)

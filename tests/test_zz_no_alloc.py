@@ -47,3 +47,22 @@ def test_noalloc_refuses_sizes_beyond_its_scratch(cuda, lib_built):
                                             out.data_ptr(), out.data_ptr(), None)
     assert rc == -4
     assert b"exceed its fixed scratch" in _lib.load().fjb_last_error(eng._h)
+
+
+def test_noalloc_build_matches_oracle(cuda, lib_built, oracle_lib):
+    """The no-allocation build held directly to the oracle (3-atom cluster,
+    every class to (ff|ff), unscreened), at the plain FP64 bar."""
+    import torch
+    w = configs.cluster(3, 5)
+    eng = FockEngine(w.basis)
+    eng.plan(w.D, 0.0, 4)
+    D = torch.tensor(w.D, device=cuda)
+    J, K, G = (torch.full_like(D, np.nan) for _ in range(3))
+    st = C.c_void_p(torch.cuda.current_stream(cuda).cuda_stream)
+    _lib.check(_lib.load().fjb_fock_build_noalloc(eng._h, D.data_ptr(), J.data_ptr(), K.data_ptr(),
+                                                  G.data_ptr(), st), eng._h)
+    torch.cuda.synchronize()
+    Jo, Ko = oracle_lib.jk(oracle_lib.OracleBasis.of(w.basis), w.D)
+    assert np.abs(J.cpu().numpy() - Jo).max() <= 1e-11
+    assert np.abs(K.cpu().numpy() - Ko).max() <= 1e-11
+    assert np.abs(G.cpu().numpy() - (Jo - 0.5 * Ko)).max() <= 1e-11
