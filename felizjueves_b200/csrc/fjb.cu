@@ -29,6 +29,7 @@
 #include "plan.h"
 #include "scatter.h"
 #include "router.cuh"
+#include "rys_fock.cuh"
 
 namespace fjb {
 std::vector<double> boys_table();
@@ -721,6 +722,12 @@ struct ClassEntry {
 
 struct ClassRun {
     ClassDev dev;  // the interpreter kernel's layout (kept valid for every class)
+    // the Rys kernel (rys_fock.cuh) for this class's FP64 / FP32 units, when
+    // it takes the class: its carve-up, grid and the tabulated rule it reads
+    bool rys64 = false, rys32 = false;
+    RysDev ry64{}, ry32{};
+    int grid_r64 = 0, grid_r32 = 0;
+    const double *rys_tab = nullptr;
     ClassDev dev32;  // the FP32 interpreter's layout (routed builds of classes without has32)
     int unit0 = 0, n_units = 0;
     int grid = 0;
@@ -764,16 +771,29 @@ int sm_count() {
 // warps to a CTA; the interpreter one CTA on a unit.
 int run_grid(const ClassRun &r);
 
-// The FP64 path of a class run (its register kernel, else the interpreter).
+// The FP64 path of a class run: its register kernel, else the Rys kernel,
+// else the interpreter (which alone serves the atomics-free build's slots).
 cudaError_t launch_run(const ClassRun &r, cudaStream_t st, const KArgs &a) {
     if (r.compiled) return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, false, r.grid, st, a);
+    if (r.rys64 && !a.W) {
+        KArgs ar = a;
+        ar.Y = r.ry64;
+        ar.rys_tab = r.rys_tab;
+        return rys_launch(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, false, r.grid_r64, st, ar);
+    }
     return launch_hgp<double>(r.dev, r.grid, st, a);
 }
 
 // The FP32 kernel of a class run (routed builds): its register kernel, else
-// the interpreter in FP32 with its own layout.
+// the Rys kernel in FP32, else the interpreter in FP32 with its own layout.
 cudaError_t launch_run32(const ClassRun &r, cudaStream_t st, const KArgs &a) {
     if (r.has32) return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, true, r.grid32, st, a);
+    if (r.rys32 && !a.W) {
+        KArgs ar = a;
+        ar.Y = r.ry32;
+        ar.rys_tab = r.rys_tab;
+        return rys_launch(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, true, r.grid_r32, st, ar);
+    }
     KArgs a32 = a;
     a32.C = r.dev32;
     return launch_hgp<float>(r.dev32, r.grid32, st, a32);
@@ -793,6 +813,8 @@ struct fjb_handle {
     std::map<std::tuple<int, int, int, int>, std::pair<int, int>> cfg;    // (threads, slots) overrides
     std::map<std::tuple<int, int, int, int>, std::pair<int, int>> cfg32;  // the FP32 interpreter's
     DevBuf<double> boys;
+    DevBuf<double> rys;  // the tabulated Rys rule (rys_rule.h)
+    bool use_rys = true;  // the Rys kernel takes the classes it covers (fjb_set_rys)
     DevBuf<int> sh_off, sh_nc;
     // plan
     bool planned = false;
@@ -1098,6 +1120,14 @@ int append_shells(fjb_handle *h, const fjb_basis *b, int max_l) {
 
 // Device staging common to every handle: the Boys table, shell offsets and
 // sizes, the build events.
+// The Rys rule's table, built once per process (rys_table.cpp).
+const std::vector<double> &rys_table_cached() {
+    static std::once_flag once;
+    static std::vector<double> t;
+    std::call_once(once, [] { t = rys_table(); });
+    return t;
+}
+
 int finish_create(std::unique_ptr<fjb_handle> &h, fjb_handle **out) {
     const int device = h->device;
     if (device < 0) {  // host-only handle: plans and exports, no builds
@@ -1107,6 +1137,7 @@ int finish_create(std::unique_ptr<fjb_handle> &h, fjb_handle **out) {
     if (cudaSetDevice(device) != cudaSuccess) return fail(nullptr, FJB_E_CUDA, "cudaSetDevice failed");
     try {
         h->boys.upload(boys_table());
+        h->rys.upload(rys_table_cached());
         std::vector<int> off(h->basis.offsets), nc;
         for (auto &s : h->basis.shells) nc.push_back((s.l + 1) * (s.l + 2) / 2);
         h->sh_off.upload(off);
@@ -1280,6 +1311,11 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
                 run.dev32 = ce.dev(deg.first, deg.second, ov32->second.first, ov32->second.second, 4);
             run.compiled = compiled_available(la, lb, lc, ld, false) && (th == 0 || th == 1);
             run.has32 = compiled_available(la, lb, lc, ld, true);
+            run.rys_tab = h->rys.p;
+            if (h->use_rys && !run.compiled && rys_available(la, lb, lc, ld, false))
+                run.rys64 = rys_layout(la, lb, lc, ld, deg.first, deg.second, false, kSmemBudgetDoubles, &run.ry64);
+            if (h->use_rys && !run.has32 && rys_available(la, lb, lc, ld, true))
+                run.rys32 = rys_layout(la, lb, lc, ld, deg.first, deg.second, true, kSmemBudgetDoubles, &run.ry32);
             run.unit0 = kv.second.first;
             run.n_units = kv.second.second;
             h->runs.push_back(run);
@@ -1303,6 +1339,12 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     for (auto &r : h->runs) {
         r.grid = run_grid(r);
         r.grid32 = run_grid32(r);
+        const auto rgrid = [&](bool fp32, const RysDev &d) {
+            const int per_sm = std::max(1, rys_blocks_per_sm(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, fp32, d));
+            return std::max(1, std::min(r.n_units, per_sm * sm_count()));
+        };
+        if (r.rys64) r.grid_r64 = rgrid(false, r.ry64);
+        if (r.rys32) r.grid_r32 = rgrid(true, r.ry32);
     }
     h->free_class_events();
     for (size_t i = 0; i < h->runs.size(); ++i) {
@@ -1996,6 +2038,28 @@ int fjb_set_class_config(fjb_handle *h, int la, int lb, int lc, int ld, int thre
             return fail(h, FJB_E_LIMIT, e.what());
         }
     }
+    return FJB_OK;
+}
+
+int fjb_set_rys(fjb_handle *h, int enable) {
+    if (!h) return fail(h, FJB_E_ARG, "null handle");
+    h->use_rys = enable != 0;
+    if (h->device < 0) return FJB_OK;
+    cudaSetDevice(h->device);
+    for (auto &r : h->runs) {
+        const int la = r.dev.la, lb = r.dev.lb, lc = r.dev.lc, ld = r.dev.ld;
+        r.rys64 = h->use_rys && !r.compiled && rys_available(la, lb, lc, ld, false) &&
+                  rys_layout(la, lb, lc, ld, r.max_kab, r.max_kcd, false, kSmemBudgetDoubles, &r.ry64);
+        r.rys32 = h->use_rys && !r.has32 && rys_available(la, lb, lc, ld, true) &&
+                  rys_layout(la, lb, lc, ld, r.max_kab, r.max_kcd, true, kSmemBudgetDoubles, &r.ry32);
+        const auto rgrid = [&](bool fp32, const RysDev &d) {
+            const int per_sm = std::max(1, rys_blocks_per_sm(la, lb, lc, ld, fp32, d));
+            return std::max(1, std::min(r.n_units, per_sm * sm_count()));
+        };
+        if (r.rys64) r.grid_r64 = rgrid(false, r.ry64);
+        if (r.rys32) r.grid_r32 = rgrid(true, r.ry32);
+    }
+    h->drop_graph();
     return FJB_OK;
 }
 

@@ -99,4 +99,14 @@ struct ClassDev {
     int vregion;      // doubles in the V region (also holds X and Y)
 };
 
+// The Rys kernel's launch configuration and shared-memory carve-up (offsets
+// in doubles), chosen on the host per class and precision (rys_fock.cu).
+struct RysDev {
+    int threads;   // CTA width
+    int group;     // kets per group (G)
+    int chunk;     // primitive quartets per table chunk (P)
+    int kab, kcd;  // staged primitive-pair capacity of a bra and of a ket
+    int sm_braP, sm_cb, sm_Dab, sm_Jab, sm_ketP, sm_ck, sm_Dk, sm_tab, sm_X, sm_total;
+};
+
 }  // namespace fjb

@@ -47,6 +47,9 @@ struct KArgs {
     const int64_t *w_base;   // per launch: its first slot in W
     double *wab;             // per unit: the bra block's partial sums
     const int64_t *wab_off;  // per unit of this run: its offset in wab
+    // the Rys kernel (rys_fock.cuh): its layout and the tabulated rule
+    RysDev Y;
+    const double *rys_tab;
 };
 
 // A quartet's first ket-block slot (block element 0) in the atomics-free

@@ -289,6 +289,11 @@ class FockEngine:
                       C.c_void_p(st.cuda_stream)), self._h)
         return tuple(out)
 
+    def set_rys(self, enable: bool = True) -> None:
+        """Run the large classes on the Rys kernel (the default) or, with
+        False, on the HGP shared-memory interpreter (fjb_set_rys)."""
+        _lib.check(self._L.fjb_set_rys(self._h, int(bool(enable))), self._h)
+
     def build_host(self, D, *, precision: int = _lib.FJB_FP64, threshold: float = 0.0, out=None):
         """Host build through the C ABI's host-buffer entry point: numpy in,
         (J, K, G) numpy out -- into `out`, three C-contiguous float64 n x n
