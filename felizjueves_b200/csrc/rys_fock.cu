@@ -14,17 +14,21 @@ int dd(long n) { return (int)((n + 1) & ~1L); }
 template <int LA, int LB, int LC, int LD>
 bool layout_one(int max_kab, int max_kcd, int rsize, int budget, RysDev *o) {
     using S = rys::Shape<LA, LB, LC, LD>;
+    const int minb = rsize == 8 ? S::template minb<double>() : S::template minb<float>();
+    budget = std::min(budget, rys::rys_smem_budget(minb));
+    const int nt = S::nt();
     *o = RysDev{};
-    o->threads = kRysThreads;
+    o->threads = nt;
     o->kab = max_kab;
     o->kcd = max_kcd;
     const int K = max_kab * max_kcd;
-    for (int G = std::min(kKetChunk, std::max(1, kRysThreads / S::NBF)); G >= 1; --G) {
+    for (int G = std::min(kKetChunk, std::max(1, nt / S::NBF)); G >= 1; --G) {
         const int fixed = dd(kPrimWords * max_kab) + rd(S::NCB, rsize) + 2 * dd(S::NAB) +
                           dd((long)G * kPrimWords * max_kcd) + rd((long)G * S::NCK, rsize) + dd((long)G * S::N5) +
                           rd((long)G * S::NAB * S::XS, rsize);
         for (int P = K; P >= 1; --P) {
-            const int tabs = rd(std::max((long)G * P * S::NR * 3 * S::TS, (long)G * S::NAB * S::YS), rsize);
+            const int tsp = rsize == 8 ? S::template tsp<double>() : S::template tsp<float>();
+            const int tabs = rd(std::max((long)G * P * S::NR * 3 * tsp, (long)G * S::NAB * S::YS), rsize);
             if (fixed + tabs > budget) continue;
             o->group = G;
             o->chunk = P;

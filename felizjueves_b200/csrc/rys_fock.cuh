@@ -60,7 +60,6 @@
 
 namespace fjb {
 
-constexpr int kRysThreads = 256;  // the Rys kernel's CTA width
 
 // host side (rys_fock.cu)
 bool rys_available(int la, int lb, int lc, int ld, bool fp32);
@@ -142,6 +141,16 @@ struct Shape {
     static constexpr int E = LA + LB, F = LC + LD;
     static constexpr int NR = (E + F) / 2 + 1;  // Rys roots
     static constexpr int TS = (E + 1) * (F + 1);  // one axis' 2D table
+    // the tables as stored: per axis F+1 rows (ket index k), each the E+1
+    // values of the bra index padded to whole 16-byte vectors
+    template <typename R>
+    __host__ __device__ static constexpr int rp() {
+        return ((E + 1) * (int)sizeof(R) + 15) / 16 * 16 / (int)sizeof(R);
+    }
+    template <typename R>
+    __host__ __device__ static constexpr int tsp() {
+        return (F + 1) * rp<R>();
+    }
     static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     static constexpr int NAB = NA * NB, NCD = NC * ND;
     static constexpr int NBE = nrange(LA, E), NBF = nrange(LC, F);
@@ -149,7 +158,25 @@ struct Shape {
     static constexpr int XS = NBF | 1;  // X row stride, odd: rows start in different banks
     static constexpr int YS = NCD | 1;
     static constexpr int N5 = NCD + NA * NC + NA * ND + NB * NC + NB * ND;
+    // CTA width: 128 threads (a thread per (ket, f) item, G = 128 / NBF kets
+    // a group), 256 for the ff kets (NBF = 74) so that a group holds more
+    // than one ket
+    __host__ __device__ static constexpr int nt() { return NBF > 64 ? 256 : 128; }
+    // CTAs an SM holds: 512 threads of 128 registers, unless the bra column
+    // the boundary phase keeps in registers is too long to fit in those
+    // (df and ff bras in FP64, the ff bra in FP32): then half as many
+    template <typename R>
+    __host__ __device__ static constexpr int minb() {
+        return (nt() == 256 ? 2 : 4) / (NBE > (sizeof(R) == 8 ? 34 : 52) ? 2 : 1);
+    }
 };
+
+// Dynamic shared memory of one CTA (doubles) when `minb` CTAs share an SM:
+// its share of the SM's 228 KiB less the 1 KiB the hardware reserves per CTA
+// and the kernel's static arrays (below 3 KiB).
+__host__ __device__ constexpr int rys_smem_budget(int minb) {
+    return minb <= 1 ? kSmemBudgetDoubles : (233472 / minb - 1024 - 3072) / 8;
+}
 
 // One root of the n-point rule at T (rys_rule, one root's two series).
 template <int N>
@@ -204,6 +231,17 @@ __device__ __forceinline__ R hrr_coef(int idx, const double *sep) {
 }
 
 
+// N values of R from a 16-byte aligned shared-memory row, as 16-byte loads.
+template <typename R, int N>
+__device__ __forceinline__ void ld_row(const R *p, R *out) {
+    static_assert(N * sizeof(R) % 16 == 0, "whole 16-byte vectors");
+#pragma unroll
+    for (int v = 0; v < N * (int)sizeof(R) / 16; ++v) {
+        const float4 t = reinterpret_cast<const float4 *>(p)[v];
+        memcpy(out + v * (16 / (int)sizeof(R)), &t, 16);
+    }
+}
+
 // The position of Cartesian index t of cartesians-range LO..HI as (x, y, z),
 // for a run-time index (the thread's own f).
 template <int LO, int HI>
@@ -230,9 +268,11 @@ __device__ __forceinline__ void cart_of(int t, int *x, int *y, int *z) {
 }  // namespace rys
 
 template <int LA, int LB, int LC, int LD, typename R, int NT>
-__global__ void __launch_bounds__(NT, 1) rys_fock_kernel(const KArgs A) {
+__global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb<R>()))
+    rys_fock_kernel(const KArgs A) {
     using S = rys::Shape<LA, LB, LC, LD>;
-    constexpr int E = S::E, F = S::F, NR = S::NR, TS = S::TS;
+    constexpr int E = S::E, F = S::F, NR = S::NR;
+    constexpr int RP = S::template rp<R>(), TSP = S::template tsp<R>();
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NAB = S::NAB, NCD = S::NCD;
     constexpr int NBE = S::NBE, NBF = S::NBF, NCB = S::NCB, NCK = S::NCK, XS = S::XS, YS = S::YS;
     constexpr int N5 = S::N5;
@@ -249,6 +289,7 @@ __global__ void __launch_bounds__(NT, 1) rys_fock_kernel(const KArgs A) {
 
     extern __shared__ __align__(16) double sm[];
     __shared__ int s_ket[kKetChunk];
+    __shared__ PairRec s_pair[kKetChunk];  // the unit's computed kets, in ket order
     __shared__ int s_oc[kKetChunk], s_od[kKetChunk];
     __shared__ double s_deg[kKetChunk];
     __shared__ int s_n;
@@ -292,7 +333,11 @@ __global__ void __launch_bounds__(NT, 1) rys_fock_kernel(const KArgs A) {
                 on = !skip6(A.Dsh, A.n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G, A.tau);
             }
             const unsigned m = __ballot_sync(0xffffffffu, on);
-            if (on) s_ket[__popc(m & ((1u << tid) - 1u))] = ik;
+            if (on) {
+                const int at = __popc(m & ((1u << tid) - 1u));
+                s_ket[at] = ik;
+                s_pair[at] = A.pairs[LR.ket_pair0 + ik];
+            }
             if (tid == 0) s_n = __popc(m);
         }
         __syncthreads();
@@ -306,18 +351,15 @@ __global__ void __launch_bounds__(NT, 1) rys_fock_kernel(const KArgs A) {
             // -- the group's kets: primitive pairs, HRR coefficients, densities
             for (int i = tid; i < ng * kcd * kPrimWords; i += NT) {
                 const int g = i / (kcd * kPrimWords), r = i - g * (kcd * kPrimWords);
-                const PairRec ket = A.pairs[LR.ket_pair0 + s_ket[g0 + g]];
-                ketP[i] = reinterpret_cast<const double *>(A.prims + ket.prim0)[r];
+                ketP[i] = reinterpret_cast<const double *>(A.prims + s_pair[g0 + g].prim0)[r];
             }
             for (int i = tid; i < ng * NCK; i += NT) {
                 const int g = i / NCK;
-                const PairRec ket = A.pairs[LR.ket_pair0 + s_ket[g0 + g]];
-                ck[i] = rys::hrr_coef<LD, R>(i - g * NCK, ket.AB);
+                ck[i] = rys::hrr_coef<LD, R>(i - g * NCK, s_pair[g0 + g].AB);
             }
             for (int i = tid; i < ng * N5; i += NT) {
                 const int g = i / N5, o = i - g * N5;
-                const PairRec ket = A.pairs[LR.ket_pair0 + s_ket[g0 + g]];
-                const int oc = ket.ao_a, od = ket.ao_b;
+                const int oc = s_pair[g0 + g].ao_a, od = s_pair[g0 + g].ao_b;
                 size_t at;
                 if (o < NCD) {
                     at = (size_t)(oc + o / ND) * n_ao + od + o % ND;
@@ -338,7 +380,7 @@ __global__ void __launch_bounds__(NT, 1) rys_fock_kernel(const KArgs A) {
             }
             if (tid < ng) {
                 const int ik = s_ket[g0 + tid];
-                const PairRec ket = A.pairs[LR.ket_pair0 + ik];
+                const PairRec &ket = s_pair[g0 + tid];
                 s_oc[tid] = ket.ao_a;
                 s_od[tid] = ket.ao_b;
                 s_deg[tid] = bra_deg * (ket.a == ket.b ? 0.5 : 1.0) * ((LR.diag && ik == U.ib) ? 0.5 : 1.0);
@@ -369,7 +411,7 @@ __global__ void __launch_bounds__(NT, 1) rys_fock_kernel(const KArgs A) {
                     rys::rule_root<NR>(r, T, A.rys_tab, &x, &w);
                     const double seedw = pb[7] * pk[7] * kTwoOverSqrtPi * sqrt(rho) * w;
                     const double b00 = 0.5 * inv * x, b10 = pb[8] * (1.0 - qi * x), b01 = pk[8] * (1.0 - pi * x);
-                    R *out = tab + ((size_t)(g * P + tl) * NR + r) * (3 * TS);
+                    R *out = tab + ((size_t)(g * P + tl) * NR + r) * (3 * TSP);
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         const double c00 = pb[3 + d] - qi * PQ[d] * x, c00p = pk[3 + d] + pi * PQ[d] * x;
@@ -390,23 +432,20 @@ __global__ void __launch_bounds__(NT, 1) rys_fock_kernel(const KArgs A) {
 #pragma unroll
                         for (int i = 0; i <= E; ++i)
 #pragma unroll
-                            for (int k = 0; k <= F; ++k) out[d * TS + i * (F + 1) + k] = (R)I[i][k];
+                            for (int k = 0; k <= F; ++k) out[d * TSP + k * RP + i] = (R)I[i][k];
                     }
                 }
                 __syncthreads();
                 if (item) {
                     for (int tl = 0; tl < np; ++tl) {
-                        const R *base = tab + (size_t)(gme * P + tl) * NR * (3 * TS);
+                        const R *base = tab + (size_t)(gme * P + tl) * NR * (3 * TSP);
 #pragma unroll
                         for (int r = 0; r < NR; ++r) {
-                            const R *Ix = base + r * (3 * TS), *Iy = Ix + TS, *Iz = Iy + TS;
-                            R ix[E + 1], iy[E + 1], iz[E + 1];
-#pragma unroll
-                            for (int i = 0; i <= E; ++i) {
-                                ix[i] = Ix[i * (F + 1) + fx];
-                                iy[i] = Iy[i * (F + 1) + fy];
-                                iz[i] = Iz[i * (F + 1) + fz];
-                            }
+                            const R *Ix = base + r * (3 * TSP), *Iy = Ix + TSP, *Iz = Iy + TSP;
+                            R ix[RP], iy[RP], iz[RP];
+                            rys::ld_row<R, RP>(Ix + fx * RP, ix);
+                            rys::ld_row<R, RP>(Iy + fy * RP, iy);
+                            rys::ld_row<R, RP>(Iz + fz * RP, iz);
                             R pxy[E + 1][E + 1];
 #pragma unroll
                             for (int a = 0; a <= E; ++a)
@@ -440,29 +479,40 @@ __global__ void __launch_bounds__(NT, 1) rys_fock_kernel(const KArgs A) {
             }
             __syncthreads();
 
-            // -- D: the ket HRR, Y[g][ab][cd]
-            for (int it = tid; it < ng * NAB; it += NT) {
-                const int g = it / NAB;
-                const R *xr = X + (size_t)it * XS;
-                R *yr = Ym + (size_t)it * YS;
+            // -- D: the ket HRR, Y[g][ab][cd], one (ket, ab, c) per thread
+            for (int it = tid; it < ng * NAB * NC; it += NT) {
+                const int row = it / NC, c = it - row * NC, g = row / NAB;
+                const R *xr = X + (size_t)row * XS;
+                R *yr = Ym + (size_t)row * YS + c * ND;
                 const R *ckg = ck + g * NCK;
+                int cx = 0, cy = 0, cz = 0;
 #pragma unroll
-                for (int c = 0; c < NC; ++c) {
-                    R xk[rys::CSet<0, LD>::N];
-#pragma unroll
-                    for (int k = 0; k < rys::CSet<0, LD>::N; ++k) xk[k] = xr[fs.idx[cc.x[c] + ks.x[k]][cc.y[c] + ks.y[k]][cc.z[c] + ks.z[k]]];
-#pragma unroll
-                    for (int d = 0; d < ND; ++d) {
-                        R v = (R)0;
-                        int ci = hd.off[d];
-#pragma unroll
-                        for (int kx = 0; kx <= cds.x[d]; ++kx)
-#pragma unroll
-                            for (int ky = 0; ky <= cds.y[d]; ++ky)
-#pragma unroll
-                                for (int kz = 0; kz <= cds.z[d]; ++kz, ++ci) v += ckg[ci] * xk[ks.idx[kx][ky][kz]];
-                        yr[c * ND + d] = v;
+                for (int j = 0; j < NC; ++j)
+                    if (j == c) {
+                        cx = cc.x[j];
+                        cy = cc.y[j];
+                        cz = cc.z[j];
                     }
+                R xk[rys::CSet<0, LD>::N];
+#pragma unroll
+                for (int k = 0; k < rys::CSet<0, LD>::N; ++k) {
+                    // f index of c + k: the level offset of |c + k| plus the
+                    // position inside cartesians(|c + k|)
+                    const int ix = cx + ks.x[k], iy = cy + ks.y[k], l = LC + ks.x[k] + ks.y[k] + ks.z[k];
+                    const int f = rys::nrange(LC, l - 1) + (l - ix) * (l - ix + 1) / 2 + (l - ix - iy);
+                    xk[k] = xr[f];
+                }
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    R v = (R)0;
+                    int ci = hd.off[d];
+#pragma unroll
+                    for (int kx = 0; kx <= cds.x[d]; ++kx)
+#pragma unroll
+                        for (int ky = 0; ky <= cds.y[d]; ++ky)
+#pragma unroll
+                            for (int kz = 0; kz <= cds.z[d]; ++kz, ++ci) v += ckg[ci] * xk[ks.idx[kx][ky][kz]];
+                    yr[d] = v;
                 }
             }
             __syncthreads();
@@ -540,6 +590,7 @@ __global__ void __launch_bounds__(NT, 1) rys_fock_kernel(const KArgs A) {
 // (instantiated per precision in rys_fock64.cu and rys_fock32.cu).
 template <int LA, int LB, int LC, int LD, typename R>
 struct RysOne {
+    static constexpr int kRysThreads = rys::Shape<LA, LB, LC, LD>::nt();
     static void attr() {
         static bool done = false;  // per kernel and process: the largest carve-up any layout takes
         if (done) return;
