@@ -774,13 +774,13 @@ int run_grid(const ClassRun &r);
 // The FP64 path of a class run: its register kernel, else the Rys kernel,
 // else the interpreter (which alone serves the atomics-free build's slots).
 cudaError_t launch_run(const ClassRun &r, cudaStream_t st, const KArgs &a) {
-    if (r.compiled) return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, false, r.grid, st, a);
     if (r.rys64 && !a.W) {
         KArgs ar = a;
         ar.Y = r.ry64;
         ar.rys_tab = r.rys_tab;
         return rys_launch(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, false, r.grid_r64, st, ar);
     }
+    if (r.compiled) return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, false, r.grid, st, a);
     return launch_hgp<double>(r.dev, r.grid, st, a);
 }
 
@@ -814,7 +814,7 @@ struct fjb_handle {
     std::map<std::tuple<int, int, int, int>, std::pair<int, int>> cfg32;  // the FP32 interpreter's
     DevBuf<double> boys;
     DevBuf<double> rys;  // the tabulated Rys rule (rys_rule.h)
-    bool use_rys = true;  // the Rys kernel takes the classes it covers (fjb_set_rys)
+    int use_rys = 1;  // which classes the Rys kernel takes (fjb_set_rys)
     DevBuf<int> sh_off, sh_nc;
     // plan
     bool planned = false;
@@ -1120,6 +1120,25 @@ int append_shells(fjb_handle *h, const fjb_basis *b, int max_l) {
 
 // Device staging common to every handle: the Boys table, shell offsets and
 // sizes, the build events.
+// Which kernels a class run's units take from the Rys kernel: mode 0 none;
+// 1 the classes without an FP64 register body, and those with one where the
+// Rys kernel is the faster (rys_preferred); 2 every class it has.  FP32:
+// the classes without an FP32 register body (modes 1 and 2).
+void choose_rys(int mode, ClassRun &r) {
+    const int la = r.dev.la, lb = r.dev.lb, lc = r.dev.lc, ld = r.dev.ld;
+    const bool take64 = mode >= 1 && ((!r.compiled && rys_available(la, lb, lc, ld, false)) ||
+                                      (rys_extra(la, lb, lc, ld) && (mode == 2 || rys_preferred(la, lb, lc, ld))));
+    r.rys64 = take64 && rys_layout(la, lb, lc, ld, r.max_kab, r.max_kcd, false, kSmemBudgetDoubles, &r.ry64);
+    r.rys32 = mode >= 1 && !r.has32 && rys_available(la, lb, lc, ld, true) &&
+              rys_layout(la, lb, lc, ld, r.max_kab, r.max_kcd, true, kSmemBudgetDoubles, &r.ry32);
+    const auto rgrid = [&](bool fp32, const RysDev &d) {
+        const int per_sm = std::max(1, rys_blocks_per_sm(la, lb, lc, ld, fp32, d));
+        return std::max(1, std::min(r.n_units, per_sm * sm_count()));
+    };
+    if (r.rys64) r.grid_r64 = rgrid(false, r.ry64);
+    if (r.rys32) r.grid_r32 = rgrid(true, r.ry32);
+}
+
 // The Rys rule's table, built once per process (rys_table.cpp).
 const std::vector<double> &rys_table_cached() {
     static std::once_flag once;
@@ -1312,10 +1331,6 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
             run.compiled = compiled_available(la, lb, lc, ld, false) && (th == 0 || th == 1);
             run.has32 = compiled_available(la, lb, lc, ld, true);
             run.rys_tab = h->rys.p;
-            if (h->use_rys && !run.compiled && rys_available(la, lb, lc, ld, false))
-                run.rys64 = rys_layout(la, lb, lc, ld, deg.first, deg.second, false, kSmemBudgetDoubles, &run.ry64);
-            if (h->use_rys && !run.has32 && rys_available(la, lb, lc, ld, true))
-                run.rys32 = rys_layout(la, lb, lc, ld, deg.first, deg.second, true, kSmemBudgetDoubles, &run.ry32);
             run.unit0 = kv.second.first;
             run.n_units = kv.second.second;
             h->runs.push_back(run);
@@ -1339,12 +1354,7 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     for (auto &r : h->runs) {
         r.grid = run_grid(r);
         r.grid32 = run_grid32(r);
-        const auto rgrid = [&](bool fp32, const RysDev &d) {
-            const int per_sm = std::max(1, rys_blocks_per_sm(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, fp32, d));
-            return std::max(1, std::min(r.n_units, per_sm * sm_count()));
-        };
-        if (r.rys64) r.grid_r64 = rgrid(false, r.ry64);
-        if (r.rys32) r.grid_r32 = rgrid(true, r.ry32);
+        choose_rys(h->use_rys, r);
     }
     h->free_class_events();
     for (size_t i = 0; i < h->runs.size(); ++i) {
@@ -2041,24 +2051,13 @@ int fjb_set_class_config(fjb_handle *h, int la, int lb, int lc, int ld, int thre
     return FJB_OK;
 }
 
-int fjb_set_rys(fjb_handle *h, int enable) {
+int fjb_set_rys(fjb_handle *h, int mode) {
     if (!h) return fail(h, FJB_E_ARG, "null handle");
-    h->use_rys = enable != 0;
+    if (mode < 0 || mode > 2) return fail(h, FJB_E_ARG, "fjb_set_rys: mode is 0, 1 or 2");
+    h->use_rys = mode;
     if (h->device < 0) return FJB_OK;
     cudaSetDevice(h->device);
-    for (auto &r : h->runs) {
-        const int la = r.dev.la, lb = r.dev.lb, lc = r.dev.lc, ld = r.dev.ld;
-        r.rys64 = h->use_rys && !r.compiled && rys_available(la, lb, lc, ld, false) &&
-                  rys_layout(la, lb, lc, ld, r.max_kab, r.max_kcd, false, kSmemBudgetDoubles, &r.ry64);
-        r.rys32 = h->use_rys && !r.has32 && rys_available(la, lb, lc, ld, true) &&
-                  rys_layout(la, lb, lc, ld, r.max_kab, r.max_kcd, true, kSmemBudgetDoubles, &r.ry32);
-        const auto rgrid = [&](bool fp32, const RysDev &d) {
-            const int per_sm = std::max(1, rys_blocks_per_sm(la, lb, lc, ld, fp32, d));
-            return std::max(1, std::min(r.n_units, per_sm * sm_count()));
-        };
-        if (r.rys64) r.grid_r64 = rgrid(false, r.ry64);
-        if (r.rys32) r.grid_r32 = rgrid(true, r.ry32);
-    }
+    for (auto &r : h->runs) choose_rys(mode, r);
     h->drop_graph();
     return FJB_OK;
 }

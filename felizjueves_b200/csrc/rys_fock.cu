@@ -68,11 +68,28 @@ bool rys_available(int la, int lb, int lc, int ld, bool fp32) {
     return false;
 }
 
+bool rys_extra(int la, int lb, int lc, int ld) {
+#define FJB_X(a, b, c, d) \
+    if (la == a && lb == b && lc == c && ld == d) return true;
+    FJB_RYS64_EXTRA_CLASSES(FJB_X)
+#undef FJB_X
+    return false;
+}
+
+bool rys_preferred(int la, int lb, int lc, int ld) {
+    (void)la;
+    (void)lb;
+    (void)lc;
+    (void)ld;
+    return false;
+}
+
 bool rys_layout(int la, int lb, int lc, int ld, int max_kab, int max_kcd, bool fp32, int budget, RysDev *out) {
     const int rsize = fp32 ? 4 : 8;
 #define FJB_X(a, b, c, d) \
     if (la == a && lb == b && lc == c && ld == d) return layout_one<a, b, c, d>(max_kab, max_kcd, rsize, budget, out);
     FJB_RYS64_CLASSES(FJB_X)
+    FJB_RYS64_EXTRA_CLASSES(FJB_X)
 #undef FJB_X
     return false;
 }

@@ -52,6 +52,11 @@
     X(1, 1, 2, 3) X(1, 1, 3, 3) X(1, 2, 1, 2) X(1, 2, 1, 3) X(1, 2, 2, 2) X(1, 2, 2, 3) X(1, 2, 3, 3)    \
     X(1, 3, 1, 3) X(1, 3, 2, 2) X(1, 3, 2, 3) X(1, 3, 3, 3) X(2, 2, 2, 2) X(2, 2, 2, 3) X(2, 2, 3, 3)    \
     X(2, 3, 2, 3) X(2, 3, 3, 3) X(3, 3, 3, 3)
+// Classes the register kernel also has in FP64, where the Rys kernel can
+// take them instead (fjb_set_rys mode 2, and the classes rys_preferred names)
+#define FJB_RYS64_EXTRA_CLASSES(X)                                                                      \
+    X(0, 0, 0, 1) X(0, 1, 0, 1) X(0, 1, 0, 2) X(0, 1, 0, 3) X(0, 1, 1, 1) X(0, 1, 1, 2) X(0, 1, 1, 3)    \
+    X(0, 1, 2, 2) X(0, 2, 0, 3) X(0, 2, 1, 1) X(0, 2, 1, 2) X(0, 3, 1, 1) X(1, 1, 1, 2)
 #define FJB_RYS32_CLASSES(X)                                                                            \
     X(0, 2, 2, 3) X(0, 2, 3, 3) X(0, 3, 1, 3) X(0, 3, 2, 2) X(0, 3, 2, 3) X(0, 3, 3, 3) X(1, 1, 2, 3)    \
     X(1, 1, 3, 3) X(1, 2, 1, 3) X(1, 2, 2, 2) X(1, 2, 2, 3) X(1, 2, 3, 3) X(1, 3, 1, 3) X(1, 3, 2, 2)    \
@@ -63,6 +68,10 @@ namespace fjb {
 
 // host side (rys_fock.cu)
 bool rys_available(int la, int lb, int lc, int ld, bool fp32);
+// FP64 classes that have a register-path body too: whether the Rys kernel
+// is the faster of the two (measured on the 64-atom cluster)
+bool rys_extra(int la, int lb, int lc, int ld);
+bool rys_preferred(int la, int lb, int lc, int ld);
 // The carve-up of a class's kernel for bra and ket degrees up to max_kab,
 // max_kcd within `budget` doubles of shared memory: kets per group G from
 // the CTA width, then the largest table chunk that fits.  false if none.

@@ -289,10 +289,11 @@ class FockEngine:
                       C.c_void_p(st.cuda_stream)), self._h)
         return tuple(out)
 
-    def set_rys(self, enable: bool = True) -> None:
-        """Run the large classes on the Rys kernel (the default) or, with
-        False, on the HGP shared-memory interpreter (fjb_set_rys)."""
-        _lib.check(self._L.fjb_set_rys(self._h, int(bool(enable))), self._h)
+    def set_rys(self, mode=1) -> None:
+        """Which classes the Rys kernel takes (fjb_set_rys): 1 or True (the
+        default) the large classes, 0 or False none (the HGP interpreter),
+        2 every class it has."""
+        _lib.check(self._L.fjb_set_rys(self._h, int(mode)), self._h)
 
     def build_host(self, D, *, precision: int = _lib.FJB_FP64, threshold: float = 0.0, out=None):
         """Host build through the C ABI's host-buffer entry point: numpy in,

@@ -324,15 +324,17 @@ int fjb_set_class_config(fjb_handle *h, int la, int lb, int lc, int ld, int thre
  * and slots 0 restore the FP64 configuration's FP32 twin. */
 int fjb_set_class_config32(fjb_handle *h, int la, int lb, int lc, int ld, int threads, int slots);
 
-/* The engine of the large classes: 1 (the default) runs every class the
- * Rys kernel covers on it -- the Rys quadrature in place of the HGP
- * vertical recurrence, the reference's third engine (rys/roots.py,
- * eri/fock/kernel_frys.py:194) feeding the same HRR and digest -- in FP64
- * and for the routed build's FP32 units; 0 runs them on the HGP
- * shared-memory interpreter.  Applies to the current plan and later ones.
- * The atomics-free build (FJB_FP64_SCATTER) and the ERI tap always use the
- * interpreter. */
-int fjb_set_rys(fjb_handle *h, int enable);
+/* Which classes run on the Rys kernel -- the Rys quadrature in place of the
+ * HGP vertical recurrence, the reference's third engine (rys/roots.py,
+ * eri/fock/kernel_frys.py:194), feeding the same HRR and digest.  mode 1
+ * (the default): every class without an FP64 register body, and those with
+ * one where the Rys kernel measured faster; plus, for the routed build's
+ * FP32 units, every class without an FP32 register body.  mode 0: none (the
+ * HGP shared-memory interpreter takes them).  mode 2: every class the Rys
+ * kernel has.  Applies to the current plan and later ones.  The
+ * atomics-free build (FJB_FP64_SCATTER) and the ERI tap keep the HGP
+ * kernels. */
+int fjb_set_rys(fjb_handle *h, int mode);
 
 /* fjb_fock_build without any device allocation (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc while they run the
