@@ -321,13 +321,18 @@ def main():
     if a.precision == "routed":
         ms, ck, nl, cs_r, ls_r, Gr = timed(_lib.FJB_ROUTED, a.threshold)
         n32, n64 = route_counts(eng)
-        router_info = dict(router_info or {"kind": "bound"}, fp32_units=n32, fp64_units=n64)
+        est, rerouted = eng.route_check()
+        router_info = dict(router_info or {"kind": "bound"}, fp32_units=n32, fp64_units=n64,
+                           budget_check={"budget": 1e-8, "sample_stride": 16, "estimate": est,
+                                         "rerouted_to_fp64": rerouted})
         if a.budget_threshold > 0:
             msb, _, _, _, _, Gb = timed(_lib.FJB_ROUTED, a.budget_threshold)
+            estb, rrb = eng.route_check()
             budget = {"threshold": a.budget_threshold, "ms_per_step": round(msb, 3),
                       "speedup_vs_fp64": round(ms64 / msb, 4),
                       "max_abs_dG_vs_fp64": float((Gb - G64).abs().max()),
-                      "fp32_units": route_counts(eng)[0]}
+                      "fp32_units": route_counts(eng)[0],
+                      "budget_check": {"estimate": estb, "rerouted_to_fp64": rrb}}
         dG = float((Gr - G64).abs().max())
         prec = _lib.FJB_ROUTED
     else:
@@ -396,7 +401,9 @@ def main():
                    "tau": w.tau, "quartets_launched": launched, "quartets_computed": computed,
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                    "l2": "working set > 126 MB L2 (6 x 31.5 MB matrices + pair records); no flush"},
-        "roofline": {"bound": "fp64", "kernel": "hgp_fock_kernel class (%d%d|%d%d)" % tcls,
+        "roofline": {"bound": "fp64",
+                     "kernel": "%s class (%d%d|%d%d)" % (("hgp_fock_kernel", "hgp_compiled_kernel",
+                                                          "rys_fock_kernel")[top.get("engine", 0)], *tcls),
                      "achieved": round(ach, 3), "peak": round(peak64, 3), "unit": "TFLOP/s",
                      "frac": round(ach / peak64, 4) if peak64 else None, "traffic": None,
                      "peak_source": "measured: fjb_fma_probe FP64 FMA chains on this GPU "

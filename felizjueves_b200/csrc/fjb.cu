@@ -66,15 +66,69 @@ __global__ void density_blocks_kernel(const double *__restrict__ D, int n_ao, in
 }
 
 __global__ void close_kernel(const double *__restrict__ Jp, const double *__restrict__ Kp, int n,
-                             double *J, double *K, double *G) {
+                             double *J, double *K, double *G, const double *__restrict__ Jp2 = nullptr,
+                             const double *__restrict__ Kp2 = nullptr) {
     size_t ij = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (ij >= (size_t)n * n) return;
     size_t i = ij / n, j = ij % n, ji = j * n + i;
     double jv = Jp[ij] + Jp[ji];
     double kv = Kp[ij] + Kp[ji];
+    if (Jp2) {  // the routed build's FP32-queue accumulators
+        jv += Jp2[ij] + Jp2[ji];
+        kv += Kp2[ij] + Kp2[ji];
+    }
     if (J) J[ij] = jv;
     if (K) K[ij] = kv;
     if (G) G[ij] = jv - 0.5 * kv;
+}
+
+// The routed build's budget check.  The sampled FP32 units were built twice
+// more, in FP64 into (EJ64, EK64) and in FP32 into (EJ32, EK32): their G
+// difference, closed as the build closes G, is the sample's own FP32 error.
+// Its largest element goes to *max_bits (a non-negative double's bits order
+// like the double, so an integer atomicMax takes the maximum).
+__global__ void route_check_kernel(const double *__restrict__ EJ64, const double *__restrict__ EK64,
+                                   const double *__restrict__ EJ32, const double *__restrict__ EK32, int n,
+                                   unsigned long long *max_bits) {
+    double m = 0.0;
+    for (size_t ij = (size_t)blockIdx.x * blockDim.x + threadIdx.x; ij < (size_t)n * n;
+         ij += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = ij / n, j = ij % n, ji = j * n + i;
+        const double dj = (EJ64[ij] - EJ32[ij]) + (EJ64[ji] - EJ32[ji]);
+        const double dk = (EK64[ij] - EK32[ij]) + (EK64[ji] - EK32[ji]);
+        m = fmax(m, fabs(dj - 0.5 * dk));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(max_bits, (unsigned long long)__double_as_longlong(m));
+}
+
+// The decision: the whole FP32 queue's error is estimated as sqrt(stride)
+// x the sample's (every stride-th FP32 unit was sampled; units' FP32
+// rounding errors are independent, so a sum over stride times the units
+// grows like its square root -- on the 64-atom cluster the whole queue's
+// max|dG| was 1.25 x the sample's at stride 16, under the sqrt(16) = 4 the
+// estimate allows).  Over budget: *flag = 1 and
+// every class's conditional count (counts[4 ri + 3]) becomes its FP32 queue
+// length, so the conditional FP64 launches re-run the whole FP32 queue;
+// else those counts are 0 and the launches do nothing.
+__global__ void route_decide_kernel(const unsigned long long *max_bits, double stride, double budget,
+                                    int *counts, int n_runs, int *flag, double *estimate) {
+    const double est = sqrt(stride) * __longlong_as_double((long long)*max_bits);
+    const int over = est > budget;
+    if (threadIdx.x == 0) {
+        *flag = over;
+        *estimate = est;
+    }
+    for (int r = threadIdx.x; r < n_runs; r += blockDim.x) counts[4 * r + 3] = over ? counts[4 * r] : 0;
+}
+
+__global__ void zero_if_kernel(double *a, double *b, size_t n, const int *flag) {
+    if (!*flag) return;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        a[i] = 0.0;
+        b[i] = 0.0;
+    }
 }
 
 // The atomics-free build (scatter.h).  A bra segment is one bra pair of one
@@ -153,7 +207,8 @@ __global__ void screen_mask_kernel(const Unit *units, int n_units, const LaunchR
 // no computed quartet to neither.  Skipping stays the six-block screen's.
 __global__ void route_units_kernel(const Unit *units, int unit0, int n_units, const LaunchRec *launches,
                                    const PairRec *pairs, const double *Dsh, int n_sh, double tau,
-                                   double thresh, int *list32, int *list64, int *counts) {
+                                   double thresh, int *list32, int *list64, int *counts, int stride,
+                                   int *list_s) {
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
@@ -172,10 +227,12 @@ __global__ void route_units_kernel(const Unit *units, int unit0, int n_units, co
         const bool any = __any_sync(0xffffffffu, active);
         const bool all_low = __all_sync(0xffffffffu, low);
         if (lane == 0 && any) {
-            if (all_low)
+            if (all_low) {
                 list32[atomicAdd(counts + 0, 1)] = i;
-            else
+                if (stride > 0 && i % stride == 0) list_s[atomicAdd(counts + 2, 1)] = i;
+            } else {
                 list64[atomicAdd(counts + 1, 1)] = i;
+            }
         }
     }
 }
@@ -195,7 +252,8 @@ constexpr double kRouterReach = 1e5;  // 10^kRouterMaxGap
 __global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units, const LaunchRec *launches,
                                        const PairRec *pairs, const PrimRec *prims, const double *Dsh, int n_sh,
                                        double tau, double thresh, const float *params, float log_thr, int la,
-                                       int lb, int lc, int ld, int *list32, int *list64, int *counts) {
+                                       int lb, int lc, int ld, int *list32, int *list64, int *counts,
+                                       int stride, int *list_s) {
     __shared__ float sp[kNParams];
     for (int i = threadIdx.x; i < kNParams; i += blockDim.x) sp[i] = params[i];
     __syncthreads();
@@ -233,10 +291,12 @@ __global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units
         }
         const bool all_low = __all_sync(0xffffffffu, low);
         if (lane == 0 && any) {
-            if (all_low)
+            if (all_low) {
                 list32[atomicAdd(counts + 0, 1)] = i;
-            else
+                if (stride > 0 && i % stride == 0) list_s[atomicAdd(counts + 2, 1)] = i;
+            } else {
                 list64[atomicAdd(counts + 1, 1)] = i;
+            }
         }
     }
 }
@@ -848,7 +908,16 @@ struct fjb_handle {
     int last_launches = 0;
     // measurement
     DevBuf<unsigned long long> computed;
-    DevBuf<int> route_list, route_counts;  // the router's per-class FP32 / FP64 queues
+    DevBuf<int> route_list, route_counts;  // the router's per-class FP32 / FP64 / sampled queues
+    // the routed build's budget check (fjb_set_route_check): the FP32 queue's
+    // own accumulators, the sample's FP64 and FP32 twins, the verdict
+    double check_budget = 1e-8;
+    int check_stride = 16;
+    DevBuf<double> Jp32, Kp32, EJ64, EK64, EJ32, EK32;
+    DevBuf<unsigned long long> check_max;
+    DevBuf<int> check_flag;
+    DevBuf<double> check_est;
+    bool last_checked = false;
     std::vector<fjb_launch_stat> lstat;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> cev;
     bool built = false;
@@ -1053,6 +1122,28 @@ int ensure_scatter(fjb_handle *h) {
         return fail(h, FJB_E_CUDA, e.what());
     }
     h->scatter_ready = true;
+    return FJB_OK;
+}
+
+// The budget check's buffers (six n_ao^2 arrays and the verdict), made on
+// the first routed build -- before a capture, by fjb_fock_build_graph.
+int ensure_check(fjb_handle *h) {
+    if (h->Jp32.n) return FJB_OK;
+    const size_t nn = (size_t)h->basis.n_ao * h->basis.n_ao;
+    try {
+        h->Jp32.alloc(nn);
+        h->Kp32.alloc(nn);
+        h->EJ64.alloc(nn);
+        h->EK64.alloc(nn);
+        h->EJ32.alloc(nn);
+        h->EK32.alloc(nn);
+        h->check_max.alloc(1);
+        h->check_flag.alloc(1);
+        h->check_est.alloc(1);
+    } catch (const std::exception &e) {
+        h->Jp32.reset();
+        return fail(h, FJB_E_CUDA, e.what());
+    }
     return FJB_OK;
 }
 
@@ -1373,8 +1464,12 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
             lc.push_back(s.ld);
         }
         h->launch_cls.upload(lc);
-        h->route_list.alloc(std::max<size_t>(1, 2 * h->units_host.size()));
-        h->route_counts.alloc(std::max<size_t>(1, 2 * h->runs.size()));
+        h->route_list.alloc(std::max<size_t>(1, 3 * h->units_host.size()));
+        h->route_counts.alloc(std::max<size_t>(1, 4 * h->runs.size()));
+        if (h->Jp32.n) {  // the budget check's buffers follow the plan's size
+            h->Jp32.reset();
+            if (int rc = ensure_check(h)) return rc;
+        }
     } catch (const std::exception &e) {
         return fail(h, FJB_E_CUDA, e.what());
     }
@@ -1504,7 +1599,16 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
     CUDA_OK(h, cudaMemsetAsync(h->computed.p, 0, h->computed.n * sizeof(unsigned long long), st));
     const bool routed = route > 0.0;
     h->last_routed = routed;
+    const bool check = routed && h->check_budget > 0.0;
+    h->last_checked = check;
+    if (check)
+        if (int rc = ensure_check(h)) return rc;
     if (routed) CUDA_OK(h, cudaMemsetAsync(h->route_counts.p, 0, h->route_counts.n * sizeof(int), st));
+    if (check) {
+        for (double *b : {h->Jp32.p, h->Kp32.p, h->EJ64.p, h->EK64.p, h->EJ32.p, h->EK32.p})
+            CUDA_OK(h, cudaMemsetAsync(b, 0, nn * sizeof(double), st));
+        CUDA_OK(h, cudaMemsetAsync(h->check_max.p, 0, sizeof(unsigned long long), st));
+    }
     if (scatter) {  // unwritten slots (screened quartets, the canonical half) must hold zero
         CUDA_OK(h, cudaMemsetAsync(h->W.p, 0, h->W.n * sizeof(double), st));
         CUDA_OK(h, cudaMemsetAsync(h->wab.p, 0, h->wab.n * sizeof(double), st));
@@ -1547,25 +1651,44 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
             // an FP64 queue; each queue has its own kernel
             int *l32 = h->route_list.p + r.unit0;
             int *l64 = h->route_list.p + h->n_units + r.unit0;
-            int *cnt = h->route_counts.p + 2 * ri;
+            int *ls = h->route_list.p + 2 * (size_t)h->n_units + r.unit0;
+            int *cnt = h->route_counts.p + 4 * ri;
+            const int stride = check ? h->check_stride : 0;
             const int rgrid = std::max(1, std::min((r.n_units + 3) / 4, 16 * sm_count()));
             if (h->router_on)
                 route_units_mlp_kernel<<<rgrid, 128, 0, st>>>(
                     h->units.p, r.unit0, r.n_units, h->launches.p, h->pairs.p, h->prims.p, h->Dsh.p, nsh,
                     h->plan.tau, route, h->router_p.p, h->router_log_thr, r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld,
-                    l32, l64, cnt);
+                    l32, l64, cnt, stride, ls);
             else
                 route_units_kernel<<<rgrid, 128, 0, st>>>(h->units.p, r.unit0, r.n_units, h->launches.p,
                                                           h->pairs.p, h->Dsh.p, nsh, h->plan.tau, route, l32,
-                                                          l64, cnt);
+                                                          l64, cnt, stride, ls);
             KArgs a32 = a, a64 = a;
             a32.unit_list = l32;
             a32.unit_count = cnt;
             a64.unit_list = l64;
             a64.unit_count = cnt + 1;
+            if (check) {  // the FP32 queue into its own accumulators
+                a32.Jp = h->Jp32.p;
+                a32.Kp = h->Kp32.p;
+            }
             CUDA_OK(h, launch_run32(r, st, a32));
             CUDA_OK(h, launch_run(r, st, a64));
             launches += 3;
+            if (check) {  // the sample of the FP32 queue, in FP32 and in FP64
+                KArgs s32 = a32, s64 = a64;
+                s32.unit_list = s64.unit_list = ls;
+                s32.unit_count = s64.unit_count = cnt + 2;
+                s32.Jp = h->EJ32.p;
+                s32.Kp = h->EK32.p;
+                s64.Jp = h->EJ64.p;
+                s64.Kp = h->EK64.p;
+                s32.computed = s64.computed = nullptr;
+                CUDA_OK(h, launch_run32(r, st, s32));
+                CUDA_OK(h, launch_run(r, st, s64));
+                launches += 2;
+            }
         } else {
             CUDA_OK(h, launch_run(r, st, a));
             ++launches;
@@ -1587,9 +1710,44 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
             ++launches;
         }
     }
+    if (check) {
+        // the verdict, then the FP64 re-run of every FP32 queue if it is
+        // over budget (the conditional counts are 0 otherwise)
+        const int cgrid = std::max(1, std::min((int)((nn + 255) / 256), 8 * sm_count()));
+        route_check_kernel<<<cgrid, 256, 0, st>>>(h->EJ64.p, h->EK64.p, h->EJ32.p, h->EK32.p, nao, h->check_max.p);
+        route_decide_kernel<<<1, 256, 0, st>>>(h->check_max.p, (double)h->check_stride, h->check_budget,
+                                               h->route_counts.p, (int)h->runs.size(), h->check_flag.p,
+                                               h->check_est.p);
+        zero_if_kernel<<<cgrid, 256, 0, st>>>(h->Jp32.p, h->Kp32.p, nn, h->check_flag.p);
+        launches += 3;
+        for (size_t ri = 0; ri < h->runs.size(); ++ri) {
+            const ClassRun &r = h->runs[ri];
+            KArgs a{};
+            a.C = r.dev;
+            a.units = h->units.p + r.unit0;
+            a.n_units = r.n_units;
+            a.launches = h->launches.p;
+            a.pairs = h->pairs.p;
+            a.prims = h->prims.p;
+            a.D = D_dev;
+            a.Dsh = h->Dsh.p;
+            a.n_sh = nsh;
+            a.n_ao = nao;
+            a.tau = h->plan.tau;
+            a.Jp = h->Jp32.p;
+            a.Kp = h->Kp32.p;
+            a.boys_tab = h->boys.p;
+            a.unit_list = h->route_list.p + r.unit0;
+            a.unit_count = h->route_counts.p + 4 * ri + 3;
+            CUDA_OK(h, launch_run(r, st, a));
+            ++launches;
+        }
+    }
     h->built = true;
     CUDA_OK(h, cudaEventRecordWithFlags(h->ev1, st, ev_flags));
-    close_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(h->Jp.p, h->Kp.p, nao, J_dev, K_dev, G_dev);
+    close_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(h->Jp.p, h->Kp.p, nao, J_dev, K_dev, G_dev,
+                                                               check ? h->Jp32.p : nullptr,
+                                                               check ? h->Kp32.p : nullptr);
     ++launches;
     CUDA_OK(h, cudaGetLastError());
     h->last_launches = launches;
@@ -1604,6 +1762,8 @@ int fjb_fock_build_graph(fjb_handle *h, const double *D_dev, double *J_dev, doub
     CUDA_OK(h, cudaSetDevice(h->device));
     if (precision == FJB_FP64_SCATTER)  // staging allocates: before the capture
         if (int rc = ensure_scatter(h)) return rc;
+    if (precision == FJB_ROUTED && h->check_budget > 0.0)
+        if (int rc = ensure_check(h)) return rc;
     const void *sig[4] = {D_dev, J_dev, K_dev, G_dev};
     const bool same = h->gexec && std::equal(sig, sig + 4, h->g_sig) && h->g_prec == precision &&
                       h->g_thr == threshold;
@@ -1768,6 +1928,26 @@ int fjb_eri_blocks_fp32(fjb_handle *h, const int32_t *quartets, int n, double *o
     return eri_blocks_impl(h, quartets, n, out_dev, offsets, true);
 }
 
+int fjb_set_route_check(fjb_handle *h, double budget, int stride) {
+    if (!h) return fail(h, FJB_E_ARG, "null handle");
+    if (!(budget == budget) || stride < 1) return fail(h, FJB_E_ARG, "fjb_set_route_check: budget must be a number, stride >= 1");
+    h->check_budget = budget;
+    h->check_stride = stride;
+    h->drop_graph();
+    return FJB_OK;
+}
+
+int fjb_route_check_result(const fjb_handle *hc, double *estimate, int *rerouted) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h || !estimate || !rerouted) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->built || !h->last_checked) return fail(h, FJB_E_STATE, "the last build was not a checked routed build");
+    CUDA_OK(h, cudaEventSynchronize(h->ev1));
+    CUDA_OK(h, cudaDeviceSynchronize());
+    CUDA_OK(h, cudaMemcpy(estimate, h->check_est.p, sizeof(double), cudaMemcpyDeviceToHost));
+    CUDA_OK(h, cudaMemcpy(rerouted, h->check_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+    return FJB_OK;
+}
+
 int fjb_route_stats(const fjb_handle *hc, int64_t *n32, int64_t *n64) {
     fjb_handle *h = const_cast<fjb_handle *>(hc);
     if (!h || !n32 || !n64) return fail(h, FJB_E_ARG, "null argument");
@@ -1780,8 +1960,8 @@ int fjb_route_stats(const fjb_handle *hc, int64_t *n32, int64_t *n64) {
     *n64 = 0;
     for (size_t ri = 0; ri < h->runs.size(); ++ri) {
         if (h->last_routed) {
-            *n32 += c[2 * ri];
-            *n64 += c[2 * ri + 1];
+            *n32 += c[4 * ri];
+            *n64 += c[4 * ri + 1];
         } else {
             *n64 += h->runs[ri].n_units;
         }
@@ -2105,7 +2285,9 @@ int fjb_class_stats(const fjb_handle *hc, fjb_class_stat *out, int64_t n, int64_
         float ms = 0.f;
         CUDA_OK(h, cudaEventSynchronize(h->cev[i].second));
         CUDA_OK(h, cudaEventElapsedTime(&ms, h->cev[i].first, h->cev[i].second));
-        out[i] = fjb_class_stat{d.la, d.lb, d.lc, d.ld, (double)ms, (int64_t)h->runs[i].n_units};
+        const ClassRun &r = h->runs[i];
+        const int32_t engine = r.rys64 ? 2 : (r.compiled ? 1 : 0);
+        out[i] = fjb_class_stat{d.la, d.lb, d.lc, d.ld, (double)ms, (int64_t)r.n_units, engine, 0};
     }
     return FJB_OK;
 }

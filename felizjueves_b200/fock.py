@@ -295,6 +295,20 @@ class FockEngine:
         2 every class it has."""
         _lib.check(self._L.fjb_set_rys(self._h, int(mode)), self._h)
 
+    def set_route_check(self, budget: float = 1e-8, stride: int = 16) -> None:
+        """The routed build's error-budget check (fjb_set_route_check): a
+        sampled FP64 re-build of every stride-th FP32 unit estimates the
+        FP32 error in G; over `budget` the build re-runs its FP32 units in
+        FP64.  budget <= 0 turns it off."""
+        _lib.check(self._L.fjb_set_route_check(self._h, float(budget), int(stride)), self._h)
+
+    def route_check(self) -> tuple[float, bool]:
+        """(estimated max|dG| of the FP32 units, re-routed to FP64?) of the
+        last routed build."""
+        est, flag = C.c_double(), C.c_int()
+        _lib.check(self._L.fjb_route_check_result(self._h, C.byref(est), C.byref(flag)), self._h)
+        return float(est.value), bool(flag.value)
+
     def build_host(self, D, *, precision: int = _lib.FJB_FP64, threshold: float = 0.0, out=None):
         """Host build through the C ABI's host-buffer entry point: numpy in,
         (J, K, G) numpy out -- into `out`, three C-contiguous float64 n x n

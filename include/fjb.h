@@ -304,11 +304,14 @@ typedef struct fjb_launch_stat {
 int fjb_launch_stats(const fjb_handle *h, fjb_launch_stat *out, int64_t n);
 
 /* Per class kernel of the last build: its class, device milliseconds
- * (events around the launch on the build's stream) and work units. */
+ * (events around the launch on the build's stream), work units and the
+ * engine of its FP64 units (0 the HGP interpreter, 1 the register kernel,
+ * 2 the Rys kernel). */
 typedef struct fjb_class_stat {
     int32_t la, lb, lc, ld;
     double ms;
     int64_t units;
+    int32_t engine, pad;
 } fjb_class_stat;
 int fjb_class_stats(const fjb_handle *h, fjb_class_stat *out, int64_t n, int64_t *n_classes);
 
@@ -335,6 +338,25 @@ int fjb_set_class_config32(fjb_handle *h, int la, int lb, int lc, int ld, int th
  * atomics-free build (FJB_FP64_SCATTER) and the ERI tap keep the HGP
  * kernels. */
 int fjb_set_rys(fjb_handle *h, int mode);
+
+/* The routed build's error-budget check (on by default: budget 1e-8,
+ * stride 16).  Every stride-th unit the router puts on the FP32 queue is
+ * built twice more, in FP32 and in FP64, into side accumulators; the
+ * largest element of their G difference times sqrt(stride) estimates the
+ * FP32 queue's error in G (independent rounding errors of stride times as
+ * many units: a statistical estimate, not a bound).  If the estimate
+ * exceeds `budget`, the same build re-runs
+ * every FP32 unit in FP64 and uses those results: the build falls back to
+ * plain FP64 by itself, on the device, inside a captured graph too.  The
+ * first checked build of a handle allocates six n_ao^2 side buffers: make it
+ * before any capture of your own (fjb_fock_build_graph does).  budget <= 0
+ * turns the check off.  No counterpart in the reference; it is the
+ * routed path's "checked against the error budget, re-routed to FP64 on
+ * violation". */
+int fjb_set_route_check(fjb_handle *h, double budget, int stride);
+/* The last routed build's check: the estimate and whether it re-ran the
+ * FP32 queue in FP64 (1) or kept it (0).  Synchronises the device. */
+int fjb_route_check_result(const fjb_handle *h, double *estimate, int *rerouted);
 
 /* fjb_fock_build without any device allocation (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc while they run the
