@@ -1,0 +1,365 @@
+// df_mm.cu -- the density-fitting J/K contractions (fjb_df_jk).
+//
+//   J:  gamma_q = sum_mn B_q,mn D_mn,  J_mn = sum_q B_q,mn gamma_q
+//       (two FP64 matrix-vector passes over B, HBM-bound: df_gamma_kernel,
+//       df_jmat_kernel)
+//   K:  X_q = B_q D,  K = sum_q X_q B_q^T
+//       (two GEMMs on the 5th-generation tensor cores, df_mm_kernel)
+//
+// The reference computes no DF-J/K (eri/density_fit/__init__.py:8-9): this
+// is the standard contraction with the factors B = L^{-1} (Q|mn) of the
+// metric's Cholesky factor L (DFEngine.factors).
+//
+// Tensor-core arithmetic ("split BF16"): every FP64 operand is rounded to
+// FP32 and written as the sum of three BF16 terms hi + mid + lo
+// (df_split_kernel); the six products of total order <= 2 (hi.hi, hi.mid,
+// mid.hi, hi.lo, mid.mid, lo.hi) are accumulated in FP32 in tensor memory,
+// which keeps the FP32 operands' precision to about 2^-24 relative.
+//
+// df_mm_kernel: one CTA (four warps) per 128 x 128 output tile.  Per K-tile
+// of 64, the threads stage the six BF16 operand tiles (A and B, three parts
+// each, 96 KiB) into shared memory in the UMMA canonical K-major layout
+// without swizzle (8-row x 16-byte core matrices, 128 bytes each; LBO = 128
+// bytes between core matrices along K, SBO = 1024 bytes between 8-row
+// groups), one thread issues the 24 tcgen05.mma (six products x four
+// K = 16 steps) into the FP32 accumulator in TMEM and commits them to an
+// mbarrier that every thread waits on before the tiles are overwritten.
+// The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM
+// lanes, i.e. output rows, 32w .. 32w + 31) and writes FP64.  Every wait is
+// bounded: on timeout the kernel records an error flag, frees its TMEM and
+// returns.  Operands come from this GPU's own memory only; no multicast.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+namespace fjb {
+
+namespace {
+
+constexpr int kMmTile = 128;   // output rows (M) and columns (N) of a CTA
+constexpr int kMmK = 64;       // K per staged tile
+constexpr int kMmThreads = 128;
+constexpr int kPartBytes = kMmTile * kMmK * 2;  // one BF16 operand tile: 16 KiB
+constexpr long long kWaitLimit = 1LL << 22;     // mbarrier polls before giving up
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// UMMA shared-memory descriptor, K-major, no swizzle (layout type 0),
+// descriptor version 1: start address, LBO and SBO in 16-byte units.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Instruction descriptor of tcgen05.mma kind::f16: D F32, A and B BF16,
+// both K-major, N = 128, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kMmTile >> 3) << 17) |
+                            ((uint32_t)(kMmTile >> 4) << 24);
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// Poll the mbarrier's phase `parity` at most kWaitLimit times; false on
+// timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (long long i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+}  // namespace
+
+// Round v (FP64) to FP32 and split it into three BF16 terms.
+__device__ __forceinline__ void split3(double v, __nv_bfloat16 *h, __nv_bfloat16 *m, __nv_bfloat16 *l) {
+    const float f = (float)v;
+    const __nv_bfloat16 a = __float2bfloat16_rn(f);
+    const float r = f - __bfloat162float(a);
+    const __nv_bfloat16 b = __float2bfloat16_rn(r);
+    const float s = r - __bfloat162float(b);
+    *h = a;
+    *m = b;
+    *l = __float2bfloat16_rn(s);
+}
+
+// The split operand of a GEMM, rows x cols (cols = the contraction index),
+// written K-major into three BF16 arrays of leading dimension ldp (>= cols,
+// a multiple of kMmK) and rows_p rows (a multiple of kMmTile); the padding
+// is zero.  Element (r, c) of the source:
+//   mode 0: src[r * ld + c]
+//   mode 1: src[(c / n) * n * n + r * n + c % n]  (the aux-batched
+//           transpose: row r of every n x n block q, side by side)
+__global__ void df_split_kernel(const double *__restrict__ src, int mode, long long rows, long long cols,
+                                long long ld, long long n, long long rows_p, long long ldp, __nv_bfloat16 *hi,
+                                __nv_bfloat16 *mid, __nv_bfloat16 *lo) {
+    const long long total = rows_p * ldp;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / ldp, c = i - r * ldp;
+        double v = 0.0;
+        if (r < rows && c < cols) v = mode == 0 ? src[r * ld + c] : src[(c / n) * n * n + r * n + c % n];
+        split3(v, hi + i, mid + i, lo + i);
+    }
+}
+
+// C[M x N] (FP64, leading dimension ldc) = sum over the six split products
+// of A (rows_p x ldp, K-major) and B (cols_p x ldp, K-major): C = A B^T.
+__global__ void __launch_bounds__(kMmThreads, 1)
+    df_mm_kernel(const __nv_bfloat16 *__restrict__ A0, const __nv_bfloat16 *__restrict__ A1,
+                 const __nv_bfloat16 *__restrict__ A2, const __nv_bfloat16 *__restrict__ B0,
+                 const __nv_bfloat16 *__restrict__ B1, const __nv_bfloat16 *__restrict__ B2, long long M,
+                 long long N, long long ldp, double *__restrict__ C, long long ldc, int kt_per_split, int *err) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base;
+    unsigned char *tiles = smem;  // A0 A1 A2 B0 B1 B2, kPartBytes each
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const long long m0 = (long long)blockIdx.x * kMmTile, n0 = (long long)blockIdx.y * kMmTile;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(kMmTile));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+
+    // this CTA's K range: tiles [k_begin, k_end) of split blockIdx.z
+    const int n_k = (int)(ldp / kMmK);
+    const int k_begin = (int)blockIdx.z * kt_per_split, k_end = min(n_k, k_begin + kt_per_split);
+    const bool split = gridDim.z > 1;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int kt = k_begin; kt < k_end && ok; ++kt) {
+        // stage: 6 parts x 128 rows x 8 chunks of 16 bytes; chunk (r, c) of a
+        // part goes to (r / 8) * 1024 + c * 128 + (r % 8) * 16
+        for (int i = tid; i < 6 * kMmTile * (kMmK / 8); i += kMmThreads) {
+            const int part = i / (kMmTile * (kMmK / 8)), rem = i - part * (kMmTile * (kMmK / 8));
+            const int r = rem >> 3, c = rem & 7;
+            const __nv_bfloat16 *src = part == 0 ? A0 : part == 1 ? A1 : part == 2 ? A2 : part == 3 ? B0 : part == 4 ? B1 : B2;
+            const long long row0 = part < 3 ? m0 : n0;
+            const uint4 v = *reinterpret_cast<const uint4 *>(src + (row0 + r) * ldp + (long long)kt * kMmK + c * 8);
+            *reinterpret_cast<uint4 *>(tiles + part * kPartBytes + (r >> 3) * 1024 + c * 128 + (r & 7) * 16) = v;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t base = smem_u32(tiles);
+            const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
+#pragma unroll
+            for (int p = 0; p < 6; ++p)
+#pragma unroll
+                for (int ks = 0; ks < kMmK / 16; ++ks) {
+                    const uint64_t da = umma_desc(base + pa[p] * kPartBytes + ks * 256, 128, 1024);
+                    const uint64_t db = umma_desc(base + (3 + pb[p]) * kPartBytes + ks * 256, 128, 1024);
+                    const uint32_t acc = (kt > k_begin || p > 0 || ks > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                        "l"(da), "l"(db), "r"(kIdesc), "r"(acc));
+                }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(&bar)));
+        }
+        ok = __syncthreads_and(mbar_wait(&bar, phase)) != 0;  // one verdict for the whole CTA
+        phase ^= 1u;
+    }
+    if (k_begin >= k_end) {
+        // an empty split: no accumulator to read
+    } else if (!ok) {
+        if (tid == 0) atomicExch(err, 1);
+    } else {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // epilogue: warp w reads rows 32w + lane, 16 columns at a time
+        const long long row = m0 + warp * 32 + (tid & 31);
+        for (int c0 = 0; c0 < kMmTile; c0 += 16) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                  "=r"(v[14]), "=r"(v[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;");
+            if (row < M)
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const long long col = n0 + c0 + j;
+                    if (col < N) {
+                        // split K: the FP32 partial sums add up in FP64
+                        if (split)
+                            atomicAdd(C + row * ldc + col, (double)__uint_as_float(v[j]));
+                        else
+                            C[row * ldc + col] = (double)__uint_as_float(v[j]);
+                    }
+                }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kMmTile));
+}
+
+// gamma_q = sum_i B[q][i] D[i], i over the n_ao^2 elements (FP64): one CTA
+// per q, a block reduction.
+__global__ void df_gamma_kernel(const double *__restrict__ B, const double *__restrict__ D, long long nn,
+                                double *gamma) {
+    const double *b = B + (long long)blockIdx.x * nn;
+    double s = 0.0;
+    for (long long i = threadIdx.x; i < nn; i += blockDim.x) s += b[i] * D[i];
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) gamma[blockIdx.x] = s;
+    }
+}
+
+// J[i] = sum_q B[q][i] gamma_q (FP64): a thread per element, q in order
+// (coalesced across i).
+__global__ void df_jmat_kernel(const double *__restrict__ B, const double *__restrict__ gamma, long long nq,
+                               long long nn, double *J) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nn;
+         i += (long long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (long long q = 0; q < nq; ++q) s += B[q * nn + i] * gamma[q];
+        J[i] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side: the workspace and the launch sequence of one DF-J/K build
+
+namespace {
+
+long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
+
+struct DfShape {
+    long long nq, n;
+    long long rows1, ld1;   // GEMM 1 (X = B D): A is B as (nq n) x n, B is D
+    long long rowsn, ld2;   // GEMM 2 (K = sum_q X_q B_q^T): n x (nq n) operands
+    long long split1, split2;  // BF16 elements of one split part
+};
+
+DfShape df_shape(long long nq, long long n) {
+    DfShape s;
+    s.nq = nq;
+    s.n = n;
+    s.rows1 = round_up(nq * n, kMmTile);
+    s.ld1 = round_up(n, kMmK);
+    s.rowsn = round_up(n, kMmTile);
+    s.ld2 = round_up(nq * n, kMmK);
+    s.split1 = s.rows1 * s.ld1 + s.rowsn * s.ld1;  // A parts + B parts of GEMM 1, per term
+    s.split2 = 2 * s.rowsn * s.ld2;                // A parts + B parts of GEMM 2, per term
+    return s;
+}
+
+}  // namespace
+
+// Device bytes fjb_df_jk needs as workspace for nq aux functions and n AOs:
+// gamma, X (nq n^2 doubles), the error flag and the split operands.
+size_t df_jk_workspace_bytes(long long nq, long long n) {
+    const DfShape s = df_shape(nq, n);
+    const long long split = 3 * (s.split1 > s.split2 ? s.split1 : s.split2);
+    return (size_t)round_up((round_up(nq, 32) + nq * n * n) * (long long)sizeof(double), 256) + (size_t)split * 2;
+}
+
+static cudaError_t df_mm(const __nv_bfloat16 *a, long long a_rows, const __nv_bfloat16 *b, long long b_rows,
+                         long long ldp, long long M, long long N, double *C, long long ldc, int *err,
+                         cudaStream_t st) {
+    static bool attr = false;
+    const int smem = 6 * kPartBytes;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(df_mm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const long long pa = a_rows * ldp, pb = b_rows * ldp;
+    const long long tiles = (a_rows / kMmTile) * (b_rows / kMmTile);
+    const int n_k = (int)(ldp / kMmK);
+    // split K until the grid covers the 148 SMs twice, each split keeping
+    // at least 8 K-tiles; the splits' FP32 partials are added in FP64
+    int splits = 1;
+    if (tiles < 2 * 148) splits = (int)std::max(1LL, std::min((long long)(n_k / 8), (2 * 148 + tiles - 1) / tiles));
+    const int per = (n_k + splits - 1) / splits;
+    splits = (n_k + per - 1) / per;
+    if (splits > 1) {  // the splits add into C
+        cudaError_t e = cudaMemset2DAsync(C, (size_t)ldc * sizeof(double), 0, (size_t)N * sizeof(double),
+                                          (size_t)M, st);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((unsigned)(a_rows / kMmTile), (unsigned)(b_rows / kMmTile), (unsigned)splits);
+    df_mm_kernel<<<grid, kMmThreads, smem, st>>>(a, a + pa, a + 2 * pa, b, b + pb, b + 2 * pb, M, N, ldp, C, ldc,
+                                                 per, err);
+    return cudaGetLastError();
+}
+
+// J and K of density D from the DF factors B (nq x n x n, FP64, device):
+// J in FP64 on the CUDA cores, K by the split-BF16 tensor-core GEMMs.  `work`
+// holds df_jk_workspace_bytes(nq, n) device bytes; `err` (device int) is set
+// when a bounded wait of the GEMM kernel runs out.
+cudaError_t df_jk_launch(const double *B, long long nq, long long n, const double *D, double *J, double *K,
+                         void *work, int *err, cudaStream_t st) {
+    const DfShape s = df_shape(nq, n);
+    double *gamma = static_cast<double *>(work);
+    double *X = gamma + round_up(nq, 32);
+    // the split operands start on a 256-byte boundary (16-byte vector loads)
+    __nv_bfloat16 *sp = reinterpret_cast<__nv_bfloat16 *>(
+        static_cast<unsigned char *>(work) + round_up((round_up(nq, 32) + nq * n * n) * (long long)sizeof(double), 256));
+    const long long nn = n * n;
+    df_gamma_kernel<<<(unsigned)nq, 256, 0, st>>>(B, D, nn, gamma);
+    df_jmat_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(B, gamma, nq, nn, J);
+    // GEMM 1: X (nq n x n) = B (nq n x n) . D^T (D symmetric)
+    __nv_bfloat16 *a1 = sp, *b1 = sp + 3 * s.rows1 * s.ld1;
+    const unsigned sgrid = 148 * 16;
+    df_split_kernel<<<sgrid, 256, 0, st>>>(B, 0, nq * n, n, n, n, s.rows1, s.ld1, a1, a1 + s.rows1 * s.ld1,
+                                           a1 + 2 * s.rows1 * s.ld1);
+    df_split_kernel<<<sgrid, 256, 0, st>>>(D, 0, n, n, n, n, s.rowsn, s.ld1, b1, b1 + s.rowsn * s.ld1,
+                                           b1 + 2 * s.rowsn * s.ld1);
+    cudaError_t e = df_mm(a1, s.rows1, b1, s.rowsn, s.ld1, nq * n, n, X, n, err, st);
+    if (e != cudaSuccess) return e;
+    // GEMM 2: K (n x n) = [X_q rows side by side] . [B_q rows side by side]^T
+    __nv_bfloat16 *a2 = sp, *b2 = sp + 3 * s.rowsn * s.ld2;
+    df_split_kernel<<<sgrid, 256, 0, st>>>(X, 1, n, nq * n, 0, n, s.rowsn, s.ld2, a2, a2 + s.rowsn * s.ld2,
+                                           a2 + 2 * s.rowsn * s.ld2);
+    df_split_kernel<<<sgrid, 256, 0, st>>>(B, 1, n, nq * n, 0, n, s.rowsn, s.ld2, b2, b2 + s.rowsn * s.ld2,
+                                           b2 + 2 * s.rowsn * s.ld2);
+    e = df_mm(a2, s.rowsn, b2, s.rowsn, s.ld2, n, n, K, n, err, st);
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+}  // namespace fjb

@@ -38,6 +38,10 @@ bool compiled_available(int la, int lb, int lc, int ld, bool fp32);
 int compiled_blocks_per_sm(int la, int lb, int lc, int ld, bool fp32);
 cudaError_t launch_compiled(int la, int lb, int lc, int ld, bool fp32, int grid, cudaStream_t st,
                             const KArgs &a);
+// df_mm.cu: the DF-J/K contractions
+size_t df_jk_workspace_bytes(long long nq, long long n);
+cudaError_t df_jk_launch(const double *B, long long nq, long long n, const double *D, double *J, double *K,
+                         void *work, int *err, cudaStream_t st);
 }
 
 using namespace fjb;
@@ -874,6 +878,8 @@ struct fjb_handle {
     std::map<std::tuple<int, int, int, int>, std::pair<int, int>> cfg32;  // the FP32 interpreter's
     DevBuf<double> boys;
     DevBuf<double> rys;  // the tabulated Rys rule (rys_rule.h)
+    DevBuf<unsigned char> df_work;  // fjb_df_jk's workspace
+    DevBuf<int> df_err;
     int use_rys = 1;  // which classes the Rys kernel takes (fjb_set_rys)
     DevBuf<int> sh_off, sh_nc;
     // plan
@@ -2046,6 +2052,29 @@ int fjb_df_blocks(fjb_handle *h, int kind, const int32_t *items, int n, double *
         }
     }
     return fjb_eri_blocks(h, q.data(), n, out_dev, offsets);
+}
+
+int fjb_df_jk(fjb_handle *h, const double *B_dev, int64_t n_aux, int64_t n_ao, const double *D_dev, double *J_dev,
+              double *K_dev, void *stream) {
+    if (!h || !B_dev || !D_dev || !J_dev || !K_dev) return fail(h, FJB_E_ARG, "null argument");
+    if (n_aux < 1 || n_ao < 1) return fail(h, FJB_E_ARG, "fjb_df_jk: n_aux and n_ao must be >= 1");
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    CUDA_OK(h, cudaSetDevice(h->device));
+    const size_t bytes = df_jk_workspace_bytes(n_aux, n_ao);
+    try {
+        if (h->df_work.n < bytes) h->df_work.alloc(bytes);
+        h->df_err.alloc(1);
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, std::string("fjb_df_jk workspace: ") + e.what());
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_OK(h, cudaMemsetAsync(h->df_err.p, 0, sizeof(int), st));
+    CUDA_OK(h, df_jk_launch(B_dev, n_aux, n_ao, D_dev, J_dev, K_dev, h->df_work.p, h->df_err.p, st));
+    int err = 0;
+    CUDA_OK(h, cudaMemcpyAsync(&err, h->df_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(h, cudaStreamSynchronize(st));
+    if (err) return fail(h, FJB_E_TIMEOUT, "fjb_df_jk: a tensor-core wait ran out (the GEMM did not complete)");
+    return FJB_OK;
 }
 
 int fjb_scatter_map(const fjb_handle *hc, int launch, int32_t *el, int32_t *ptr, int32_t *src, int64_t *n_el,

@@ -13,13 +13,15 @@ Cholesky factor L (V = L L^T):
     J_mn = sum_P B_mn,P (sum_ls B_ls,P D_ls)
     K_mn = sum_P sum_ls B_ml,P D_ls B_sn,P
 
-`jk(D, mode="fp64")` runs the contractions as FP64 GEMMs; `mode="bf16x3"`
-runs them on the tensor cores as split products: each FP32 operand is the sum
-of three BF16 terms (hi + mid + lo), the six products whose orders sum to at
-most 2 are accumulated in FP32 (`torch.mm(..., out_dtype=float32)`), which
-keeps the FP32 operand's precision to about 2^-24.  The Cholesky and the
-triangular solve are FP64.  Errors of both against the exact (4-centre) J, K
-are reported by the tests.
+`jk(D, mode="bf16x3")` runs the contractions through the library's own
+kernels (`fjb_df_jk`, csrc/df_mm.cu): J by two FP64 passes over B, K by two
+GEMMs on the tensor cores (tcgen05, accumulators in tensor memory) as split
+products -- each FP32 operand the sum of three BF16 terms (hi + mid + lo),
+the six products whose orders sum to at most 2 accumulated in FP32, which
+keeps the FP32 operand's precision to about 2^-24.  `mode="fp64"` is the
+FP64 check path (device FP64 GEMMs through torch).  The Cholesky and the
+triangular solve are FP64.  Errors of both against the exact (4-centre) J,
+K are reported by the tests.
 """
 
 from __future__ import annotations
@@ -155,35 +157,15 @@ class DFEngine:
                              B.permute(0, 2, 1).reshape(nx * n, n))
             return J, K
         if mode == "bf16x3":
-            B2 = B.reshape(nx, n * n)
-            gamma = _mm3(B2, D.reshape(n * n, 1)).reshape(nx)
-            J = _mm3(B2.T.contiguous(), gamma.reshape(nx, 1)).reshape(n, n)
-            X = _mm3(B.reshape(nx * n, n), D).reshape(nx, n, n)   # X_q = B_q D, one GEMM
-            K = _mm3(X.permute(1, 0, 2).reshape(n, nx * n).contiguous(),
-                     B.permute(0, 2, 1).reshape(nx * n, n).contiguous())
+            # the library's kernels (fjb_df_jk): J in FP64, K on the tensor
+            # cores as split-BF16 products accumulated in FP32
+            Bc = B.contiguous()
+            Dc = D.contiguous()
+            J = torch.empty((n, n), dtype=torch.float64, device=Bc.device)
+            K = torch.empty_like(J)
+            st = torch.cuda.current_stream(Bc.device)
+            _lib.check(self._L.fjb_df_jk(self._h, Bc.data_ptr(), nx, n, Dc.data_ptr(), J.data_ptr(),
+                                         K.data_ptr(), C.c_void_p(st.cuda_stream)), self._h)
             return J, K
         raise ValueError(f"unknown mode {mode!r}")
 
-
-def _split3(a):
-    import torch
-    a32 = a.to(torch.float32)
-    h = a32.to(torch.bfloat16)
-    r = a32 - h.to(torch.float32)
-    m = r.to(torch.bfloat16)
-    lo = (r - m.to(torch.float32)).to(torch.bfloat16)
-    return h, m, lo
-
-
-def _mm3(a, b):
-    """a @ b on the tensor cores: three-term BF16 splits, the six products of
-    total order <= 2 accumulated in FP32, returned as FP64."""
-    import torch
-    A = _split3(a)
-    Bs = _split3(b)
-    out = None
-    for i in range(3):
-        for j in range(3 - i):
-            p = torch.mm(A[i], Bs[j], out_dtype=torch.float32)
-            out = p if out is None else out + p
-    return out.to(torch.float64)

@@ -339,6 +339,20 @@ int fjb_set_class_config32(fjb_handle *h, int la, int lb, int lc, int ld, int th
  * kernels. */
 int fjb_set_rys(fjb_handle *h, int mode);
 
+/* Density-fitted J and K of the symmetric density D (DEVICE, n_ao^2) from
+ * the factors B (DEVICE, n_aux x n_ao x n_ao, FP64: B_P = sum_Q (L^-1)_PQ
+ * (Q|mn), L the Cholesky factor of the metric (P|Q)).  J_mn = sum_P B_P,mn
+ * gamma_P, gamma_P = sum_ls B_P,ls D_ls in FP64; K_mn = sum_P (B_P D B_P^T)_mn
+ * as two GEMMs on the tensor cores, every operand split into three BF16
+ * terms and the six products of total order <= 2 accumulated in FP32.  The
+ * handle owns the workspace (about 2 n_aux n_ao^2 doubles).  The reference
+ * computes no DF-J/K (eri/density_fit/__init__.py:8-9); its (mn|P) layout
+ * ([m][n][P], eri/density_fit/eri3.py:226) is what DFEngine.factors turns
+ * into B.  Synchronises `stream`; FJB_E_TIMEOUT if a tensor-core wait ran
+ * out. */
+int fjb_df_jk(fjb_handle *h, const double *B_dev, int64_t n_aux, int64_t n_ao, const double *D_dev,
+              double *J_dev, double *K_dev, void *stream);
+
 /* The routed build's error-budget check (on by default: budget 1e-8,
  * stride 16).  Every stride-th unit the router puts on the FP32 queue is
  * built twice more, in FP32 and in FP64, into side accumulators; the

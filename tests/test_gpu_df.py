@@ -1,8 +1,10 @@
 """Density fitting on the GPU: (P|Q) and (mn|P) from the HGP kernels against
 libcint's (the reference's fixtures), and DF-J/K against the oracle's numpy
 restatement (FP64: max(1e-10, 1e-15 cond(V)) of max|.|, the metric solve
-amplifying integral rounding by its condition number; tensor-core BF16x3
-split: error reported and bounded by 1e-6 (J) and 1e-5 (K) of max|.|).
+amplifying integral rounding by its condition number; the library's
+fjb_df_jk: J in FP64 (1e-12 of max|J| against the FP64 contractions), K on
+the tensor cores as a BF16x3 split (error reported, bounded by 1e-5 of
+max|K|)).
 DF's own error against the exact
 4-centre J, K is reported (it is the fitting error, not a kernel error)."""
 
@@ -69,8 +71,28 @@ def test_df_jk_matches_oracle(cuda, lib_built, oracle_lib):
     fJ = np.abs(J.cpu().numpy() - Je).max() / np.abs(Je).max()
     fK = np.abs(K.cpu().numpy() - Ke).max() / np.abs(Ke).max()
     print(f"bf16x3 vs fp64 DF: J {eJ:.2e} K {eK:.2e}; DF vs exact: J {fJ:.2e} K {fK:.2e}")
-    # FP32-level products (2^-24) summed with cancellation: K, a sum over
-    # aux x AO of signed terms, keeps ~1e-6; both stay orders below the
+    # J is FP64 on both paths; K's FP32-level products (2^-24) summed with
+    # cancellation over aux x AO signed terms keep ~1e-6, orders below the
     # fitting error of this aux recipe (DF vs exact above).
-    assert eJ <= 1e-6 and eK <= 1e-5
+    assert eJ <= 1e-12 and eK <= 1e-5
     assert eK < 1e-2 * fK
+
+
+def test_df_tensor_core_k_over_tiles(cuda, lib_built):
+    """fjb_df_jk on a 5-atom cluster (155 AO: two 128-wide output tiles with
+    a ragged edge; 450 aux functions: 1,090 K-tiles in the second GEMM),
+    against the FP64 contractions of the same factors."""
+    import torch
+    from felizjueves_b200.df import DFEngine
+    w = configs.cluster(5, 9)
+    aux = configs.aux_basis(w)
+    eng = DFEngine(w.basis, aux)
+    D = torch.tensor(w.D, device=cuda)
+    B = eng.factors()
+    J, K = eng.jk(D, "fp64", B=B)
+    J3, K3 = eng.jk(D, "bf16x3", B=B)
+    eJ = float((J3 - J).abs().max() / J.abs().max())
+    eK = float((K3 - K).abs().max() / K.abs().max())
+    print(f"n_ao {w.n_ao} n_aux {aux.n_ao}: J {eJ:.2e} K {eK:.2e}")
+    assert eJ <= 1e-12 and eK <= 1e-5
+    assert float((K3 - K3.T).abs().max()) <= 1e-5 * float(K.abs().max())
