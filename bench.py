@@ -58,6 +58,7 @@ def parse():
                          "df: DF-J/K (FP64 and split-BF16 tensor-core GEMMs); batch: the "
                          "uneven molecule batch (c4) as one captured graph")
     ap.add_argument("--molecules", type=int, default=64, help="batch path: the first N c4 molecules")
+    ap.add_argument("--atoms", type=int, default=16, help="df path: atoms of the c1-recipe cluster")
     ap.add_argument("--threshold", type=float, default=1e-9,
                     help="routed builds: the Schwarz x density bound under which a unit runs FP32 "
                          "(config c2's rule: 1e-9)")
@@ -518,31 +519,48 @@ def side_path(a, local):
                                     "sample": f"oracle one_electron.blocks on {len(sample)} random shell pairs "
                                               f"of {len(pairs)}, {spent:.1f} s, scaled by the pair count"}
     else:
+        # DF-J/K on a cluster of the c1 recipe (--atoms; the 64-atom system's
+        # dense factors, 5,760 x 1,984^2 doubles, do not fit in HBM)
         from felizjueves_b200.df import DFEngine
+        w = configs.cluster(a.atoms, 1)
+        D = torch.tensor(w.D, device=f"cuda:{local}")
         aux = configs.aux_basis(w)
         eng = DFEngine(w.basis, aux, device=local)
         B = eng.factors()
         ms64, (J64, K64) = timed(lambda: eng.jk(D, "fp64", B=B))
         ms16, (J16, K16) = timed(lambda: eng.jk(D, "bf16x3", B=B))
+        nq, n = aux.n_ao, w.n_ao
+        useful = 4.0 * nq * n ** 3  # X = B D and K = sum_q X_q B_q^T, 2 nq n^3 flops each
         line.update(metric="DF-J/K ms/iter", value=round(ms16, 3), unit="ms/iter", dtype="bf16x3 -> f32",
-                    fp64_ms=round(ms64, 3), n_aux=aux.n_ao,
+                    config={"workload": f"{a.atoms}-atom cluster (c1 recipe), {n} AO, {nq} aux", "n_ao": n,
+                            "n_aux": nq},
+                    fp64_ms=round(ms64, 3), n_aux=nq,
+                    k_gemm_useful_tflops=round(useful / (ms16 * 1e-3) / 1e12, 3),
+                    k_gemm_tensor_tflops=round(6 * useful / (ms16 * 1e-3) / 1e12, 3),
+                    gpu_launches=10,
                     max_abs_dJ_bf16x3_vs_fp64=float((J16 - J64).abs().max()),
-                    max_abs_dK_bf16x3_vs_fp64=float((K16 - K64).abs().max()))
+                    max_abs_dK_bf16x3_vs_fp64=float((K16 - K64).abs().max()),
+                    max_abs_K_fp64=float(K64.abs().max()))
     print(json.dumps(line))
 
 
 def batch_path(a, local):
     """The c4 batch (its first --molecules molecules): the plain FP64
-    per-molecule loop, the batch as one captured graph in FP64, and in the
-    routed mode with the learned router (trained here on seeded 4-10 atom
-    clusters, calibrated, installed on every molecule); total ms per batch,
-    per-molecule device ms (p50, p99) and max|dG| against FP64."""
+    per-molecule loop (each molecule its own launches, one after another),
+    then the batched build -- one launch per angular-momentum class for the
+    whole batch over a class-sorted queue of every molecule's work units,
+    captured as one CUDA graph -- in FP64 and routed (the Schwarz x density
+    bound router at 1e-9); total ms per batch, per-molecule device ms of the
+    loop (p50, p99) and max|dG| of the batched routed build against the
+    per-molecule FP64 builds."""
     import torch
-    from felizjueves_b200 import _lib, configs, router
+    from felizjueves_b200 import _lib, configs
     from felizjueves_b200.batch import BatchBuilder
     torch.cuda.set_device(local)
+    t0 = time.perf_counter()
     ws = configs.c4(a.molecules)
     bb = BatchBuilder(ws, device=local)
+    plan_s = time.perf_counter() - t0
     st = torch.cuda.current_stream()
 
     def timed(fn):
@@ -558,27 +576,31 @@ def batch_path(a, local):
         return e0.elapsed_time(e1) / a.steps
 
     loop_ms = timed(lambda: bb.build_loop(_lib.FJB_FP64))
-    bb.capture("fp64", _lib.FJB_FP64)
-    g64_ms = timed(lambda: bb.replay("fp64"))
-    G64 = [g.clone() for g in bb.G()]
-    mlp, margin, _ = train_router()
-    for eng in bb.engines:
-        router.install(eng, mlp, threshold=1e-9, margin=margin)
-    bb.capture("routed", _lib.FJB_ROUTED, 1e-9)
-    gr_ms = timed(lambda: bb.replay("routed"))
     per = bb.device_ms()
+    G64 = [g.clone() for g in bb.G()]
+    bb.capture_merged("m64", _lib.FJB_FP64)
+    m64_ms = timed(lambda: bb.replay("m64"))
+    dG64 = max(float((g - h).abs().max()) for g, h in zip(bb.G(), G64))
+    bb.capture_merged("m32", _lib.FJB_ROUTED, 1e-9)
+    m32_ms = timed(lambda: bb.replay("m32"))
     dG = max(float((g - h).abs().max()) for g, h in zip(bb.G(), G64))
+    stats = bb.merged_stats()
     sizes = [len(w.coords) for w in ws]
     print(json.dumps({
-        "metric": "uneven batch G builds ms/batch (one graph, routed + learned router)", "value": round(gr_ms, 3),
-        "unit": "ms/batch", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "higher_is_better": False,
-        "data": "synthetic", "dtype": "f64 (routed units FP32)",
+        "metric": "uneven batch G builds ms/batch (batched build: one launch per class, routed)",
+        "value": round(m32_ms, 3), "unit": "ms/batch", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "higher_is_better": False, "data": "synthetic", "dtype": "f64 (routed units FP32)",
         "config": {"workload": f"c4: first {len(ws)} of 512 molecules, {min(sizes)}-{max(sizes)} atoms "
                                f"({sum(sizes)} atoms, {sum(w.n_ao for w in ws)} AO in all)"},
-        "fp64_loop_ms": round(loop_ms, 3), "fp64_graph_ms": round(g64_ms, 3),
-        "per_molecule_device_ms": {"p50": round(float(np.percentile(per, 50)), 3),
-                                   "p99": round(float(np.percentile(per, 99)), 3)},
-        "max_abs_dG_vs_fp64": dG, "router_margin": round(margin, 3)}))
+        "fp64_loop_ms": round(loop_ms, 3), "batched_fp64_ms": round(m64_ms, 3),
+        "speedup_batched_routed_vs_fp64_loop": round(loop_ms / m32_ms, 4),
+        "per_molecule_device_ms_fp64_loop": {"p50": round(float(np.percentile(per, 50)), 3),
+                                             "p99": round(float(np.percentile(per, 99)), 3)},
+        "max_abs_dG_batched_fp64_vs_loop": dG64, "max_abs_dG_batched_routed_vs_fp64": dG,
+        "class_launches_per_batch": stats["class_launches"], "work_units": stats["units"],
+        "gpu_launches": 2 * stats["class_launches"] + 2,
+        "host_plan_s": round(plan_s, 1)}))
+    bb.close()
 
 
 def reference_arm(a, rank, world):

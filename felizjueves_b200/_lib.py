@@ -84,6 +84,14 @@ def load():
     L.fjb_set_rys.argtypes = [vp, C.c_int]
     L.fjb_set_route_check.argtypes = [vp, dbl, C.c_int]
     L.fjb_df_jk.argtypes = [vp, vp, i64, i64, vp, vp, vp, vp]
+    L.fjb_batch_create.argtypes = [C.POINTER(vp), vp, C.c_int]
+    L.fjb_batch_set_densities.argtypes = [vp, vp, vp, vp, vp]
+    L.fjb_batch_build.argtypes = [vp, C.c_int, dbl, vp]
+    L.fjb_batch_stats.argtypes = [vp, C.POINTER(dbl), C.POINTER(i64), C.POINTER(i64)]
+    L.fjb_batch_last_error.restype = C.c_char_p
+    L.fjb_batch_last_error.argtypes = [vp]
+    L.fjb_batch_destroy.argtypes = [vp]
+    L.fjb_batch_destroy.restype = None
     L.fjb_route_check_result.argtypes = [vp, C.POINTER(dbl), C.POINTER(C.c_int)]
     L.fjb_fock_build_graph.argtypes = [vp, vp, vp, vp, vp, C.c_int, dbl, vp]
     L.fjb_create_df.argtypes = [C.POINTER(vp), C.POINTER(Basis_t), C.POINTER(Basis_t), C.c_int]
@@ -110,6 +118,8 @@ EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_
            "fjb_last_build_stats", "fjb_launch_stats", "fjb_class_stats",
            "fjb_fma_probe", "fjb_fock_build_noalloc", "fjb_set_class_config", "fjb_set_class_config32",
            "fjb_set_rys", "fjb_set_route_check", "fjb_route_check_result", "fjb_df_jk",
+           "fjb_batch_create", "fjb_batch_set_densities", "fjb_batch_build", "fjb_batch_stats",
+           "fjb_batch_last_error", "fjb_batch_destroy",
            "fjb_fock_build_graph", "fjb_create_df", "fjb_df_blocks", "fjb_mlp_n_params",
            "fjb_router_set", "fjb_router_features", "fjb_mlp_forward", "fjb_mlp_gradient",
            "fjb_mlp_adam", "fjb_route_stats", "fjb_coulomb", "fjb_j_last_launches",

@@ -135,6 +135,43 @@ __global__ void zero_if_kernel(double *a, double *b, size_t n, const int *flag) 
     }
 }
 
+// The batched build's per-molecule setup and close: one launch for every
+// molecule (blockIdx.y is the molecule).
+struct BatchMol {
+    const double *D;
+    double *Dsh;
+    const int *sh_off, *sh_nc;  // this molecule's shell AO offsets and sizes
+    int n_sh, n_ao;
+    const double *Jp, *Kp;
+    double *J, *K, *G;
+};
+
+__global__ void batch_density_blocks_kernel(const BatchMol *bm) {
+    const BatchMol &m = bm[blockIdx.y];
+    const int st = blockIdx.x * blockDim.x + threadIdx.x;
+    if (st >= m.n_sh * m.n_sh) return;
+    const int s = st / m.n_sh, t = st % m.n_sh;
+    double v = 0.0;
+    for (int i = 0; i < m.sh_nc[s]; ++i)
+        for (int j = 0; j < m.sh_nc[t]; ++j) {
+            const double x = fabs(m.D[(size_t)(m.sh_off[s] + i) * m.n_ao + m.sh_off[t] + j]);
+            if (x > v) v = x;
+        }
+    m.Dsh[st] = v;
+}
+
+__global__ void batch_close_kernel(const BatchMol *bm) {
+    const BatchMol &m = bm[blockIdx.y];
+    const size_t nn = (size_t)m.n_ao * m.n_ao;
+    for (size_t ij = (size_t)blockIdx.x * blockDim.x + threadIdx.x; ij < nn; ij += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = ij / m.n_ao, j = ij % m.n_ao, ji = j * m.n_ao + i;
+        const double jv = m.Jp[ij] + m.Jp[ji], kv = m.Kp[ij] + m.Kp[ji];
+        if (m.J) m.J[ij] = jv;
+        if (m.K) m.K[ij] = kv;
+        if (m.G) m.G[ij] = jv - 0.5 * kv;
+    }
+}
+
 // The atomics-free build (scatter.h).  A bra segment is one bra pair of one
 // launch: its units' partial bra blocks are summed in unit order into the
 // segment's bra-block slots.
@@ -212,7 +249,7 @@ __global__ void screen_mask_kernel(const Unit *units, int n_units, const LaunchR
 __global__ void route_units_kernel(const Unit *units, int unit0, int n_units, const LaunchRec *launches,
                                    const PairRec *pairs, const double *Dsh, int n_sh, double tau,
                                    double thresh, int *list32, int *list64, int *counts, int stride,
-                                   int *list_s) {
+                                   int *list_s, const MolCtx *mols = nullptr, const int32_t *launch_mol = nullptr) {
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
@@ -220,11 +257,13 @@ __global__ void route_units_kernel(const Unit *units, int unit0, int n_units, co
         const Unit U = units[unit0 + i];
         const LaunchRec L = launches[U.launch];
         const PairRec bra = pairs[L.bra_pair0 + U.ib];
+        const double *dsh = mols ? mols[launch_mol[U.launch]].Dsh : Dsh;
+        const int nsh = mols ? mols[launch_mol[U.launch]].n_sh : n_sh;
         const int ik = U.k0 + lane;
         bool active = false, low = true;
         if (ik < U.k1) {
             const PairRec ket = pairs[L.ket_pair0 + ik];
-            const double b = six_block_bound(Dsh, n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G);
+            const double b = six_block_bound(dsh, nsh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G);
             active = !(b < tau);
             low = !active || b < thresh;
         }
@@ -257,7 +296,8 @@ __global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units
                                        const PairRec *pairs, const PrimRec *prims, const double *Dsh, int n_sh,
                                        double tau, double thresh, const float *params, float log_thr, int la,
                                        int lb, int lc, int ld, int *list32, int *list64, int *counts,
-                                       int stride, int *list_s) {
+                                       int stride, int *list_s, const MolCtx *mols = nullptr,
+                                       const int32_t *launch_mol = nullptr) {
     __shared__ float sp[kNParams];
     for (int i = threadIdx.x; i < kNParams; i += blockDim.x) sp[i] = params[i];
     __syncthreads();
@@ -268,13 +308,15 @@ __global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units
         const Unit U = units[unit0 + i];
         const LaunchRec L = launches[U.launch];
         const PairRec bra = pairs[L.bra_pair0 + U.ib];
+        const double *dsh = mols ? mols[launch_mol[U.launch]].Dsh : Dsh;
+        const int nsh = mols ? mols[launch_mol[U.launch]].n_sh : n_sh;
         const int ik = U.k0 + lane;
         bool active = false, need = false, reach = true;
         PairRec ket{};
         double dmax = 0.0;
         if (ik < U.k1) {
             ket = pairs[L.ket_pair0 + ik];
-            dmax = six_block_dmax(Dsh, n_sh, bra.a, bra.b, ket.a, ket.b);
+            dmax = six_block_dmax(dsh, nsh, bra.a, bra.b, ket.a, ket.b);
             const double b = __dmul_rn(bra.G, __dmul_rn(ket.G, dmax));
             active = !(b < tau);
             need = active && !(b < thresh);
@@ -2461,3 +2503,285 @@ extern "C" int fjb_fock_build_noalloc(fjb_handle *h, const double *D_dev, double
     CUDA_OK(h, cudaGetLastError());
     return FJB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// the batched build: many planned molecules, one launch per class
+// ---------------------------------------------------------------------------
+
+struct fjb_batch {
+    int device = 0;
+    double tau = 0.0;
+    std::vector<fjb_handle *> mols;
+    DevBuf<PairRec> pairs;
+    DevBuf<PrimRec> prims;
+    DevBuf<LaunchRec> launches;
+    DevBuf<Unit> units;
+    DevBuf<int32_t> launch_mol;
+    DevBuf<MolCtx> ctx;
+    DevBuf<BatchMol> bm;
+    DevBuf<int> sh_off, sh_nc;
+    DevBuf<double> Dsh, Jp, Kp;
+    std::vector<MolCtx> ctx_host;
+    std::vector<BatchMol> bm_host;
+    std::vector<ClassRun> runs;
+    int n_units = 0, max_nsh = 0;
+    size_t max_nn = 0;
+    DevBuf<int> route_list, route_counts;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> cev;
+    bool ready = false;  // densities set
+    std::string err;
+    ~fjb_batch() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        for (auto &e : cev) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+    }
+};
+
+namespace {
+int bfail(fjb_batch *b, int code, const std::string &msg) {
+    if (b) b->err = msg;
+    g_err = msg;
+    return code;
+}
+#define BCUDA_OK(b, x)                                                                         \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess)                                                                 \
+            return bfail((b), FJB_E_CUDA, std::string(#x ": ") + cudaGetErrorString(e_));    \
+    } while (0)
+}  // namespace
+
+extern "C" {
+
+const char *fjb_batch_last_error(const fjb_batch *b) { return b ? b->err.c_str() : g_err.c_str(); }
+
+int fjb_batch_create(fjb_batch **out, fjb_handle *const *handles, int n) {
+    if (!out || !handles || n < 1) return bfail(nullptr, FJB_E_ARG, "fjb_batch_create: no molecules");
+    auto b = std::make_unique<fjb_batch>();
+    b->device = handles[0] ? handles[0]->device : -1;
+    for (int m = 0; m < n; ++m) {
+        fjb_handle *h = handles[m];
+        if (!h || !h->planned || h->device < 0 || h->df)
+            return bfail(nullptr, FJB_E_STATE, "fjb_batch_create: every handle must be a planned device handle");
+        if (h->device != b->device) return bfail(nullptr, FJB_E_ARG, "fjb_batch_create: handles on different devices");
+        if (m == 0) b->tau = h->plan.tau;
+        if (h->plan.tau != b->tau) return bfail(nullptr, FJB_E_ARG, "fjb_batch_create: the plans' tau differ");
+        b->mols.push_back(h);
+    }
+    if (cudaSetDevice(b->device) != cudaSuccess) return bfail(nullptr, FJB_E_CUDA, "cudaSetDevice failed");
+    std::vector<PairRec> pr;
+    std::vector<PrimRec> pm;
+    std::vector<LaunchRec> lr;
+    std::vector<int32_t> lmol;
+    std::map<std::tuple<int, int, int, int>, std::vector<Unit>> by_class;
+    std::map<std::tuple<int, int, int, int>, std::pair<const ClassRun *, std::pair<int, int>>> first;
+    std::vector<int> sh_off, sh_nc;
+    std::vector<int64_t> dsh0, nn0;
+    int64_t dsh_total = 0, nn_total = 0;
+    try {
+        for (int m = 0; m < n; ++m) {
+            fjb_handle *h = b->mols[m];
+            const int P0 = (int)pr.size(), Q0 = (int)pm.size(), L0 = (int)lr.size();
+            std::vector<PrimRec> hp(h->prims.n);
+            if (!hp.empty() &&
+                cudaMemcpy(hp.data(), h->prims.p, hp.size() * sizeof(PrimRec), cudaMemcpyDeviceToHost) != cudaSuccess)
+                return bfail(nullptr, FJB_E_CUDA, "fjb_batch_create: reading a handle's primitive pairs");
+            pm.insert(pm.end(), hp.begin(), hp.end());
+            for (PairRec p : h->pr_host) {
+                p.prim0 += Q0;
+                pr.push_back(p);
+            }
+            for (LaunchRec L : h->lr_host) {
+                L.bra_pair0 += P0;
+                L.ket_pair0 += P0;
+                lr.push_back(L);
+                lmol.push_back(m);
+            }
+            for (const ClassRun &r : h->runs) {
+                const auto key = std::make_tuple(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld);
+                auto &v = by_class[key];
+                for (int u = r.unit0; u < r.unit0 + r.n_units; ++u) {
+                    Unit U = h->units_host[u];
+                    U.launch += L0;
+                    v.push_back(U);
+                }
+                auto it = first.find(key);
+                if (it == first.end())
+                    first[key] = {&r, {r.max_kab, r.max_kcd}};
+                else
+                    it->second.second = {std::max(it->second.second.first, r.max_kab),
+                                         std::max(it->second.second.second, r.max_kcd)};
+            }
+            const int nsh = (int)h->basis.shells.size(), nao = h->basis.n_ao;
+            BatchMol bmh{};
+            bmh.n_sh = nsh;
+            bmh.n_ao = nao;
+            b->bm_host.push_back(bmh);
+            sh_off.insert(sh_off.end(), h->basis.offsets.begin(), h->basis.offsets.begin() + nsh);
+            for (auto &sh : h->basis.shells) sh_nc.push_back((sh.l + 1) * (sh.l + 2) / 2);
+            dsh0.push_back(dsh_total);
+            nn0.push_back(nn_total);
+            dsh_total += (int64_t)nsh * nsh;
+            nn_total += (int64_t)nao * nao;
+            b->max_nsh = std::max(b->max_nsh, nsh);
+            b->max_nn = std::max(b->max_nn, (size_t)nao * nao);
+        }
+        std::vector<Unit> units;
+        for (auto &kv : by_class) {
+            const ClassRun *src = first[kv.first].first;
+            ClassRun r = *src;
+            r.unit0 = (int)units.size();
+            r.n_units = (int)kv.second.size();
+            r.max_kab = first[kv.first].second.first;
+            r.max_kcd = first[kv.first].second.second;
+            units.insert(units.end(), kv.second.begin(), kv.second.end());
+            b->runs.push_back(r);
+        }
+        b->n_units = (int)units.size();
+        b->pairs.upload(pr);
+        b->prims.upload(pm);
+        b->launches.upload(lr);
+        b->units.upload(units);
+        b->launch_mol.upload(lmol);
+        b->sh_off.upload(sh_off);
+        b->sh_nc.upload(sh_nc);
+        b->Dsh.alloc(std::max<int64_t>(1, dsh_total));
+        b->Jp.alloc(std::max<int64_t>(1, nn_total));
+        b->Kp.alloc(std::max<int64_t>(1, nn_total));
+        int sh0 = 0;
+        for (int m = 0; m < n; ++m) {
+            BatchMol &x = b->bm_host[m];
+            x.Dsh = b->Dsh.p + dsh0[m];
+            x.sh_off = b->sh_off.p + sh0;
+            x.sh_nc = b->sh_nc.p + sh0;
+            x.Jp = b->Jp.p + nn0[m];
+            x.Kp = b->Kp.p + nn0[m];
+            sh0 += x.n_sh;
+            b->ctx_host.push_back(MolCtx{nullptr, x.Dsh, b->Jp.p + nn0[m], b->Kp.p + nn0[m], x.n_ao, x.n_sh});
+        }
+        b->ctx.alloc(n);
+        b->bm.alloc(n);
+        b->route_list.alloc(std::max<size_t>(1, 2 * (size_t)b->n_units));
+        b->route_counts.alloc(std::max<size_t>(1, 4 * b->runs.size()));
+    } catch (const std::exception &e) {
+        return bfail(nullptr, FJB_E_CUDA, std::string("fjb_batch_create: ") + e.what());
+    }
+    for (auto &r : b->runs) {
+        choose_rys(1, r);
+        r.grid = run_grid(r);
+        r.grid32 = run_grid32(r);
+        if (!r.compiled && !r.rys64)
+            return bfail(nullptr, FJB_E_LIMIT, "fjb_batch_create: a class has neither a register nor a Rys kernel");
+        cudaEvent_t e0, e1;
+        if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+            return bfail(nullptr, FJB_E_CUDA, "cudaEventCreate failed");
+        b->cev.emplace_back(e0, e1);
+    }
+    if (cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+        return bfail(nullptr, FJB_E_CUDA, "cudaEventCreate failed");
+    *out = b.release();
+    return FJB_OK;
+}
+
+void fjb_batch_destroy(fjb_batch *b) { delete b; }
+
+int fjb_batch_set_densities(fjb_batch *b, const double *const *D_dev, double *const *J_dev, double *const *K_dev,
+                            double *const *G_dev) {
+    if (!b || !D_dev) return bfail(b, FJB_E_ARG, "null argument");
+    BCUDA_OK(b, cudaSetDevice(b->device));
+    const size_t n = b->mols.size();
+    for (size_t m = 0; m < n; ++m) {
+        if (!D_dev[m]) return bfail(b, FJB_E_ARG, "fjb_batch_set_densities: a null density");
+        b->ctx_host[m].D = D_dev[m];
+        b->bm_host[m].D = D_dev[m];
+        b->bm_host[m].J = J_dev ? J_dev[m] : nullptr;
+        b->bm_host[m].K = K_dev ? K_dev[m] : nullptr;
+        b->bm_host[m].G = G_dev ? G_dev[m] : nullptr;
+    }
+    BCUDA_OK(b, cudaMemcpy(b->ctx.p, b->ctx_host.data(), n * sizeof(MolCtx), cudaMemcpyHostToDevice));
+    BCUDA_OK(b, cudaMemcpy(b->bm.p, b->bm_host.data(), n * sizeof(BatchMol), cudaMemcpyHostToDevice));
+    b->ready = true;
+    return FJB_OK;
+}
+
+int fjb_batch_build(fjb_batch *b, int precision, double threshold, void *stream) {
+    if (!b) return bfail(b, FJB_E_ARG, "null batch");
+    if (!b->ready) return bfail(b, FJB_E_STATE, "fjb_batch_build: set the densities first (fjb_batch_set_densities)");
+    if (precision != FJB_FP64 && precision != FJB_ROUTED)
+        return bfail(b, FJB_E_ARG, "fjb_batch_build: precision FJB_FP64 or FJB_ROUTED");
+    const double route = precision == FJB_ROUTED ? (threshold > 0.0 ? threshold : 1e-9) : 0.0;
+    BCUDA_OK(b, cudaSetDevice(b->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned nm = (unsigned)b->mols.size();
+    batch_density_blocks_kernel<<<dim3((unsigned)((b->max_nsh * b->max_nsh + 255) / 256), nm), 256, 0, st>>>(b->bm.p);
+    BCUDA_OK(b, cudaMemsetAsync(b->Jp.p, 0, b->Jp.n * sizeof(double), st));
+    BCUDA_OK(b, cudaMemsetAsync(b->Kp.p, 0, b->Kp.n * sizeof(double), st));
+    const bool routed = route > 0.0;
+    if (routed) BCUDA_OK(b, cudaMemsetAsync(b->route_counts.p, 0, b->route_counts.n * sizeof(int), st));
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    BCUDA_OK(b, cudaStreamIsCapturing(st, &cap));
+    const unsigned ev_flags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
+    BCUDA_OK(b, cudaEventRecordWithFlags(b->ev0, st, ev_flags));
+    const fjb_handle *h0 = b->mols[0];
+    for (size_t ri = 0; ri < b->runs.size(); ++ri) {
+        const ClassRun &r = b->runs[ri];
+        BCUDA_OK(b, cudaEventRecordWithFlags(b->cev[ri].first, st, ev_flags));
+        KArgs a{};
+        a.C = r.dev;
+        a.units = b->units.p + r.unit0;
+        a.n_units = r.n_units;
+        a.launches = b->launches.p;
+        a.pairs = b->pairs.p;
+        a.prims = b->prims.p;
+        a.tau = b->tau;
+        a.boys_tab = h0->boys.p;
+        a.mols = b->ctx.p;
+        a.launch_mol = b->launch_mol.p;
+        if (routed) {
+            if (!r.has32 && !r.rys32)
+                return bfail(b, FJB_E_LIMIT, "fjb_batch_build: a class has no FP32 kernel for routed units");
+            int *l32 = b->route_list.p + r.unit0;
+            int *l64 = b->route_list.p + b->n_units + r.unit0;
+            int *cnt = b->route_counts.p + 4 * ri;
+            const int rgrid = std::max(1, std::min((r.n_units + 3) / 4, 16 * sm_count()));
+            route_units_kernel<<<rgrid, 128, 0, st>>>(b->units.p, r.unit0, r.n_units, b->launches.p, b->pairs.p,
+                                                      nullptr, 0, b->tau, route, l32, l64, cnt, 0, nullptr,
+                                                      b->ctx.p, b->launch_mol.p);
+            KArgs a32 = a, a64 = a;
+            a32.unit_list = l32;
+            a32.unit_count = cnt;
+            a64.unit_list = l64;
+            a64.unit_count = cnt + 1;
+            BCUDA_OK(b, launch_run32(r, st, a32));
+            BCUDA_OK(b, launch_run(r, st, a64));
+        } else {
+            BCUDA_OK(b, launch_run(r, st, a));
+        }
+        BCUDA_OK(b, cudaEventRecordWithFlags(b->cev[ri].second, st, ev_flags));
+    }
+    BCUDA_OK(b, cudaEventRecordWithFlags(b->ev1, st, ev_flags));
+    const unsigned cx = (unsigned)std::min<size_t>((b->max_nn + 255) / 256, 1024);
+    batch_close_kernel<<<dim3(cx, nm), 256, 0, st>>>(b->bm.p);
+    BCUDA_OK(b, cudaGetLastError());
+    return FJB_OK;
+}
+
+int fjb_batch_stats(const fjb_batch *bc, double *ms, int64_t *n_classes, int64_t *n_units) {
+    fjb_batch *b = const_cast<fjb_batch *>(bc);
+    if (!b) return bfail(b, FJB_E_ARG, "null batch");
+    if (n_classes) *n_classes = (int64_t)b->runs.size();
+    if (n_units) *n_units = b->n_units;
+    if (ms) {
+        float f = 0.f;
+        BCUDA_OK(b, cudaEventSynchronize(b->ev1));
+        BCUDA_OK(b, cudaEventElapsedTime(&f, b->ev0, b->ev1));
+        *ms = f;
+    }
+    return FJB_OK;
+}
+
+}  // extern "C"

@@ -79,8 +79,9 @@ __device__ __forceinline__ double warp_sum(double v) {
 // The primitive loop, the HRR and the digest of one quartet in recurrence
 // type R.  jab[] collects this lane's share of the bra block (FP64).
 template <int LA, int LB, int LC, int LD, typename R>
-__device__ __forceinline__ void quartet_compiled(const KArgs &A, const PairRec &bra, const PairRec &ket,
-                                                 double deg, double *jab, double *wq, int wstride) {
+__device__ __forceinline__ void quartet_compiled(const KArgs &A, const MolCtx &M, const PairRec &bra,
+                                                 const PairRec &ket, double deg, double *jab, double *wq,
+                                                 int wstride) {
     using H = HgpCode<LA, LB, LC, LD>;
     constexpr int NA = cnc(LA), NB = cnc(LB), NC = cnc(LC), ND = cnc(LD);
     constexpr int NAB = NA * NB, NCD = NC * ND, L = LA + LB + LC + LD;
@@ -135,30 +136,30 @@ __device__ __forceinline__ void quartet_compiled(const KArgs &A, const PairRec &
     H::template hrr<R>(acc, cb, ck, eri);
 
     // the six-block digest, FP64
-    const int n_ao = A.n_ao;
+    const int n_ao = M.n_ao;
     const int oa = bra.ao_a, ob = bra.ao_b, oc = ket.ao_a, od = ket.ao_b;
     double dab[NAB], dcd[NCD], dac[NA * NC], dad[NA * ND], dbc[NB * NC], dbd[NB * ND];
 #pragma unroll
     for (int i = 0; i < NA; ++i)
 #pragma unroll
-        for (int j = 0; j < NB; ++j) dab[i * NB + j] = __ldg(A.D + (size_t)(oa + i) * n_ao + ob + j);
+        for (int j = 0; j < NB; ++j) dab[i * NB + j] = __ldg(M.D + (size_t)(oa + i) * n_ao + ob + j);
 #pragma unroll
     for (int i = 0; i < NC; ++i)
 #pragma unroll
-        for (int j = 0; j < ND; ++j) dcd[i * ND + j] = __ldg(A.D + (size_t)(oc + i) * n_ao + od + j);
+        for (int j = 0; j < ND; ++j) dcd[i * ND + j] = __ldg(M.D + (size_t)(oc + i) * n_ao + od + j);
 #pragma unroll
     for (int i = 0; i < NA; ++i) {
 #pragma unroll
-        for (int j = 0; j < NC; ++j) dac[i * NC + j] = __ldg(A.D + (size_t)(oa + i) * n_ao + oc + j);
+        for (int j = 0; j < NC; ++j) dac[i * NC + j] = __ldg(M.D + (size_t)(oa + i) * n_ao + oc + j);
 #pragma unroll
-        for (int j = 0; j < ND; ++j) dad[i * ND + j] = __ldg(A.D + (size_t)(oa + i) * n_ao + od + j);
+        for (int j = 0; j < ND; ++j) dad[i * ND + j] = __ldg(M.D + (size_t)(oa + i) * n_ao + od + j);
     }
 #pragma unroll
     for (int i = 0; i < NB; ++i) {
 #pragma unroll
-        for (int j = 0; j < NC; ++j) dbc[i * NC + j] = __ldg(A.D + (size_t)(ob + i) * n_ao + oc + j);
+        for (int j = 0; j < NC; ++j) dbc[i * NC + j] = __ldg(M.D + (size_t)(ob + i) * n_ao + oc + j);
 #pragma unroll
-        for (int j = 0; j < ND; ++j) dbd[i * ND + j] = __ldg(A.D + (size_t)(ob + i) * n_ao + od + j);
+        for (int j = 0; j < ND; ++j) dbd[i * ND + j] = __ldg(M.D + (size_t)(ob + i) * n_ao + od + j);
     }
     double jcd[NCD], kac[NA * NC], kad[NA * ND], kbc[NB * NC], kbd[NB * ND];
 #pragma unroll
@@ -209,20 +210,20 @@ __device__ __forceinline__ void quartet_compiled(const KArgs &A, const PairRec &
 #pragma unroll
     for (int kk = 0; kk < NC; ++kk)
 #pragma unroll
-        for (int l = 0; l < ND; ++l) atomicAdd(A.Jp + (size_t)(oc + kk) * n_ao + od + l, w2 * jcd[kk * ND + l]);
+        for (int l = 0; l < ND; ++l) atomicAdd(M.Jp + (size_t)(oc + kk) * n_ao + od + l, w2 * jcd[kk * ND + l]);
 #pragma unroll
     for (int i = 0; i < NA; ++i) {
 #pragma unroll
-        for (int kk = 0; kk < NC; ++kk) atomicAdd(A.Kp + (size_t)(oa + i) * n_ao + oc + kk, deg * kac[i * NC + kk]);
+        for (int kk = 0; kk < NC; ++kk) atomicAdd(M.Kp + (size_t)(oa + i) * n_ao + oc + kk, deg * kac[i * NC + kk]);
 #pragma unroll
-        for (int l = 0; l < ND; ++l) atomicAdd(A.Kp + (size_t)(oa + i) * n_ao + od + l, deg * kad[i * ND + l]);
+        for (int l = 0; l < ND; ++l) atomicAdd(M.Kp + (size_t)(oa + i) * n_ao + od + l, deg * kad[i * ND + l]);
     }
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
 #pragma unroll
-        for (int kk = 0; kk < NC; ++kk) atomicAdd(A.Kp + (size_t)(ob + j) * n_ao + oc + kk, deg * kbc[j * NC + kk]);
+        for (int kk = 0; kk < NC; ++kk) atomicAdd(M.Kp + (size_t)(ob + j) * n_ao + oc + kk, deg * kbc[j * NC + kk]);
 #pragma unroll
-        for (int l = 0; l < ND; ++l) atomicAdd(A.Kp + (size_t)(ob + j) * n_ao + od + l, deg * kbd[j * ND + l]);
+        for (int l = 0; l < ND; ++l) atomicAdd(M.Kp + (size_t)(ob + j) * n_ao + od + l, deg * kbd[j * ND + l]);
     }
 }
 
@@ -245,12 +246,13 @@ __global__ void __launch_bounds__(128) hgp_compiled_kernel(const KArgs A) {
         const Unit U = A.units[u];
         const LaunchRec LR = A.launches[U.launch];
         const PairRec bra = A.pairs[LR.bra_pair0 + U.ib];
+        const MolCtx M = mol_of(A, U.launch);
         const int ik = U.k0 + lane;
         bool active = ik < U.k1;
         PairRec ket{};
         if (active) {
             ket = A.pairs[LR.ket_pair0 + ik];
-            active = !skip6(A.Dsh, A.n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G, A.tau);
+            active = !skip6(M.Dsh, M.n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G, A.tau);
         }
         const unsigned mask = __ballot_sync(0xffffffffu, active);
         if (!mask) continue;
@@ -264,7 +266,7 @@ __global__ void __launch_bounds__(128) hgp_compiled_kernel(const KArgs A) {
             constexpr int NC = cnc(LC), ND = cnc(LD);
             constexpr int S5 = NC * ND + NA * NC + NA * ND + NB * NC + NB * ND;
             double *wq = A.W ? ket_slots(A, U.launch, LR.n_ket, U.ib, ik, NAB, S5) : nullptr;
-            quartet_compiled<LA, LB, LC, LD, R>(A, bra, ket, deg, jab, wq, LR.n_ket);
+            quartet_compiled<LA, LB, LC, LD, R>(A, M, bra, ket, deg, jab, wq, LR.n_ket);
         }
 #pragma unroll
         for (int t = 0; t < NAB; ++t) {
@@ -272,7 +274,7 @@ __global__ void __launch_bounds__(128) hgp_compiled_kernel(const KArgs A) {
             if (A.W) {
                 if (lane == 0) A.wab[A.wab_off[u] + t] = v;  // the unit's partial, reduced in unit order
             } else if (lane == 0 && v != 0.0) {
-                atomicAdd(A.Jp + (size_t)(bra.ao_a + t / NB) * A.n_ao + bra.ao_b + t % NB, v);
+                atomicAdd(M.Jp + (size_t)(bra.ao_a + t / NB) * M.n_ao + bra.ao_b + t % NB, v);
             }
         }
     }

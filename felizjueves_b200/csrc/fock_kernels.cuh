@@ -22,6 +22,15 @@
 
 namespace fjb {
 
+// One molecule's density, shell-block maxima and accumulators: the batched
+// build (fjb_batch_build) runs many molecules' units in one launch per class
+// and each unit finds its molecule through its launch.
+struct MolCtx {
+    const double *D, *Dsh;
+    double *Jp, *Kp;
+    int n_ao, n_sh;
+};
+
 struct KArgs {
     ClassDev C;
     const Unit *units;
@@ -50,7 +59,16 @@ struct KArgs {
     // the Rys kernel (rys_fock.cuh): its layout and the tabulated rule
     RysDev Y;
     const double *rys_tab;
+    // the batched build: per molecule its context, per launch its molecule
+    // (null: one molecule, the fields above)
+    const MolCtx *mols;
+    const int32_t *launch_mol;
 };
+
+__device__ __forceinline__ MolCtx mol_of(const KArgs &A, int launch) {
+    if (A.mols) return A.mols[A.launch_mol[launch]];
+    return MolCtx{A.D, A.Dsh, A.Jp, A.Kp, A.n_ao, A.n_sh};
+}
 
 // A quartet's first ket-block slot (block element 0) in the atomics-free
 // build: bra pair ib, ket position ik of launch `launch`; element e of the

@@ -27,8 +27,8 @@ bool layout_one(int max_kab, int max_kcd, int rsize, int budget, RysDev *o) {
                           dd((long)G * kPrimWords * max_kcd) + rd((long)G * S::NCK, rsize) + dd((long)G * S::N5) +
                           rd((long)G * S::NAB * S::XS, rsize);
         for (int P = K; P >= 1; --P) {
-            const int tsp = rsize == 8 ? S::template tsp<double>() : S::template tsp<float>();
-            const int tabs = rd(std::max((long)G * P * S::NR * 3 * tsp, (long)G * S::NAB * S::YS), rsize);
+            const int kst = rsize == 8 ? S::template kstride<double>(P) : S::template kstride<float>(P);
+            const int tabs = rd(std::max((long)G * kst, (long)G * S::NAB * S::YS), rsize);
             if (fixed + tabs > budget) continue;
             o->group = G;
             o->chunk = P;

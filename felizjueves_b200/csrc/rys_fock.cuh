@@ -151,14 +151,27 @@ struct Shape {
     static constexpr int NR = (E + F) / 2 + 1;  // Rys roots
     static constexpr int TS = (E + 1) * (F + 1);  // one axis' 2D table
     // the tables as stored: per axis F+1 rows (ket index k), each the E+1
-    // values of the bra index padded to whole 16-byte vectors
+    // values of the bra index padded to whole 16-byte vectors (rp); rows
+    // rps apart, an odd number of 16-byte vectors, so that the rows of
+    // up to eight different k fall in different banks
     template <typename R>
     __host__ __device__ static constexpr int rp() {
         return ((E + 1) * (int)sizeof(R) + 15) / 16 * 16 / (int)sizeof(R);
     }
     template <typename R>
+    __host__ __device__ static constexpr int rps() {
+        return ((((E + 1) * (int)sizeof(R) + 15) / 16) | 1) * 16 / (int)sizeof(R);
+    }
+    template <typename R>
     __host__ __device__ static constexpr int tsp() {
-        return (F + 1) * rp<R>();
+        return (F + 1) * rps<R>();
+    }
+    // one ket's tables for a chunk of P primitive quartets, padded to an odd
+    // number of 16-byte vectors so that different kets' rows do not share
+    // banks
+    template <typename R>
+    __host__ __device__ static constexpr int kstride(int P) {
+        return P * NR * 3 * tsp<R>() + (((P * NR * 3 * tsp<R>() * (int)sizeof(R) / 16) & 1) ? 0 : 16 / (int)sizeof(R));
     }
     static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     static constexpr int NAB = NA * NB, NCD = NC * ND;
@@ -281,7 +294,7 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
     rys_fock_kernel(const KArgs A) {
     using S = rys::Shape<LA, LB, LC, LD>;
     constexpr int E = S::E, F = S::F, NR = S::NR;
-    constexpr int RP = S::template rp<R>(), TSP = S::template tsp<R>();
+    constexpr int RP = S::template rp<R>(), RPS = S::template rps<R>(), TSP = S::template tsp<R>();
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND, NAB = S::NAB, NCD = S::NCD;
     constexpr int NBE = S::NBE, NBF = S::NBF, NCB = S::NCB, NCK = S::NCK, XS = S::XS, YS = S::YS;
     constexpr int N5 = S::N5;
@@ -315,7 +328,7 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
     R *X = reinterpret_cast<R *>(sm + L.sm_X);
     const int tid = threadIdx.x;
     const int G = L.group, P = L.chunk;
-    const int n_ao = A.n_ao;
+    const int KSTR = S::template kstride<R>(P);
     const int n_todo = A.unit_list ? *A.unit_count : A.n_units;
 
     for (int ui = blockIdx.x; ui < n_todo; ui += gridDim.x) {
@@ -323,6 +336,8 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
         const Unit U = A.units[u];
         const LaunchRec LR = A.launches[U.launch];
         const PairRec bra = A.pairs[LR.bra_pair0 + U.ib];
+        const MolCtx M = mol_of(A, U.launch);
+        const int n_ao = M.n_ao;
         const int kab = bra.nprim;
         const int oa = bra.ao_a, ob = bra.ao_b;
         {
@@ -331,7 +346,7 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
         }
         for (int i = tid; i < NCB; i += NT) cb[i] = rys::hrr_coef<LB, R>(i, bra.AB);
         for (int i = tid; i < NAB; i += NT) {
-            Dab[i] = A.D[(size_t)(oa + i / NB) * n_ao + ob + i % NB];
+            Dab[i] = M.D[(size_t)(oa + i / NB) * n_ao + ob + i % NB];
             Jab[i] = 0.0;
         }
         if (tid < 32) {
@@ -339,7 +354,7 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
             bool on = false;
             if (ik < U.k1) {
                 const PairRec ket = A.pairs[LR.ket_pair0 + ik];
-                on = !skip6(A.Dsh, A.n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G, A.tau);
+                on = !skip6(M.Dsh, M.n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G, A.tau);
             }
             const unsigned m = __ballot_sync(0xffffffffu, on);
             if (on) {
@@ -385,7 +400,7 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
                     const int r = o - NCD - NA * NC - NA * ND - NB * NC;
                     at = (size_t)(ob + r / ND) * n_ao + od + r % ND;
                 }
-                Dk[i] = A.D[at];
+                Dk[i] = M.D[at];
             }
             if (tid < ng) {
                 const int ik = s_ket[g0 + tid];
@@ -420,7 +435,7 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
                     rys::rule_root<NR>(r, T, A.rys_tab, &x, &w);
                     const double seedw = pb[7] * pk[7] * kTwoOverSqrtPi * sqrt(rho) * w;
                     const double b00 = 0.5 * inv * x, b10 = pb[8] * (1.0 - qi * x), b01 = pk[8] * (1.0 - pi * x);
-                    R *out = tab + ((size_t)(g * P + tl) * NR + r) * (3 * TSP);
+                    R *out = tab + (size_t)g * KSTR + (size_t)(tl * NR + r) * (3 * TSP);
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         const double c00 = pb[3 + d] - qi * PQ[d] * x, c00p = pk[3 + d] + pi * PQ[d] * x;
@@ -441,20 +456,20 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
 #pragma unroll
                         for (int i = 0; i <= E; ++i)
 #pragma unroll
-                            for (int k = 0; k <= F; ++k) out[d * TSP + k * RP + i] = (R)I[i][k];
+                            for (int k = 0; k <= F; ++k) out[d * TSP + k * RPS + i] = (R)I[i][k];
                     }
                 }
                 __syncthreads();
                 if (item) {
                     for (int tl = 0; tl < np; ++tl) {
-                        const R *base = tab + (size_t)(gme * P + tl) * NR * (3 * TSP);
+                        const R *base = tab + (size_t)gme * KSTR + (size_t)tl * NR * (3 * TSP);
 #pragma unroll
                         for (int r = 0; r < NR; ++r) {
                             const R *Ix = base + r * (3 * TSP), *Iy = Ix + TSP, *Iz = Iy + TSP;
                             R ix[RP], iy[RP], iz[RP];
-                            rys::ld_row<R, RP>(Ix + fx * RP, ix);
-                            rys::ld_row<R, RP>(Iy + fy * RP, iy);
-                            rys::ld_row<R, RP>(Iz + fz * RP, iz);
+                            rys::ld_row<R, RP>(Ix + fx * RPS, ix);
+                            rys::ld_row<R, RP>(Iy + fy * RPS, iy);
+                            rys::ld_row<R, RP>(Iz + fz * RPS, iz);
                             R pxy[E + 1][E + 1];
 #pragma unroll
                             for (int a = 0; a <= E; ++a)
@@ -551,7 +566,7 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
                     const int c = o / ND, d = o - c * ND;
 #pragma unroll
                     for (int ab = 0; ab < NAB; ++ab) acc2 += Dab[ab] * (double)Y[ab * YS + o];
-                    atomicAdd(A.Jp + (size_t)(oc + c) * n_ao + od + d, 2.0 * deg * acc2);
+                    atomicAdd(M.Jp + (size_t)(oc + c) * n_ao + od + d, 2.0 * deg * acc2);
                 } else if (o < NCD + NA * NC) {
                     const int r = o - NCD, a = r / NC, c = r - a * NC;
                     const double *dbd = dk + NCD + NA * NC + NA * ND + NB * NC;
@@ -559,7 +574,7 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
                     for (int b = 0; b < NB; ++b)
 #pragma unroll
                         for (int d = 0; d < ND; ++d) acc2 += dbd[b * ND + d] * (double)Y[(a * NB + b) * YS + c * ND + d];
-                    atomicAdd(A.Kp + (size_t)(oa + a) * n_ao + oc + c, deg * acc2);
+                    atomicAdd(M.Kp + (size_t)(oa + a) * n_ao + oc + c, deg * acc2);
                 } else if (o < NCD + NA * NC + NA * ND) {
                     const int r = o - NCD - NA * NC, a = r / ND, d = r - a * ND;
                     const double *dbc = dk + NCD + NA * NC + NA * ND;
@@ -567,7 +582,7 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
                     for (int b = 0; b < NB; ++b)
 #pragma unroll
                         for (int c = 0; c < NC; ++c) acc2 += dbc[b * NC + c] * (double)Y[(a * NB + b) * YS + c * ND + d];
-                    atomicAdd(A.Kp + (size_t)(oa + a) * n_ao + od + d, deg * acc2);
+                    atomicAdd(M.Kp + (size_t)(oa + a) * n_ao + od + d, deg * acc2);
                 } else if (o < NCD + NA * NC + NA * ND + NB * NC) {
                     const int r = o - NCD - NA * NC - NA * ND, b = r / NC, c = r - b * NC;
                     const double *dad = dk + NCD + NA * NC;
@@ -575,7 +590,7 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
                     for (int a = 0; a < NA; ++a)
 #pragma unroll
                         for (int d = 0; d < ND; ++d) acc2 += dad[a * ND + d] * (double)Y[(a * NB + b) * YS + c * ND + d];
-                    atomicAdd(A.Kp + (size_t)(ob + b) * n_ao + oc + c, deg * acc2);
+                    atomicAdd(M.Kp + (size_t)(ob + b) * n_ao + oc + c, deg * acc2);
                 } else {
                     const int r = o - NCD - NA * NC - NA * ND - NB * NC, b = r / ND, d = r - b * ND;
                     const double *dac = dk + NCD;
@@ -583,13 +598,13 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
                     for (int a = 0; a < NA; ++a)
 #pragma unroll
                         for (int c = 0; c < NC; ++c) acc2 += dac[a * NC + c] * (double)Y[(a * NB + b) * YS + c * ND + d];
-                    atomicAdd(A.Kp + (size_t)(ob + b) * n_ao + od + d, deg * acc2);
+                    atomicAdd(M.Kp + (size_t)(ob + b) * n_ao + od + d, deg * acc2);
                 }
             }
             __syncthreads();
         }
         for (int i = tid; i < NAB; i += NT)
-            if (Jab[i] != 0.0) atomicAdd(A.Jp + (size_t)(oa + i / NB) * n_ao + ob + i % NB, Jab[i]);
+            if (Jab[i] != 0.0) atomicAdd(M.Jp + (size_t)(oa + i / NB) * n_ao + ob + i % NB, Jab[i]);
         if (A.computed && tid == 0 && n_list) atomicAdd(A.computed + U.launch, (unsigned long long)n_list);
         __syncthreads();
     }

@@ -114,34 +114,52 @@ class DFEngine:
         import torch
         A, X = self.basis, self.aux
         na, nx = len(A.shells), len(X.shells)
-        items = np.array([(a, b, p) for a in range(na) for b in range(a, na) for p in range(nx)],
-                         np.int32)
+        a_i, b_i = np.triu_indices(na)
+        items = np.stack([np.repeat(a_i, nx), np.repeat(b_i, nx), np.tile(np.arange(nx), len(a_i))],
+                         axis=1).astype(np.int32)
         out, off = self._blocks(FJB_DF_ERI3, items)
-        m_idx, n_idx, p_idx = [], [], []
-        for (a, b, p) in items:
-            sa, sb, sp = A.shells[a].n_cart, A.shells[b].n_cart, X.shells[p].n_cart
-            i, j, k = np.meshgrid(np.arange(sa), np.arange(sb), np.arange(sp), indexing="ij")
-            m_idx.append(A.offsets[a] + i.ravel())
-            n_idx.append(A.offsets[b] + j.ravel())
-            p_idx.append(X.offsets[p] + k.ravel())
-        mi = torch.as_tensor(np.concatenate(m_idx), device=out.device)
-        ni = torch.as_tensor(np.concatenate(n_idx), device=out.device)
-        pi = torch.as_tensor(np.concatenate(p_idx), device=out.device)
+        nc_a = np.array([s.n_cart for s in A.shells])
+        nc_x = np.array([s.n_cart for s in X.shells])
+        oA, oX = np.asarray(A.offsets), np.asarray(X.offsets)
+        sa, sb, sp = nc_a[items[:, 0]], nc_a[items[:, 1]], nc_x[items[:, 2]]
         T = torch.zeros((A.n_ao, A.n_ao, X.n_ao), dtype=torch.float64, device=out.device)
-        vals = out[: len(mi)]
-        T.index_put_((ni, mi, pi), vals)
-        T.index_put_((mi, ni, pi), vals)
+        Tf = T.view(-1)
+        dev = out.device
+        # one vectorised scatter per block shape (sa, sb, sp)
+        for shape in set(zip(sa.tolist(), sb.tolist(), sp.tolist())):
+            g = np.nonzero((sa == shape[0]) & (sb == shape[1]) & (sp == shape[2]))[0]
+            i, j, k = (x.ravel() for x in np.meshgrid(np.arange(shape[0]), np.arange(shape[1]),
+                                                      np.arange(shape[2]), indexing="ij"))
+            m = torch.as_tensor(oA[items[g, 0]][:, None] + i[None, :], device=dev)
+            n_ = torch.as_tensor(oA[items[g, 1]][:, None] + j[None, :], device=dev)
+            p = torch.as_tensor(oX[items[g, 2]][:, None] + k[None, :], device=dev)
+            src = torch.as_tensor(off[g][:, None] + np.arange(len(i))[None, :], device=dev)
+            vals = out[src]
+            nx_ao, n_ao = X.n_ao, A.n_ao
+            Tf[(n_ * n_ao + m) * nx_ao + p] = vals
+            Tf[(m * n_ao + n_) * nx_ao + p] = vals
         return T
 
     def factors(self):
-        """B = (mn|P) L^{-T} as (n_aux, n_ao, n_ao), FP64."""
+        """B = (mn|P) L^{-T} as (n_aux, n_ao, n_ao), FP64, L the metric's
+        Cholesky factor.  When the metric is numerically singular (an
+        even-tempered aux set on close atoms is nearly linearly dependent
+        and the Cholesky breaks down), the factors come from its eigenvectors
+        instead: B = Lambda^{-1/2} U^T (P|mn) over the eigenvalues above
+        1e-12 of the largest (canonical orthogonalisation), with fewer rows
+        than n_aux."""
         import torch
         V = self.metric()
-        L = torch.linalg.cholesky(V)
         T = self.eri3().reshape(self.basis.n_ao ** 2, self.aux.n_ao)
-        B = torch.linalg.solve_triangular(L, T.T, upper=False)  # L^{-1} T^T
         n = self.basis.n_ao
-        return B.reshape(self.aux.n_ao, n, n)
+        try:
+            L = torch.linalg.cholesky(V)
+            B = torch.linalg.solve_triangular(L, T.T, upper=False)  # L^{-1} T^T
+        except torch.linalg.LinAlgError:
+            w, U = torch.linalg.eigh(V)
+            keep = w > 1e-12 * w.max()
+            B = (U[:, keep] / torch.sqrt(w[keep])).T @ T.T
+        return B.reshape(-1, n, n).contiguous()
 
     def jk(self, D, mode: str = "fp64", B=None):
         """(J, K) of the density D (torch, cuda, FP64) by density fitting."""

@@ -339,6 +339,29 @@ int fjb_set_class_config32(fjb_handle *h, int la, int lb, int lc, int ld, int th
  * kernels. */
 int fjb_set_rys(fjb_handle *h, int mode);
 
+/* The batched build: many molecules, each a planned handle (same device,
+ * same tau), built together with ONE launch per angular-momentum class --
+ * every molecule's work units of that class in one class-sorted queue, each
+ * unit finding its molecule's density and accumulators through its launch
+ * -- plus one launch for all molecules' density blocks and one for their
+ * closing.  The batch reads the handles' plans when it is made (they must
+ * outlive it); fjb_batch_set_densities binds each molecule's DEVICE D and
+ * its J, K, G outputs (any may be NULL) once, fjb_batch_build then runs and
+ * is stream-ordered and capturable (FJB_FP64, or FJB_ROUTED with the
+ * Schwarz x density bound router; the budget check and the learned router
+ * are single-molecule features).  No counterpart in the reference, whose
+ * launches are per molecule (eri/fock/walk_f.py:306). */
+typedef struct fjb_batch fjb_batch;
+int fjb_batch_create(fjb_batch **out, fjb_handle *const *handles, int n);
+int fjb_batch_set_densities(fjb_batch *b, const double *const *D_dev, double *const *J_dev,
+                            double *const *K_dev, double *const *G_dev);
+int fjb_batch_build(fjb_batch *b, int precision, double threshold, void *stream);
+/* Device milliseconds of the last batch build's class launches, the number
+ * of class launches and of work units. */
+int fjb_batch_stats(const fjb_batch *b, double *ms, int64_t *n_classes, int64_t *n_units);
+const char *fjb_batch_last_error(const fjb_batch *b);
+void fjb_batch_destroy(fjb_batch *b);
+
 /* Density-fitted J and K of the symmetric density D (DEVICE, n_ao^2) from
  * the factors B (DEVICE, n_aux x n_ao x n_ao, FP64: B_P = sum_Q (L^-1)_PQ
  * (Q|mn), L the Cholesky factor of the metric (P|Q)).  J_mn = sum_P B_P,mn
