@@ -101,38 +101,75 @@ __device__ __forceinline__ void split3(double v, __nv_bfloat16 *h, __nv_bfloat16
 }
 
 // The split operand of a GEMM, rows x cols (cols = the contraction index),
-// written K-major into three BF16 arrays of leading dimension ldp (>= cols,
-// a multiple of kMmK) and rows_p rows (a multiple of kMmTile); the padding
-// is zero.  Element (r, c) of the source:
+// written into three BF16 arrays of rows_p rows (a multiple of kMmTile) and
+// ldp columns (a multiple of kMmK), zero-padded, in TILE order: the 128 x 64
+// tile (row tile rt, K tile kt) is 16 KiB at ((rt * ldp / 64) + kt) * 8192
+// elements, laid out exactly as the MMA reads it from shared memory (the
+// canonical K-major no-swizzle layout: element (r, k) of the tile at
+// (r / 8) * 512 + (k / 8) * 64 + (r % 8) * 8 + k % 8), so that a tile is
+// staged by one contiguous bulk copy.  Element (r, c) of the source:
 //   mode 0: src[r * ld + c]
 //   mode 1: src[(c / n) * n * n + r * n + c % n]  (the aux-batched
 //           transpose: row r of every n x n block q, side by side)
 __global__ void df_split_kernel(const double *__restrict__ src, int mode, long long rows, long long cols,
                                 long long ld, long long n, long long rows_p, long long ldp, __nv_bfloat16 *hi,
                                 __nv_bfloat16 *mid, __nv_bfloat16 *lo) {
-    const long long total = rows_p * ldp;
+    const long long total = rows_p * ldp, kts = ldp / kMmK;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const long long r = i / ldp, c = i - r * ldp;
+        const long long tile = i >> 13, w = i & 8191;
+        const long long rt = tile / kts, kt = tile - rt * kts;
+        const int rem = (int)(w & 511), r8 = (int)(w >> 9);
+        const long long r = rt * kMmTile + r8 * 8 + ((rem & 63) >> 3);
+        const long long c = kt * kMmK + (rem >> 6) * 8 + (rem & 7);
         double v = 0.0;
         if (r < rows && c < cols) v = mode == 0 ? src[r * ld + c] : src[(c / n) * n * n + r * n + c % n];
         split3(v, hi + i, mid + i, lo + i);
     }
 }
 
+namespace {
+
+// One bulk (non-tensor) TMA copy global -> shared, completing on `bar`.
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+constexpr int kStages = 2;
+constexpr int kStageBytes = 6 * kPartBytes;  // A0 A1 A2 B0 B1 B2
+
+}  // namespace
+
 // C[M x N] (FP64, leading dimension ldc) = sum over the six split products
-// of A (rows_p x ldp, K-major) and B (cols_p x ldp, K-major): C = A B^T.
+// of A (rows_p x ldp) and B (cols_p x ldp), both in tile order: C = A B^T,
+// over this CTA's K tiles [z kt_per_split, (z + 1) kt_per_split).  Thread 0
+// drives a two-stage pipeline: the six 16 KiB tiles of a K step arrive by
+// bulk copies on the stage's `full` barrier (transaction-counted); the 24
+// MMAs that read them are committed to the stage's `empty` barrier, which
+// releases the stage for the copies two K steps ahead.
 __global__ void __launch_bounds__(kMmThreads, 1)
     df_mm_kernel(const __nv_bfloat16 *__restrict__ A0, const __nv_bfloat16 *__restrict__ A1,
                  const __nv_bfloat16 *__restrict__ A2, const __nv_bfloat16 *__restrict__ B0,
                  const __nv_bfloat16 *__restrict__ B1, const __nv_bfloat16 *__restrict__ B2, long long M,
                  long long N, long long ldp, double *__restrict__ C, long long ldc, int kt_per_split, int *err) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t full[kStages], empty[kStages], done;
     __shared__ uint32_t tmem_base;
-    unsigned char *tiles = smem;  // A0 A1 A2 B0 B1 B2, kPartBytes each
+    __shared__ int s_ok;
     const int tid = threadIdx.x, warp = tid >> 5;
-    const long long m0 = (long long)blockIdx.x * kMmTile, n0 = (long long)blockIdx.y * kMmTile;
+    const long long kts = ldp / kMmK;
+    const long long mt = blockIdx.x, nt = blockIdx.y;
+    const int k_begin = (int)blockIdx.z * kt_per_split;
+    const int k_end = (int)min((long long)(k_begin + kt_per_split), kts);
+    const bool split = gridDim.z > 1;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
@@ -140,36 +177,42 @@ __global__ void __launch_bounds__(kMmThreads, 1)
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        mbar_init(&bar, 1);
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;");
+        s_ok = 1;
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
 
-    // this CTA's K range: tiles [k_begin, k_end) of split blockIdx.z
-    const int n_k = (int)(ldp / kMmK);
-    const int k_begin = (int)blockIdx.z * kt_per_split, k_end = min(n_k, k_begin + kt_per_split);
-    const bool split = gridDim.z > 1;
-    uint32_t phase = 0;
-    bool ok = true;
-    for (int kt = k_begin; kt < k_end && ok; ++kt) {
-        // stage: 6 parts x 128 rows x 8 chunks of 16 bytes; chunk (r, c) of a
-        // part goes to (r / 8) * 1024 + c * 128 + (r % 8) * 16
-        for (int i = tid; i < 6 * kMmTile * (kMmK / 8); i += kMmThreads) {
-            const int part = i / (kMmTile * (kMmK / 8)), rem = i - part * (kMmTile * (kMmK / 8));
-            const int r = rem >> 3, c = rem & 7;
-            const __nv_bfloat16 *src = part == 0 ? A0 : part == 1 ? A1 : part == 2 ? A2 : part == 3 ? B0 : part == 4 ? B1 : B2;
-            const long long row0 = part < 3 ? m0 : n0;
-            const uint4 v = *reinterpret_cast<const uint4 *>(src + (row0 + r) * ldp + (long long)kt * kMmK + c * 8);
-            *reinterpret_cast<uint4 *>(tiles + part * kPartBytes + (r >> 3) * 1024 + c * 128 + (r & 7) * 16) = v;
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+    if (tid == 0 && k_begin < k_end) {
+        const __nv_bfloat16 *parts[6] = {A0, A1, A2, B0, B1, B2};
+        auto issue = [&](int kt, int s) {
+            unsigned char *st = smem + s * kStageBytes;
+            mbar_expect_tx(&full[s], kStageBytes);
+#pragma unroll
+            for (int p = 0; p < 6; ++p) {
+                const long long tile = (p < 3 ? mt : nt) * kts + kt;
+                bulk_copy(st + p * kPartBytes, parts[p] + tile * (kPartBytes / 2), kPartBytes, &full[s]);
+            }
+        };
+        const int nk = k_end - k_begin;
+        for (int i = 0; i < kStages && i < nk; ++i) issue(k_begin + i, i);
+        bool ok = true;
+        for (int i = 0; i < nk && ok; ++i) {
+            const int s = i % kStages;
+            const uint32_t ph = (uint32_t)((i / kStages) & 1);
+            if (!mbar_wait(&full[s], ph)) {
+                ok = false;
+                break;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t base = smem_u32(tiles);
+            const uint32_t base = smem_u32(smem + s * kStageBytes);
             const int pa[6] = {0, 0, 1, 0, 1, 2}, pb[6] = {0, 1, 0, 2, 1, 0};
 #pragma unroll
             for (int p = 0; p < 6; ++p)
@@ -177,7 +220,7 @@ __global__ void __launch_bounds__(kMmThreads, 1)
                 for (int ks = 0; ks < kMmK / 16; ++ks) {
                     const uint64_t da = umma_desc(base + pa[p] * kPartBytes + ks * 256, 128, 1024);
                     const uint64_t db = umma_desc(base + (3 + pb[p]) * kPartBytes + ks * 256, 128, 1024);
-                    const uint32_t acc = (kt > k_begin || p > 0 || ks > 0) ? 1u : 0u;
+                    const uint32_t acc = (i > 0 || p > 0 || ks > 0) ? 1u : 0u;
                     asm volatile(
                         "{\n\t.reg .pred p;\n\t"
                         "setp.ne.b32 p, %4, 0;\n\t"
@@ -185,11 +228,23 @@ __global__ void __launch_bounds__(kMmThreads, 1)
                         "l"(da), "l"(db), "r"(kIdesc), "r"(acc));
                 }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                smem_u32(&bar)));
+                smem_u32(&empty[s])));
+            if (i + kStages < nk) {  // the stage is free once these MMAs have read it
+                if (!mbar_wait(&empty[s], ph)) {
+                    ok = false;
+                    break;
+                }
+                issue(k_begin + i + kStages, s);
+            }
         }
-        ok = __syncthreads_and(mbar_wait(&bar, phase)) != 0;  // one verdict for the whole CTA
-        phase ^= 1u;
+        // every MMA issued so far completes before `done`
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            smem_u32(&done)));
+        if (!ok) s_ok = 0;
     }
+    __syncthreads();
+    bool ok = s_ok != 0;
+    if (k_begin < k_end) ok = __syncthreads_and(mbar_wait(&done, 0) && ok) != 0;
     if (k_begin >= k_end) {
         // an empty split: no accumulator to read
     } else if (!ok) {
@@ -197,7 +252,7 @@ __global__ void __launch_bounds__(kMmThreads, 1)
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;");
         // epilogue: warp w reads rows 32w + lane, 16 columns at a time
-        const long long row = m0 + warp * 32 + (tid & 31);
+        const long long row = mt * kMmTile + warp * 32 + (tid & 31);
         for (int c0 = 0; c0 < kMmTile; c0 += 16) {
             uint32_t v[16];
             const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
@@ -212,7 +267,7 @@ __global__ void __launch_bounds__(kMmThreads, 1)
             if (row < M)
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    const long long col = n0 + c0 + j;
+                    const long long col = nt * kMmTile + c0 + j;
                     if (col < N) {
                         // split K: the FP32 partial sums add up in FP64
                         if (split)
@@ -301,7 +356,7 @@ static cudaError_t df_mm(const __nv_bfloat16 *a, long long a_rows, const __nv_bf
                          long long ldp, long long M, long long N, double *C, long long ldc, int *err,
                          cudaStream_t st) {
     static bool attr = false;
-    const int smem = 6 * kPartBytes;
+    const int smem = kStages * kStageBytes;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(df_mm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
