@@ -584,6 +584,14 @@ def batch_path(a, local):
     bb.capture_merged("m32", _lib.FJB_ROUTED, 1e-9)
     m32_ms = timed(lambda: bb.replay("m32"))
     dG = max(float((g - h).abs().max()) for g, h in zip(bb.G(), G64))
+    # the learned router (trained here on seeded 4-10 atom clusters,
+    # calibrated, installed on the batch's first molecule: it routes them all)
+    from felizjueves_b200 import router
+    mlp, margin, n_tr = train_router()
+    router.install(bb.engines[0], mlp, threshold=1e-9, margin=margin)
+    bb.capture_merged("mlp", _lib.FJB_ROUTED, 1e-9)
+    mlp_ms = timed(lambda: bb.replay("mlp"))
+    dG_mlp = max(float((g - h).abs().max()) for g, h in zip(bb.G(), G64))
     stats = bb.merged_stats()
     sizes = [len(w.coords) for w in ws]
     print(json.dumps({
@@ -597,6 +605,8 @@ def batch_path(a, local):
         "per_molecule_device_ms_fp64_loop": {"p50": round(float(np.percentile(per, 50)), 3),
                                              "p99": round(float(np.percentile(per, 99)), 3)},
         "max_abs_dG_batched_fp64_vs_loop": dG64, "max_abs_dG_batched_routed_vs_fp64": dG,
+        "batched_learned_router_ms": round(mlp_ms, 3), "max_abs_dG_batched_learned_vs_fp64": dG_mlp,
+        "router_training_quartets": n_tr,
         "class_launches_per_batch": stats["class_launches"], "work_units": stats["units"],
         "gpu_launches": 2 * stats["class_launches"] + 2,
         "host_plan_s": round(plan_s, 1)}))

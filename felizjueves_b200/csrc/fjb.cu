@@ -2748,9 +2748,15 @@ int fjb_batch_build(fjb_batch *b, int precision, double threshold, void *stream)
             int *l64 = b->route_list.p + b->n_units + r.unit0;
             int *cnt = b->route_counts.p + 4 * ri;
             const int rgrid = std::max(1, std::min((r.n_units + 3) / 4, 16 * sm_count()));
-            route_units_kernel<<<rgrid, 128, 0, st>>>(b->units.p, r.unit0, r.n_units, b->launches.p, b->pairs.p,
-                                                      nullptr, 0, b->tau, route, l32, l64, cnt, 0, nullptr,
-                                                      b->ctx.p, b->launch_mol.p);
+            if (h0->router_on)  // the first molecule's learned router routes the whole batch
+                route_units_mlp_kernel<<<rgrid, 128, 0, st>>>(
+                    b->units.p, r.unit0, r.n_units, b->launches.p, b->pairs.p, b->prims.p, nullptr, 0, b->tau,
+                    route, h0->router_p.p, h0->router_log_thr, r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, l32, l64,
+                    cnt, 0, nullptr, b->ctx.p, b->launch_mol.p);
+            else
+                route_units_kernel<<<rgrid, 128, 0, st>>>(b->units.p, r.unit0, r.n_units, b->launches.p,
+                                                          b->pairs.p, nullptr, 0, b->tau, route, l32, l64, cnt, 0,
+                                                          nullptr, b->ctx.p, b->launch_mol.p);
             KArgs a32 = a, a64 = a;
             a32.unit_list = l32;
             a32.unit_count = cnt;

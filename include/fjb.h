@@ -347,9 +347,10 @@ int fjb_set_rys(fjb_handle *h, int mode);
  * closing.  The batch reads the handles' plans when it is made (they must
  * outlive it); fjb_batch_set_densities binds each molecule's DEVICE D and
  * its J, K, G outputs (any may be NULL) once, fjb_batch_build then runs and
- * is stream-ordered and capturable (FJB_FP64, or FJB_ROUTED with the
- * Schwarz x density bound router; the budget check and the learned router
- * are single-molecule features).  No counterpart in the reference, whose
+ * is stream-ordered and capturable (FJB_FP64, or FJB_ROUTED: by the
+ * learned router when the first handle has one installed, fjb_router_set,
+ * else by the Schwarz x density bound; the budget check is a
+ * single-molecule feature).  No counterpart in the reference, whose
  * launches are per molecule (eri/fock/walk_f.py:306). */
 typedef struct fjb_batch fjb_batch;
 int fjb_batch_create(fjb_batch **out, fjb_handle *const *handles, int n);

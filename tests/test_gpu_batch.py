@@ -87,3 +87,29 @@ def test_merged_batch_matches_oracle(cuda, lib_built, oracle_lib):
         for g, go in zip(bb.G(), Go):
             assert float(np.abs(g.cpu().numpy() - go).max()) <= bar, name
     bb.close()
+
+
+def test_merged_batch_learned_router_matches_loop(cuda, lib_built):
+    """With a network installed on the first molecule, the batched build
+    routes every molecule by it: the same network installed on each
+    molecule's own handle makes the per-molecule routed builds take the
+    same routing decisions, so the two agree to FP64 rounding."""
+    import torch
+    from felizjueves_b200 import _lib, router
+    from felizjueves_b200.batch import BatchBuilder
+    ws = [configs.cluster(n, 4400 + n) for n in (3, 2, 3)]
+    bb = BatchBuilder(ws)
+    X = np.random.default_rng(0).normal(size=(64, 12)).astype(np.float32)
+    mlp = router.MLP(router.init_params(X, seed=3))
+    for eng in bb.engines:
+        router.install(eng, mlp, threshold=1e-9, margin=0.5)
+        eng.set_route_check(0.0, 16)  # the batch has no per-build check
+    bb.build_loop(_lib.FJB_ROUTED, 1e-9)
+    torch.cuda.synchronize()
+    loop = [g.clone() for g in bb.G()]
+    bb.capture_merged("mlp", _lib.FJB_ROUTED, 1e-9)
+    bb.replay("mlp")
+    torch.cuda.synchronize()
+    for g, h in zip(bb.G(), loop):
+        assert float((g - h).abs().max()) <= 1e-11
+    bb.close()
