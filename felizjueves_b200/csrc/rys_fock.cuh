@@ -186,10 +186,12 @@ struct Shape {
     __host__ __device__ static constexpr int nt() { return NBF > 64 ? 256 : 128; }
     // CTAs an SM holds: 512 threads of 128 registers, unless the bra column
     // the boundary phase keeps in registers is too long to fit in those
-    // (df and ff bras in FP64, the ff bra in FP32): then half as many
+    // (df and ff bras in FP64, the ff bra in FP32): then half as many; the
+    // FP32 tier's small bras (up to 20 boundary values) fit six CTAs of 80
+    // registers, with no more than a few dozen bytes of spill
     template <typename R>
     __host__ __device__ static constexpr int minb() {
-        return (nt() == 256 ? 2 : 4) / (NBE > (sizeof(R) == 8 ? 34 : 52) ? 2 : 1);
+        return sizeof(R) == 4 && nt() == 128 && NBE <= 20 ? 6 : (nt() == 256 ? 2 : 4) / (NBE > (sizeof(R) == 8 ? 34 : 52) ? 2 : 1);
     }
 };
 
