@@ -518,9 +518,12 @@ def side_path(a, local):
                                     "cores": 1, "kind": "port",
                                     "sample": f"oracle one_electron.blocks on {len(sample)} random shell pairs "
                                               f"of {len(pairs)}, {spent:.1f} s, scaled by the pair count"}
+    elif a.atoms >= 32:
+        return df_stream_path(a, local, line)
     else:
         # DF-J/K on a cluster of the c1 recipe (--atoms; the 64-atom system's
-        # dense factors, 5,760 x 1,984^2 doubles, do not fit in HBM)
+        # dense factors, 5,760 x 1,984^2 doubles, do not fit in HBM: from 32
+        # atoms the streamed build, df_stream_path)
         from felizjueves_b200.df import DFEngine
         w = configs.cluster(a.atoms, 1)
         D = torch.tensor(w.D, device=f"cuda:{local}")
@@ -541,6 +544,70 @@ def side_path(a, local):
                     max_abs_dJ_bf16x3_vs_fp64=float((J16 - J64).abs().max()),
                     max_abs_dK_bf16x3_vs_fp64=float((K16 - K64).abs().max()),
                     max_abs_K_fp64=float(K64.abs().max()))
+    print(json.dumps(line))
+
+
+def df_stream_path(a, local, line):
+    """Config c2's DF half at full size (`--path df --atoms 64`): the c1
+    system with the even-tempered s..g aux basis (5,760 functions), DF-J/K
+    by DFEngine.jk_streamed -- (mn|P) one aux block at a time from the
+    three-centre Rys kernel, never held whole -- with K on the tensor cores
+    (split BF16) and, once, in FP64; errors of both against the exact FP64
+    build of the same density (the 4-centre fused build), per phase CUDA-event
+    times.  The metric and its factor are set up once, outside the timed
+    steps (as the dense path's factors are)."""
+    import time as _t
+    import torch
+    from felizjueves_b200 import configs
+    from felizjueves_b200.df import DFEngine
+    from felizjueves_b200.fock import FockEngine
+    w = configs.cluster(a.atoms, 1)
+    dev = f"cuda:{local}"
+    D = torch.tensor(w.D, device=dev)
+    ex = FockEngine(w.basis, device=local)
+    ex.plan(w.D, w.tau, w.n_mag)
+    Jx, Kx, Gx = (t.clone() for t in ex.build(D))
+    torch.cuda.synchronize()
+    ex.close()
+    del ex
+    aux = configs.aux_basis(w)
+    eng = DFEngine(w.basis, aux, device=local)
+    t0 = _t.perf_counter()
+    factor = eng.metric_factor()
+    torch.cuda.synchronize()
+    setup_s = _t.perf_counter() - t0
+    st = torch.cuda.current_stream()
+
+    def run(mode, n):
+        tm = {}
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(n):
+            J, K = eng.jk_streamed(D, mode=mode, tau=w.tau, factor=factor, timings=tm)
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n, J, K, tm
+
+    for _ in range(a.warmup):
+        run("bf16x3", 1)
+    ms, J, K, tm = run("bf16x3", a.steps)
+    ms64, J64, K64, tm64 = run("fp64", 1)
+
+    def err(X, R):
+        return {"max_abs": float((X - R).abs().max()), "rel_max": float((X - R).abs().max() / R.abs().max())}
+
+    G, G64 = J - 0.5 * K, J64 - 0.5 * K64
+    nq, n = aux.n_ao, w.n_ao
+    line.update(metric="DF-J/K ms/iter (streamed)", value=round(ms, 3), unit="ms/iter", dtype="f64; K bf16x3 -> f32",
+                config={"workload": f"c2: {a.atoms}-atom c1-recipe cluster, {n} AO, {nq} aux (s..g, 0.1 2.2^k)",
+                        "n_ao": n, "n_aux": nq, "aux_block_functions": 384, "tau": w.tau},
+                phases_ms={k: round(v, 3) if isinstance(v, float) else v for k, v in tm.items()},
+                fp64_k_ms=round(ms64, 3), fp64_k_phases_ms={k: round(v, 3) if isinstance(v, float) else v
+                                                            for k, v in tm64.items()},
+                metric_setup_s=round(setup_s, 2),
+                dJ_vs_exact=err(J, Jx), dK_vs_exact=err(K, Kx), dG_vs_exact=err(G, Gx),
+                dK_bf16x3_vs_fp64_df=err(K, K64), dG_fp64_df_vs_exact=err(G64, Gx),
+                gpu_launches=None)
     print(json.dumps(line))
 
 

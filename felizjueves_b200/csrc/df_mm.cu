@@ -352,9 +352,11 @@ size_t df_jk_workspace_bytes(long long nq, long long n) {
     return (size_t)round_up((round_up(nq, 32) + nq * n * n) * (long long)sizeof(double), 256) + (size_t)split * 2;
 }
 
+// max_per_split > 0 caps the K tiles one CTA accumulates in FP32 (more
+// splits, each added into C in FP64): the bound on the FP32 sums' length.
 static cudaError_t df_mm(const __nv_bfloat16 *a, long long a_rows, const __nv_bfloat16 *b, long long b_rows,
                          long long ldp, long long M, long long N, double *C, long long ldc, int *err,
-                         cudaStream_t st) {
+                         cudaStream_t st, int max_per_split = 0) {
     static bool attr = false;
     const int smem = kStages * kStageBytes;
     if (!attr) {
@@ -369,6 +371,7 @@ static cudaError_t df_mm(const __nv_bfloat16 *a, long long a_rows, const __nv_bf
     // at least 8 K-tiles; the splits' FP32 partials are added in FP64
     int splits = 1;
     if (tiles < 2 * 148) splits = (int)std::max(1LL, std::min((long long)(n_k / 8), (2 * 148 + tiles - 1) / tiles));
+    if (max_per_split > 0) splits = std::max(splits, (n_k + max_per_split - 1) / max_per_split);
     const int per = (n_k + splits - 1) / splits;
     splits = (n_k + per - 1) / per;
     if (splits > 1) {  // the splits add into C
@@ -413,6 +416,27 @@ cudaError_t df_jk_launch(const double *B, long long nq, long long n, const doubl
     df_split_kernel<<<sgrid, 256, 0, st>>>(B, 1, n, nq * n, 0, n, s.rowsn, s.ld2, b2, b2 + s.rowsn * s.ld2,
                                            b2 + 2 * s.rowsn * s.ld2);
     e = df_mm(a2, s.rowsn, b2, s.rowsn, s.ld2, n, n, K, n, err, st);
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+// K = Z Z^T for Z (rows x cols, FP64, row-major, device): the occupied-
+// orbital DF exchange, Z[m][(i, Q)] = sum_P Y[m][i][P] W[P][Q] for the
+// metric's inverse factor W.  Split-BF16 products on the tensor cores as in
+// fjb_df_jk; FP32 sums of at most 256 K tiles (16,384 products), added in
+// FP64.  `work` holds df_syrk_workspace_bytes(rows, cols) device bytes.
+size_t df_syrk_workspace_bytes(long long rows, long long cols) {
+    return (size_t)(3 * round_up(rows, kMmTile) * round_up(cols, kMmK)) * 2;
+}
+
+cudaError_t df_syrk_launch(const double *Z, long long rows, long long cols, double *K, void *work, int *err,
+                           cudaStream_t st) {
+    const long long rp = round_up(rows, kMmTile), ldp = round_up(cols, kMmK);
+    __nv_bfloat16 *a = static_cast<__nv_bfloat16 *>(work);
+    df_split_kernel<<<148 * 16, 256, 0, st>>>(Z, 0, rows, cols, cols, 0, rp, ldp, a, a + rp * ldp, a + 2 * rp * ldp);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = df_mm(a, rp, a, rp, ldp, rows, rows, K, rows, err, st, 256);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }

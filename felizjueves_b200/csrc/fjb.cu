@@ -30,6 +30,7 @@
 #include "scatter.h"
 #include "router.cuh"
 #include "rys_fock.cuh"
+#include "df_eri3.cuh"
 
 namespace fjb {
 std::vector<double> boys_table();
@@ -42,6 +43,9 @@ cudaError_t launch_compiled(int la, int lb, int lc, int ld, bool fp32, int grid,
 size_t df_jk_workspace_bytes(long long nq, long long n);
 cudaError_t df_jk_launch(const double *B, long long nq, long long n, const double *D, double *J, double *K,
                          void *work, int *err, cudaStream_t st);
+size_t df_syrk_workspace_bytes(long long rows, long long cols);
+cudaError_t df_syrk_launch(const double *Z, long long rows, long long cols, double *K, void *work, int *err,
+                           cudaStream_t st);
 }
 
 using namespace fjb;
@@ -978,6 +982,18 @@ struct fjb_handle {
     // a density-fitting handle: AO shells, then aux shells, then the unit shell
     bool df = false;
     int df_ao_shells = 0, df_aux_shells = 0;
+    // the three-centre kernel's records (fjb_df_eri3), staged on first use:
+    // AO pairs (la >= lb) with their Schwarz factors, the aux shells as
+    // (P, unit) pairs sorted by (l, degree, index), the per-class layouts
+    bool e3_ready = false;
+    DevBuf<PairRec> e3_pairs, e3_kets;
+    DevBuf<PrimRec> e3_prims, e3_kprims;
+    DevBuf<E3Unit> e3_units;
+    std::vector<PairRec> e3_pairs_host, e3_kets_host;
+    std::vector<int> e3_ket_pos;  // aux shell -> its position in the sorted list
+    std::vector<int> e3_aux_off;  // aux shell -> first function in the aux basis (n_aux at the end)
+    double e3_gp_max = 0.0;       // the largest aux Schwarz factor
+    std::map<std::tuple<int, int, int>, E3Dev> e3_dev;
     // the captured build (fjb_fock_build_graph)
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -2116,6 +2132,232 @@ int fjb_df_jk(fjb_handle *h, const double *B_dev, int64_t n_aux, int64_t n_ao, c
     CUDA_OK(h, cudaMemcpyAsync(&err, h->df_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_OK(h, cudaStreamSynchronize(st));
     if (err) return fail(h, FJB_E_TIMEOUT, "fjb_df_jk: a tensor-core wait ran out (the GEMM did not complete)");
+    return FJB_OK;
+}
+
+int fjb_df_syrk(fjb_handle *h, const double *Z_dev, int64_t rows, int64_t cols, double *K_dev, void *stream) {
+    if (!h || !Z_dev || !K_dev) return fail(h, FJB_E_ARG, "null argument");
+    if (rows < 1 || cols < 1) return fail(h, FJB_E_ARG, "fjb_df_syrk: rows and cols must be >= 1");
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    CUDA_OK(h, cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t bytes = df_syrk_workspace_bytes(rows, cols);
+    try {
+        if (h->df_work.n < bytes) {
+            CUDA_OK(h, cudaStreamSynchronize(st));  // a previous call may still read the old workspace
+            h->df_work.alloc(bytes);
+        }
+        h->df_err.alloc(1);
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, std::string("fjb_df_syrk workspace: ") + e.what());
+    }
+    CUDA_OK(h, cudaMemsetAsync(h->df_err.p, 0, sizeof(int), st));
+    CUDA_OK(h, df_syrk_launch(Z_dev, rows, cols, K_dev, h->df_work.p, h->df_err.p, st));
+    int err = 0;
+    CUDA_OK(h, cudaMemcpyAsync(&err, h->df_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(h, cudaStreamSynchronize(st));
+    if (err) return fail(h, FJB_E_TIMEOUT, "fjb_df_syrk: a tensor-core wait ran out (the GEMM did not complete)");
+    return FJB_OK;
+}
+
+namespace {
+
+// The three-centre kernel's records, staged once per handle: the Schwarz
+// factors sqrt(max |(ab|ab)|) of every AO shell pair and sqrt(max |(P|P)|)
+// of every aux shell from the ERI tap, the AO pairs oriented la >= lb, the
+// aux shells as (P, unit) pairs sorted by (l, degree, index).
+int ensure_eri3(fjb_handle *h) {
+    if (h->e3_ready) return FJB_OK;
+    const int nao_sh = h->df_ao_shells, nx = h->df_aux_shells, unit = nao_sh + nx;
+    const HostBasis &B = h->basis;
+    const int ao_end = B.offsets[nao_sh];  // AO functions; the aux basis numbers from here
+    // Schwarz factors: one diagonal block per AO pair and per aux shell
+    std::vector<int32_t> q;
+    std::vector<std::pair<int, int>> ab;
+    for (int a = 0; a < nao_sh; ++a)
+        for (int b = a; b < nao_sh; ++b) {
+            ab.emplace_back(a, b);
+            const int x = B.shells[a].l <= B.shells[b].l ? a : b, y = x == a ? b : a;
+            q.insert(q.end(), {x, y, x, y});
+        }
+    for (int P = 0; P < nx; ++P) q.insert(q.end(), {nao_sh + P, unit, nao_sh + P, unit});
+    const int nq = (int)(q.size() / 4);
+    std::vector<int64_t> off((size_t)nq + 1, 0);
+    for (int i = 0; i < nq; ++i) {
+        int nabcd = 1;
+        for (int k = 0; k < 4; ++k) nabcd *= ncart(B.shells[q[4 * (size_t)i + k]].l);
+        off[i + 1] = off[i] + nabcd;
+    }
+    std::vector<double> diag;
+    try {
+        DevBuf<double> dv;
+        dv.alloc((size_t)off[nq]);
+        if (int rc = eri_blocks_impl(h, q.data(), nq, dv.p, off.data(), false)) return rc;
+        diag.resize((size_t)off[nq]);
+        CUDA_OK(h, cudaMemcpy(diag.data(), dv.p, diag.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, std::string("fjb_df_eri3 Schwarz factors: ") + e.what());
+    }
+    auto gmax = [&](int i) {
+        double m = 0.0;
+        for (int64_t k = off[i]; k < off[i + 1]; ++k) m = std::max(m, std::fabs(diag[(size_t)k]));
+        return std::sqrt(m);
+    };
+    std::vector<PairRec> pr;
+    std::vector<PrimRec> pm;
+    for (size_t i = 0; i < ab.size(); ++i) {
+        int a = ab[i].first, b = ab[i].second;
+        if (B.shells[a].l < B.shells[b].l) std::swap(a, b);
+        const HostShell &sa = B.shells[a], &sb = B.shells[b];
+        const int K = (int)(sa.exps.size() * sb.exps.size());
+        pr.push_back(pair_record(B, a, b, gmax((int)i), (int)pm.size(), K));
+        for (int k = 0; k < K; ++k) pm.push_back(prim_record(sa, sb, k));
+    }
+    std::vector<int> order(nx);
+    for (int P = 0; P < nx; ++P) order[P] = P;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const HostShell &sx = B.shells[nao_sh + x], &sy = B.shells[nao_sh + y];
+        if (sx.l != sy.l) return sx.l < sy.l;
+        return sx.exps.size() < sy.exps.size();
+    });
+    std::vector<PairRec> kr;
+    std::vector<PrimRec> km;
+    h->e3_ket_pos.assign(nx, 0);
+    h->e3_gp_max = 0.0;
+    for (int i = 0; i < nx; ++i) {
+        const int P = order[i];
+        const HostShell &sp = B.shells[nao_sh + P];
+        const int K = (int)sp.exps.size();
+        const double g = gmax((int)ab.size() + P);
+        h->e3_gp_max = std::max(h->e3_gp_max, g);
+        PairRec r = pair_record(B, nao_sh + P, unit, g, (int)km.size(), K);
+        r.ao_a = B.offsets[nao_sh + P] - ao_end;
+        kr.push_back(r);
+        for (int k = 0; k < K; ++k) km.push_back(prim_record(sp, B.shells[unit], k));
+        h->e3_ket_pos[P] = i;
+    }
+    h->e3_aux_off.assign(nx + 1, 0);
+    for (int P = 0; P < nx; ++P) h->e3_aux_off[P] = B.offsets[nao_sh + P] - ao_end;
+    h->e3_aux_off[nx] = B.offsets[unit] - ao_end;
+    try {
+        h->e3_pairs.upload(pr);
+        h->e3_prims.upload(pm);
+        h->e3_kets.upload(kr);
+        h->e3_kprims.upload(km);
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, e.what());
+    }
+    h->e3_pairs_host = std::move(pr);
+    h->e3_kets_host = std::move(kr);
+    h->e3_dev.clear();
+    h->e3_ready = true;
+    return FJB_OK;
+}
+
+}  // namespace
+
+int fjb_df_eri3(fjb_handle *h, int aux_shell0, int aux_shell1, double tau, double *out_dev, void *stream) {
+    if (!h || !out_dev) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->df) return fail(h, FJB_E_STATE, "not a density-fitting handle (fjb_create_df)");
+    const int nx = h->df_aux_shells;
+    if (aux_shell0 < 0 || aux_shell1 > nx || aux_shell0 >= aux_shell1)
+        return fail(h, FJB_E_ARG, "fjb_df_eri3: need 0 <= aux_shell0 < aux_shell1 <= the aux shell count");
+    if (!(tau == tau)) return fail(h, FJB_E_ARG, "fjb_df_eri3: tau is not a number");
+    CUDA_OK(h, cudaSetDevice(h->device));
+    if (int rc = ensure_eri3(h)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const HostBasis &B = h->basis;
+    const int n_ao = B.offsets[h->df_ao_shells];
+    const int p0 = h->e3_aux_off[aux_shell0], nb = h->e3_aux_off[aux_shell1] - p0;
+    // the block's aux shells in sorted order: runs of equal (l, degree),
+    // cut into units of at most kE3Kets
+    std::vector<int> pos;
+    for (int P = aux_shell0; P < aux_shell1; ++P) pos.push_back(h->e3_ket_pos[P]);
+    std::sort(pos.begin(), pos.end());
+    struct Run {
+        int lp, k0, k1;
+    };
+    std::vector<Run> runs;
+    for (size_t i = 0; i < pos.size();) {
+        const PairRec &k = h->e3_kets_host[pos[i]];
+        const int lp = B.shells[k.a].l, deg = k.nprim;
+        size_t j = i + 1;
+        while (j < pos.size() && pos[j] == pos[j - 1] + 1 && j - i < (size_t)kE3Kets &&
+               B.shells[h->e3_kets_host[pos[j]].a].l == lp && h->e3_kets_host[pos[j]].nprim == deg)
+            ++j;
+        runs.push_back({lp, pos[i], pos[j - 1] + 1});
+        i = j;
+    }
+    // units class by class: (la, lb) of the pair, lp of the run
+    struct Launch {
+        int la, lb, lp, max_kab, max_kcd;
+        size_t u0, n;
+    };
+    std::vector<Launch> launches;
+    std::vector<E3Unit> units;
+    for (const auto &r : runs)
+        if (r.lp > FJB_E3_MAX_LP) return fail(h, FJB_E_LIMIT, "fjb_df_eri3: aux l above 4");
+    std::map<int, std::vector<int>> by;  // lp -> run indices
+    for (size_t r = 0; r < runs.size(); ++r) by[runs[r].lp].push_back((int)r);
+    std::map<std::pair<int, int>, std::vector<int>> pairs_of;
+    const double gate = tau > 0.0 ? tau / std::max(h->e3_gp_max, 1e-300) : -1.0;
+    for (size_t i = 0; i < h->e3_pairs_host.size(); ++i) {
+        const PairRec &p = h->e3_pairs_host[i];
+        if (gate > 0.0 && p.G < gate) continue;  // below tau against every aux shell
+        pairs_of[{B.shells[p.a].l, B.shells[p.b].l}].push_back((int)i);
+    }
+    for (auto &kv : pairs_of) {
+        const int la = kv.first.first, lb = kv.first.second;
+        int max_kab = 1;
+        for (int i : kv.second) max_kab = std::max(max_kab, h->e3_pairs_host[i].nprim);
+        for (int lp = 0; lp <= FJB_E3_MAX_LP; ++lp) {
+            auto it = by.find(lp);
+            if (it == by.end()) continue;
+            int max_kcd = 1;
+            for (int r : it->second)
+                for (int k = runs[r].k0; k < runs[r].k1; ++k) max_kcd = std::max(max_kcd, h->e3_kets_host[k].nprim);
+            Launch L{la, lb, lp, max_kab, max_kcd, units.size(), 0};
+            for (int i : kv.second)
+                for (int r : it->second) units.push_back(E3Unit{i, runs[r].k0, runs[r].k1, 0});
+            L.n = units.size() - L.u0;
+            if (L.n) launches.push_back(L);
+        }
+    }
+    try {
+        CUDA_OK(h, cudaStreamSynchronize(st));  // an earlier call's kernels may still read the units
+        h->e3_units.upload(units);
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, e.what());
+    }
+    CUDA_OK(h, cudaMemsetAsync(out_dev, 0, (size_t)n_ao * n_ao * nb * sizeof(double), st));
+    const int sms = sm_count();
+    for (const Launch &L : launches) {
+        auto key = std::make_tuple(L.la, L.lb, L.lp);
+        auto it = h->e3_dev.find(key);
+        if (it == h->e3_dev.end() || it->second.kab < L.max_kab || it->second.kcd < L.max_kcd) {
+            E3Dev d;
+            if (!eri3_layout(L.la, L.lb, L.lp, L.max_kab, L.max_kcd, &d))
+                return fail(h, FJB_E_LIMIT, "fjb_df_eri3: a class does not fit in shared memory");
+            it = h->e3_dev.insert_or_assign(key, d).first;
+        }
+        E3Args a{};
+        a.Y = it->second;
+        a.units = h->e3_units.p + L.u0;
+        a.n_units = (int)L.n;
+        a.pairs = h->e3_pairs.p;
+        a.prims = h->e3_prims.p;
+        a.kets = h->e3_kets.p;
+        a.kprims = h->e3_kprims.p;
+        a.out = out_dev;
+        a.n_ao = n_ao;
+        a.p0 = p0;
+        a.nb = nb;
+        a.tau = tau;
+        a.rys_tab = h->rys.p;
+        const int per_sm = std::max(1, eri3_blocks_per_sm(L.la, L.lb, L.lp, a.Y));
+        const int grid = (int)std::min<size_t>(L.n, (size_t)per_sm * sms);
+        CUDA_OK(h, eri3_launch(L.la, L.lb, L.lp, grid, st, a));
+    }
     return FJB_OK;
 }
 

@@ -377,6 +377,31 @@ void fjb_batch_destroy(fjb_batch *b);
 int fjb_df_jk(fjb_handle *h, const double *B_dev, int64_t n_aux, int64_t n_ao, const double *D_dev,
               double *J_dev, double *K_dev, void *stream);
 
+/* The three-centre integrals (mn|P) of one aux block, on the device, by
+ * Rys quadrature (eri/density_fit/eri3.py:226 eri3_tensor, restricted to
+ * the aux functions of aux shells [aux_shell0, aux_shell1)): out_dev
+ * (DEVICE, n_ao x n_ao x nb doubles, nb the block's aux functions) receives
+ * (mn|P) at [m][n][P - p0], aux fastest, both (m, n) and (n, m) written;
+ * p0 is the first function of aux_shell0.  A (shell pair, aux shell) block
+ * whose Schwarz product sqrt(max|(ab|ab)|) sqrt(max|(P|P)|) is below tau is
+ * zero (tau <= 0: none is).  The first call stages the AO pairs and their
+ * Schwarz factors (from the ERI tap; synchronises); every call synchronises
+ * `stream` before staging its work units, then runs asynchronously on it.
+ * Aux shells to l = 4 (FJB_E_LIMIT above).  A block of nb aux functions
+ * holds 8 n_ao^2 nb bytes: this is how a caller streams the DF build of a
+ * system whose whole tensor does not fit (DFEngine.jk_streamed). */
+int fjb_df_eri3(fjb_handle *h, int aux_shell0, int aux_shell1, double tau, double *out_dev, void *stream);
+
+/* K = Z Z^T (DEVICE, rows x rows, FP64) for Z (DEVICE, rows x cols, FP64,
+ * row-major) on the tensor cores: Z split into three BF16 terms, the six
+ * products of total order <= 2 accumulated in FP32 over at most 16,384
+ * terms of the contraction, those partial sums added in FP64.  The
+ * occupied-orbital DF exchange: Z[m][(i, Q)] = sum_P (m i|P) W_PQ, W the
+ * metric's inverse factor.  The handle owns the workspace (6 rows cols
+ * bytes, rounded up to whole tiles).  Synchronises `stream`; FJB_E_TIMEOUT
+ * if a tensor-core wait ran out. */
+int fjb_df_syrk(fjb_handle *h, const double *Z_dev, int64_t rows, int64_t cols, double *K_dev, void *stream);
+
 /* The routed build's error-budget check (on by default: budget 1e-8,
  * stride 16).  Every stride-th unit the router puts on the FP32 queue is
  * built twice more, in FP32 and in FP64, into side accumulators; the
