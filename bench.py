@@ -59,6 +59,10 @@ def parse():
                          "uneven molecule batch (c4) as one captured graph")
     ap.add_argument("--molecules", type=int, default=64, help="batch path: the first N c4 molecules")
     ap.add_argument("--atoms", type=int, default=16, help="df path: atoms of the c1-recipe cluster")
+    ap.add_argument("--df-block", type=int, default=768,
+                    help="streamed df path: aux functions per block of (mn|P) (n_ao^2 x block doubles)")
+    ap.add_argument("--df-stream", action="store_true",
+                    help="df path: the streamed build (DFEngine.jk_streamed) below 32 atoms too")
     ap.add_argument("--threshold", type=float, default=1e-9,
                     help="routed builds: the Schwarz x density bound under which a unit runs FP32 "
                          "(config c2's rule: 1e-9)")
@@ -518,7 +522,7 @@ def side_path(a, local):
                                     "cores": 1, "kind": "port",
                                     "sample": f"oracle one_electron.blocks on {len(sample)} random shell pairs "
                                               f"of {len(pairs)}, {spent:.1f} s, scaled by the pair count"}
-    elif a.atoms >= 32:
+    elif a.atoms >= 32 or a.df_stream:
         return df_stream_path(a, local, line)
     else:
         # DF-J/K on a cluster of the c1 recipe (--atoms; the 64-atom system's
@@ -583,7 +587,7 @@ def df_stream_path(a, local, line):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         for _ in range(n):
-            J, K = eng.jk_streamed(D, mode=mode, tau=w.tau, factor=factor, timings=tm)
+            J, K = eng.jk_streamed(D, mode=mode, tau=w.tau, factor=factor, timings=tm, block=a.df_block)
         e1.record(st)
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / n, J, K, tm
@@ -600,14 +604,14 @@ def df_stream_path(a, local, line):
     nq, n = aux.n_ao, w.n_ao
     line.update(metric="DF-J/K ms/iter (streamed)", value=round(ms, 3), unit="ms/iter", dtype="f64; K bf16x3 -> f32",
                 config={"workload": f"c2: {a.atoms}-atom c1-recipe cluster, {n} AO, {nq} aux (s..g, 0.1 2.2^k)",
-                        "n_ao": n, "n_aux": nq, "aux_block_functions": 384, "tau": w.tau},
+                        "n_ao": n, "n_aux": nq, "aux_block_functions": a.df_block, "tau": w.tau},
                 phases_ms={k: round(v, 3) if isinstance(v, float) else v for k, v in tm.items()},
                 fp64_k_ms=round(ms64, 3), fp64_k_phases_ms={k: round(v, 3) if isinstance(v, float) else v
                                                             for k, v in tm64.items()},
                 metric_setup_s=round(setup_s, 2),
                 dJ_vs_exact=err(J, Jx), dK_vs_exact=err(K, Kx), dG_vs_exact=err(G, Gx),
                 dK_bf16x3_vs_fp64_df=err(K, K64), dG_fp64_df_vs_exact=err(G64, Gx),
-                gpu_launches=None)
+                gpu_launches=tm.get("fjb_launches"))
     print(json.dumps(line))
 
 

@@ -84,7 +84,7 @@ def load():
     L.fjb_set_rys.argtypes = [vp, C.c_int]
     L.fjb_set_route_check.argtypes = [vp, dbl, C.c_int]
     L.fjb_df_jk.argtypes = [vp, vp, i64, i64, vp, vp, vp, vp]
-    L.fjb_df_eri3.argtypes = [vp, C.c_int, C.c_int, dbl, vp, vp]
+    L.fjb_df_eri3.argtypes = [vp, C.c_int, C.c_int, dbl, vp, C.POINTER(C.c_int32), vp]
     L.fjb_df_syrk.argtypes = [vp, vp, i64, i64, vp, vp]
     L.fjb_batch_create.argtypes = [C.POINTER(vp), vp, C.c_int]
     L.fjb_batch_set_densities.argtypes = [vp, vp, vp, vp, vp]

@@ -2256,8 +2256,10 @@ int ensure_eri3(fjb_handle *h) {
 
 }  // namespace
 
-int fjb_df_eri3(fjb_handle *h, int aux_shell0, int aux_shell1, double tau, double *out_dev, void *stream) {
+int fjb_df_eri3(fjb_handle *h, int aux_shell0, int aux_shell1, double tau, double *out_dev, int32_t *n_launches,
+                void *stream) {
     if (!h || !out_dev) return fail(h, FJB_E_ARG, "null argument");
+    if (n_launches) *n_launches = 0;
     if (!h->df) return fail(h, FJB_E_STATE, "not a density-fitting handle (fjb_create_df)");
     const int nx = h->df_aux_shells;
     if (aux_shell0 < 0 || aux_shell1 > nx || aux_shell0 >= aux_shell1)
@@ -2357,6 +2359,7 @@ int fjb_df_eri3(fjb_handle *h, int aux_shell0, int aux_shell1, double tau, doubl
         const int per_sm = std::max(1, eri3_blocks_per_sm(L.la, L.lb, L.lp, a.Y));
         const int grid = (int)std::min<size_t>(L.n, (size_t)per_sm * sms);
         CUDA_OK(h, eri3_launch(L.la, L.lb, L.lp, grid, st, a));
+        if (n_launches) ++*n_launches;
     }
     return FJB_OK;
 }

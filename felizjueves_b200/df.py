@@ -57,6 +57,7 @@ class DFEngine:
 
     def __init__(self, basis: Basis, aux: Basis, device: int = 0):
         self.basis, self.aux, self.device = basis, aux, int(device)
+        self.launches = 0  # the library's kernels launched by eri3_block and syrk
         self._L = _lib.load()
         a, self._fa = _basis_t(basis)
         x, self._fx = _basis_t(aux)
@@ -166,8 +167,10 @@ class DFEngine:
         if out is None:
             out = torch.empty((n, n, p1 - p0), dtype=torch.float64, device=f"cuda:{self.device}")
         st = stream if stream is not None else torch.cuda.current_stream(out.device)
-        _lib.check(self._L.fjb_df_eri3(self._h, int(s0), int(s1), float(tau), out.data_ptr(),
+        nl = C.c_int32()
+        _lib.check(self._L.fjb_df_eri3(self._h, int(s0), int(s1), float(tau), out.data_ptr(), C.byref(nl),
                                        C.c_void_p(st.cuda_stream)), self._h)
+        self.launches += nl.value
         return out
 
     def syrk(self, Z, out=None):
@@ -177,11 +180,12 @@ class DFEngine:
         rows, cols = Z.shape
         K = out if out is not None else torch.empty((rows, rows), dtype=torch.float64, device=Z.device)
         st = torch.cuda.current_stream(Z.device)
+        self.launches += 2  # the split, the GEMM
         _lib.check(self._L.fjb_df_syrk(self._h, Z.data_ptr(), rows, cols, K.data_ptr(),
                                        C.c_void_p(st.cuda_stream)), self._h)
         return K
 
-    def jk_streamed(self, D, *, tau: float = 1e-12, block: int = 384, mode: str = "bf16x3", factor=None,
+    def jk_streamed(self, D, *, tau: float = 1e-12, block: int = 768, mode: str = "bf16x3", factor=None,
                     occ_tol: float = 1e-10, timings: dict | None = None):
         """DF J and K of the symmetric density D (torch, cuda, FP64) without
         holding (mn|P) whole: the integrals are computed one aux block at a
@@ -192,21 +196,24 @@ class DFEngine:
         Z = Y W (W from metric_factor) and K = Z_+ Z_+^T - Z_- Z_-^T
         (mode "bf16x3": fjb_df_syrk on the tensor cores; "fp64": FP64
         GEMMs); c = W W^T d; pass 2 forms J_mn = sum_P (mn|P) c_P.  Memory:
-        one block of n_ao^2 block doubles, Y and Z of n_ao n_occ n_aux each.
+        one block of n_ao^2 block doubles (768 aux functions: 24 GB at
+        1,984 AO), Y and Z of n_ao n_occ n_aux each.
         `timings`, if given, receives CUDA-event milliseconds per phase."""
         import torch
         if mode not in ("bf16x3", "fp64"):
             raise ValueError(f"unknown mode {mode!r}")
         dev = D.device
         n, nx = self.basis.n_ao, self.aux.n_ao
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        launches0 = self.launches
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         ev[0].record()
         W, L = factor if factor is not None else self.metric_factor()
-        ev[1].record()
+        ev[5].record()
         w, U = torch.linalg.eigh(D)
         big = w.abs() > occ_tol * w.abs().max()
         Cs = [U[:, big & (w > 0)] * torch.sqrt(w[big & (w > 0)]),
               U[:, big & (w < 0)] * torch.sqrt(-w[big & (w < 0)])]
+        ev[1].record()
         blocks = self.aux_blocks(block)
         nbmax = max(p1 - p0 for _, _, p0, p1 in blocks)
         T = torch.empty(n * n * nbmax, dtype=torch.float64, device=dev)
@@ -247,9 +254,11 @@ class DFEngine:
         ev[4].record()
         if timings is not None:
             torch.cuda.synchronize(dev)
-            timings.update({"factor_ms": ev[0].elapsed_time(ev[1]), "pass1_ms": ev[1].elapsed_time(ev[2]),
+            timings.update({"factor_ms": ev[0].elapsed_time(ev[5]), "occupied_ms": ev[5].elapsed_time(ev[1]),
+                            "pass1_ms": ev[1].elapsed_time(ev[2]),
                             "k_ms": ev[2].elapsed_time(ev[3]), "pass2_ms": ev[3].elapsed_time(ev[4]),
                             "blocks": len(blocks), "n_occ": [int(c.shape[1]) for c in Cs],
+                            "fjb_launches": self.launches - launches0,
                             "aux_kept": int(W.shape[1])})
         return J.view(n, n), 0.5 * (K + K.T)
 

@@ -389,8 +389,11 @@ int fjb_df_jk(fjb_handle *h, const double *B_dev, int64_t n_aux, int64_t n_ao, c
  * `stream` before staging its work units, then runs asynchronously on it.
  * Aux shells to l = 4 (FJB_E_LIMIT above).  A block of nb aux functions
  * holds 8 n_ao^2 nb bytes: this is how a caller streams the DF build of a
- * system whose whole tensor does not fit (DFEngine.jk_streamed). */
-int fjb_df_eri3(fjb_handle *h, int aux_shell0, int aux_shell1, double tau, double *out_dev, void *stream);
+ * system whose whole tensor does not fit (DFEngine.jk_streamed).
+ * n_launches (HOST, may be NULL) receives the number of class kernels
+ * launched. */
+int fjb_df_eri3(fjb_handle *h, int aux_shell0, int aux_shell1, double tau, double *out_dev, int32_t *n_launches,
+                void *stream);
 
 /* K = Z Z^T (DEVICE, rows x rows, FP64) for Z (DEVICE, rows x cols, FP64,
  * row-major) on the tensor cores: Z split into three BF16 terms, the six
