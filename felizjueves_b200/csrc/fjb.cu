@@ -838,6 +838,7 @@ struct ClassRun {
     RysDev ry64{}, ry32{};
     int grid_r64 = 0, grid_r32 = 0;
     const double *rys_tab = nullptr;
+    const float *rys_tab32 = nullptr;
     ClassDev dev32;  // the FP32 interpreter's layout (routed builds of classes without has32)
     int unit0 = 0, n_units = 0;
     int grid = 0;
@@ -888,6 +889,7 @@ cudaError_t launch_run(const ClassRun &r, cudaStream_t st, const KArgs &a) {
         KArgs ar = a;
         ar.Y = r.ry64;
         ar.rys_tab = r.rys_tab;
+        ar.rys_tab32 = r.rys_tab32;
         return rys_launch(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, false, r.grid_r64, st, ar);
     }
     if (r.compiled) return launch_compiled(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, false, r.grid, st, a);
@@ -902,6 +904,7 @@ cudaError_t launch_run32(const ClassRun &r, cudaStream_t st, const KArgs &a) {
         KArgs ar = a;
         ar.Y = r.ry32;
         ar.rys_tab = r.rys_tab;
+        ar.rys_tab32 = r.rys_tab32;
         return rys_launch(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, true, r.grid_r32, st, ar);
     }
     KArgs a32 = a;
@@ -924,6 +927,7 @@ struct fjb_handle {
     std::map<std::tuple<int, int, int, int>, std::pair<int, int>> cfg32;  // the FP32 interpreter's
     DevBuf<double> boys;
     DevBuf<double> rys;  // the tabulated Rys rule (rys_rule.h)
+    DevBuf<float> rys32;  // its FP32 copy (the Rys kernel's FP32 tier)
     DevBuf<unsigned char> df_work;  // fjb_df_jk's workspace
     DevBuf<int> df_err;
     int use_rys = 1;  // which classes the Rys kernel takes (fjb_set_rys)
@@ -1312,6 +1316,8 @@ int finish_create(std::unique_ptr<fjb_handle> &h, fjb_handle **out) {
     try {
         h->boys.upload(boys_table());
         h->rys.upload(rys_table_cached());
+        const std::vector<double> &t = rys_table_cached();
+        h->rys32.upload(std::vector<float>(t.begin(), t.end()));
         std::vector<int> off(h->basis.offsets), nc;
         for (auto &s : h->basis.shells) nc.push_back((s.l + 1) * (s.l + 2) / 2);
         h->sh_off.upload(off);
@@ -1486,6 +1492,7 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
             run.compiled = compiled_available(la, lb, lc, ld, false) && (th == 0 || th == 1);
             run.has32 = compiled_available(la, lb, lc, ld, true);
             run.rys_tab = h->rys.p;
+            run.rys_tab32 = h->rys32.p;
             run.unit0 = kv.second.first;
             run.n_units = kv.second.second;
             h->runs.push_back(run);

@@ -59,6 +59,7 @@ struct KArgs {
     // the Rys kernel (rys_fock.cuh): its layout and the tabulated rule
     RysDev Y;
     const double *rys_tab;
+    const float *rys_tab32;  // its FP32 copy (the FP32 tier)
     // the batched build: per molecule its context, per launch its molecule
     // (null: one molecule, the fields above)
     const MolCtx *mols;

@@ -33,9 +33,9 @@
 // as the VRR of the fused HGP build: the boundary is the same set of values
 // the HGP VRR produces, so the HRR and digest are the build's own.  Every
 // loop over Cartesians is a compile-time constant of the class.  R = double
-// is the plain FP64 path; R = float the routed path's FP32 tier (tables,
-// boundary and HRR in FP32; the rule, the scalars, densities and every J/K
-// accumulation FP64).
+// is the plain FP64 path; R = float the routed path's FP32 tier (the rule
+// from an FP32 copy of its table, the tables, boundary and HRR in FP32; T,
+// the pair scalars, densities and every J/K accumulation FP64).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -186,12 +186,13 @@ struct Shape {
     __host__ __device__ static constexpr int nt() { return NBF > 64 ? 256 : 128; }
     // CTAs an SM holds: 512 threads of 128 registers, unless the bra column
     // the boundary phase keeps in registers is too long to fit in those
-    // (df and ff bras in FP64, the ff bra in FP32): then half as many; the
-    // FP32 tier's small bras (up to 20 boundary values) fit six CTAs of 80
-    // registers, with no more than a few dozen bytes of spill
+    // (df and ff bras in FP64, the ff bra in FP32): then half as many; a bra
+    // column of at most 80 bytes (10 FP64 or 20 FP32 boundary values) fits
+    // six CTAs of 80 registers, with no more than a few dozen bytes of spill
     template <typename R>
     __host__ __device__ static constexpr int minb() {
-        return sizeof(R) == 4 && nt() == 128 && NBE <= 20 ? 6 : (nt() == 256 ? 2 : 4) / (NBE > (sizeof(R) == 8 ? 34 : 52) ? 2 : 1);
+        return nt() == 128 && NBE * (int)sizeof(R) <= 80 ? 6
+                                                          : (nt() == 256 ? 2 : 4) / (NBE > (sizeof(R) == 8 ? 34 : 52) ? 2 : 1);
     }
 };
 
@@ -227,6 +228,36 @@ __device__ __forceinline__ void rule_root(int r, double T, const double *__restr
         const double *a = tab + kRysAsym + (size_t)(N - 1) * kRysMaxN * 2;
         *x = __ldg(a + 2 * r) / T;
         *w = __ldg(a + 2 * r + 1) * (0.5 / sqrt(T));
+    }
+}
+
+// The same root in FP32 from the table's FP32 copy (the routed path's FP32
+// tier): the interval and its local coordinate from T in FP64, the series
+// in FP32 (relative error about 1e-6, inside the tier's own).
+template <int N>
+__device__ __forceinline__ void rule_root_f(int r, double T, const float *__restrict__ tab, float *x, float *w) {
+    if (T < kRysTSwitch) {
+        int i = (int)T;
+        if (i > kRysNI - 1) i = kRysNI - 1;
+        const float u = (float)(2.0 * (T - (double)i) - 1.0);
+        const float *blk = tab + ((size_t)(N - 1) * kRysNI + i) * kRysBlock + (size_t)(2 * r) * (kRysDeg + 1);
+        float bx1 = 0.f, bx2 = 0.f, bw1 = 0.f, bw2 = 0.f;
+        const float u2 = 2.f * u;
+#pragma unroll
+        for (int k = kRysDeg; k >= 1; --k) {
+            const float bx0 = u2 * bx1 - bx2 + __ldg(blk + k);
+            const float bw0 = u2 * bw1 - bw2 + __ldg(blk + kRysDeg + 1 + k);
+            bx2 = bx1;
+            bx1 = bx0;
+            bw2 = bw1;
+            bw1 = bw0;
+        }
+        *x = u * bx1 - bx2 + __ldg(blk);
+        *w = u * bw1 - bw2 + __ldg(blk + kRysDeg + 1);
+    } else {
+        const float *a = tab + kRysAsym + (size_t)(N - 1) * kRysMaxN * 2;
+        *x = (float)(__ldg(a + 2 * r) / T);
+        *w = (float)(__ldg(a + 2 * r + 1) * (0.5 / sqrt(T)));
     }
 }
 
@@ -433,32 +464,39 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
                     const double qi = q * inv, pi = p * inv;  // rho/p, rho/q
                     const double PQ[3] = {pb[0] - pk[0], pb[1] - pk[1], pb[2] - pk[2]};
                     const double T = rho * (PQ[0] * PQ[0] + PQ[1] * PQ[1] + PQ[2] * PQ[2]);
-                    double x, w;
-                    rys::rule_root<NR>(r, T, A.rys_tab, &x, &w);
-                    const double seedw = pb[7] * pk[7] * kTwoOverSqrtPi * sqrt(rho) * w;
-                    const double b00 = 0.5 * inv * x, b10 = pb[8] * (1.0 - qi * x), b01 = pk[8] * (1.0 - pi * x);
+                    // the rule and the 2D recurrences in R: FP64, or FP32 on
+                    // the routed FP32 tier (T and the pair scalars FP64)
+                    R x, w;
+                    if constexpr (sizeof(R) == 4) {
+                        rys::rule_root_f<NR>(r, T, A.rys_tab32, &x, &w);
+                    } else {
+                        rys::rule_root<NR>(r, T, A.rys_tab, &x, &w);
+                    }
+                    const R seedw = (R)(pb[7] * pk[7] * kTwoOverSqrtPi * sqrt(rho)) * w;
+                    const R b00 = (R)(0.5 * inv) * x, b10 = (R)pb[8] * ((R)1 - (R)qi * x),
+                            b01 = (R)pk[8] * ((R)1 - (R)pi * x);
                     R *out = tab + (size_t)g * KSTR + (size_t)(tl * NR + r) * (3 * TSP);
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
-                        const double c00 = pb[3 + d] - qi * PQ[d] * x, c00p = pk[3 + d] + pi * PQ[d] * x;
-                        double I[E + 1][F + 1];
-                        I[0][0] = d == 2 ? seedw : 1.0;
+                        const R c00 = (R)pb[3 + d] - (R)(qi * PQ[d]) * x, c00p = (R)pk[3 + d] + (R)(pi * PQ[d]) * x;
+                        R I[E + 1][F + 1];
+                        I[0][0] = d == 2 ? seedw : (R)1;
 #pragma unroll
                         for (int i = 0; i < E; ++i)
-                            I[i + 1][0] = c00 * I[i][0] + (i ? (double)i * b10 * I[i - 1][0] : 0.0);
+                            I[i + 1][0] = c00 * I[i][0] + (i ? (R)i * b10 * I[i - 1][0] : (R)0);
 #pragma unroll
                         for (int k = 0; k < F; ++k)
 #pragma unroll
                             for (int i = 0; i <= E; ++i) {
-                                double v = c00p * I[i][k];
-                                if (k) v += (double)k * b01 * I[i][k - 1];
-                                if (i) v += (double)i * b00 * I[i - 1][k];
+                                R v = c00p * I[i][k];
+                                if (k) v += (R)k * b01 * I[i][k - 1];
+                                if (i) v += (R)i * b00 * I[i - 1][k];
                                 I[i][k + 1] = v;
                             }
 #pragma unroll
                         for (int i = 0; i <= E; ++i)
 #pragma unroll
-                            for (int k = 0; k <= F; ++k) out[d * TSP + k * RPS + i] = (R)I[i][k];
+                            for (int k = 0; k <= F; ++k) out[d * TSP + k * RPS + i] = I[i][k];
                     }
                 }
                 __syncthreads();
