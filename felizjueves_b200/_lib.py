@@ -84,6 +84,12 @@ def load():
     L.fjb_set_rys.argtypes = [vp, C.c_int]
     L.fjb_set_route_check.argtypes = [vp, dbl, C.c_int]
     L.fjb_df_jk.argtypes = [vp, vp, i64, i64, vp, vp, vp, vp]
+    L.fjb_hjk_plan.argtypes = [vp, vp, dbl, C.c_int, C.c_int]
+    L.fjb_hjk_counts.argtypes = [vp, vp]
+    L.fjb_hjk_export.argtypes = [vp, vp, vp, vp, vp]
+    L.fjb_hjk_keys.argtypes = [vp, C.c_int, vp, vp]
+    L.fjb_hjk_k.argtypes = [vp, vp, vp, vp]
+    L.fjb_hjk_computed.argtypes = [vp, vp]
     L.fjb_df_eri3.argtypes = [vp, C.c_int, C.c_int, dbl, vp, C.POINTER(C.c_int32), vp]
     L.fjb_df_syrk.argtypes = [vp, vp, i64, i64, vp, vp]
     L.fjb_batch_create.argtypes = [C.POINTER(vp), vp, C.c_int]
@@ -120,6 +126,7 @@ EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_
            "fjb_last_build_stats", "fjb_launch_stats", "fjb_class_stats",
            "fjb_fma_probe", "fjb_fock_build_noalloc", "fjb_set_class_config", "fjb_set_class_config32",
            "fjb_set_rys", "fjb_set_route_check", "fjb_route_check_result", "fjb_df_jk", "fjb_df_eri3", "fjb_df_syrk",
+           "fjb_hjk_plan", "fjb_hjk_counts", "fjb_hjk_export", "fjb_hjk_keys", "fjb_hjk_k", "fjb_hjk_computed",
            "fjb_batch_create", "fjb_batch_set_densities", "fjb_batch_build", "fjb_batch_stats",
            "fjb_batch_last_error", "fjb_batch_destroy",
            "fjb_fock_build_graph", "fjb_create_df", "fjb_df_blocks", "fjb_mlp_n_params",

@@ -28,7 +28,7 @@ REPO = os.path.dirname(HERE)
 
 CU_SOURCES = ["fjb.cu", "fock_compiled.cu", "router.cu", "jengine.cu", "onee.cu", "rys_fock.cu",
               "rys_fock64.cu", "rys_fock32.cu", "df_mm.cu", "df_eri3.cu"]
-CPP_SOURCES = ["plan.cpp", "hgp_tables.cpp", "boys_table.cpp", "scatter.cpp", "rys_table.cpp"]
+CPP_SOURCES = ["plan.cpp", "hgp_tables.cpp", "boys_table.cpp", "scatter.cpp", "rys_table.cpp", "hjk_plan.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -407,6 +407,7 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
     const int nbe = C.nbe, nbf = C.nbf, L = C.L, n_ao = A.n_ao;
     const int nbnd = nbe * nbf;
     const bool tap = A.tap_out != nullptr;
+    const bool hk = A.hk != 0;
 
     const int n_todo = A.unit_list ? *A.unit_count : A.n_units;
     for (int ui = blockIdx.x; ui < n_todo; ui += gridDim.x) {
@@ -424,7 +425,7 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
             cb[i] = (R)((double)h.binom * ipow(bra.AB[0], h.px) * ipow(bra.AB[1], h.py) *
                         ipow(bra.AB[2], h.pz));
         }
-        if (!tap)
+        if (!tap && !hk)
             for (int i = tid; i < nab; i += nt) {
                 Dab[i] = A.D[(size_t)(bra.ao_a + i / nb) * n_ao + bra.ao_b + i % nb];
                 Jab[i] = 0.0;
@@ -436,6 +437,11 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
             if (ik < U.k1) {
                 if (tap) {
                     on = true;
+                } else if (hk) {  // K's one-block key (launch_hjk.py:153)
+                    const PairRec ket = A.pairs[LR.ket_pair0 + ik];
+                    const int x[4] = {bra.a, bra.b, ket.a, ket.b};
+                    const int r = (LR.pad0 >> 2) & 3, s_ = (LR.pad0 >> 6) & 3;
+                    on = !(bra.G * ket.G * A.Dsh[(size_t)x[r] * A.n_sh + x[s_]] < A.tau);
                 } else {
                     const PairRec ket = A.pairs[LR.ket_pair0 + ik];
                     on = !skip6(A.Dsh, A.n_sh, bra.a, bra.b, ket.a, ket.b, bra.G, ket.G, A.tau);
@@ -643,7 +649,7 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                     ck[i] = (R)((double)h.binom * ipow(ket.AB[0], h.px) * ipow(ket.AB[1], h.py) *
                                 ipow(ket.AB[2], h.pz));
                 }
-                if (!tap) {
+                if (!tap && !hk) {
                     const int oa = bra.ao_a, ob = bra.ao_b, oc = ket.ao_a, od = ket.ao_b;
                     for (int i = tid; i < ncd; i += nt)
                         Dcd[i] = A.D[(size_t)(oc + i / nd) * n_ao + od + i % nd];
@@ -672,6 +678,27 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                 if (tap) {
                     double *out = A.tap_out + A.tap_off[u] + (size_t)(ik - U.k0) * nab * ncd;
                     for (int i = tid; i < nab * ncd; i += nt) out[i] = Y[i];
+                    __syncthreads();
+                    continue;
+                }
+                if (hk) {
+                    // K[x_p][x_q] += sum_{k, l} D[x_r][x_s] (x_0 x_1|x_2 x_3), no weight:
+                    // every ordered quartet is visited once
+                    const int n4[4] = {na, nb, nc, nd};
+                    const int o4[4] = {bra.ao_a, bra.ao_b, ket.ao_a, ket.ao_b};
+                    const int p = LR.pad0 & 3, r = (LR.pad0 >> 2) & 3, q = (LR.pad0 >> 4) & 3,
+                              s_ = (LR.pad0 >> 6) & 3;
+                    const int st4[4] = {nb * ncd, ncd, nd, 1};  // strides of Y[e0][e1][e2][e3]
+                    for (int o = tid; o < n4[p] * n4[q]; o += nt) {
+                        const int i = o / n4[q], j = o - i * n4[q];
+                        double acc = 0.0;
+                        for (int k = 0; k < n4[r]; ++k) {
+                            const double *drow = A.D + (size_t)(o4[r] + k) * n_ao + o4[s_];
+                            const R *y = Y + (size_t)i * st4[p] + (size_t)j * st4[q] + (size_t)k * st4[r];
+                            for (int l = 0; l < n4[s_]; ++l) acc += drow[l] * (double)y[(size_t)l * st4[s_]];
+                        }
+                        atomicAdd(A.Kp + (size_t)(o4[p] + i) * n_ao + o4[q] + j, acc);
+                    }
                     __syncthreads();
                     continue;
                 }
@@ -735,9 +762,9 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
                 __syncthreads();
             }
         }
-        if (!tap && A.W)
+        if (!tap && !hk && A.W)
             for (int i = tid; i < nab; i += nt) A.wab[A.wab_off[u] + i] = Jab[i];  // reduced in unit order
-        else if (!tap)
+        else if (!tap && !hk)
             for (int i = tid; i < nab; i += nt)
                 atomicAdd(A.Jp + (size_t)(bra.ao_a + i / nb) * n_ao + bra.ao_b + i % nb, Jab[i]);
         if (A.computed && tid == 0 && n_list)
@@ -986,6 +1013,18 @@ struct fjb_handle {
     // a density-fitting handle: AO shells, then aux shells, then the unit shell
     bool df = false;
     int df_ao_shells = 0, df_aux_shells = 0;
+    // the split K build's stream (fjb_hjk_plan) and its staged records
+    bool hjk_planned = false, hjk_staged = false;
+    HjkPlan hjk;
+    DevBuf<PairRec> hk_pairs;
+    DevBuf<PrimRec> hk_prims;
+    DevBuf<LaunchRec> hk_launches;
+    DevBuf<Unit> hk_units;
+    DevBuf<unsigned long long> hk_computed;  // per launch: quartets the last fjb_hjk_k computed
+    struct HkRun {
+        int la, lb, lc, ld, unit0, n_units, max_kab, max_kcd;
+    };
+    std::vector<HkRun> hk_runs;
     // the three-centre kernel's records (fjb_df_eri3), staged on first use:
     // AO pairs (la >= lb) with their Schwarz factors, the aux shells as
     // (P, unit) pairs sorted by (l, degree, index), the per-class layouts
@@ -2139,6 +2178,250 @@ int fjb_df_jk(fjb_handle *h, const double *B_dev, int64_t n_aux, int64_t n_ao, c
     CUDA_OK(h, cudaMemcpyAsync(&err, h->df_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_OK(h, cudaStreamSynchronize(st));
     if (err) return fail(h, FJB_E_TIMEOUT, "fjb_df_jk: a tensor-core wait ran out (the GEMM did not complete)");
+    return FJB_OK;
+}
+
+int fjb_hjk_plan(fjb_handle *h, const double *D_host, double tau, int mode, int screen) {
+    if (!h || !D_host) return fail(h, FJB_E_ARG, "null argument");
+    if (h->df) return fail(h, FJB_E_STATE, "a density-fitting handle has no pair stream");
+    h->hjk_planned = h->hjk_staged = false;
+    try {
+        const unsigned nt = std::max(1u, std::thread::hardware_concurrency());
+        h->hjk = hjk_launches(h->basis, D_host, tau, mode, screen, (int)nt);
+    } catch (const std::length_error &e) {
+        return fail(h, FJB_E_LIMIT, e.what());
+    } catch (const std::invalid_argument &e) {
+        return fail(h, FJB_E_ARG, e.what());
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_PLAN, e.what());
+    }
+    h->hjk_planned = true;
+    return FJB_OK;
+}
+
+int fjb_hjk_counts(const fjb_handle *hc, int64_t *counts) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h || !counts) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->hjk_planned) return fail(h, FJB_E_STATE, "no split stream: call fjb_hjk_plan first");
+    const HjkPlan &P = h->hjk;
+    std::vector<std::array<int, 4>> cls;
+    for (size_t l = 0; l < P.launches.size(); ++l) cls.push_back(P.kernel_class((int)l, nullptr));
+    std::sort(cls.begin(), cls.end());
+    const int64_t n_cls = (int64_t)(std::unique(cls.begin(), cls.end()) - cls.begin());
+    // the skipped visits: every (bra pair, ket pair) of every launch
+    const int nt = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::vector<int64_t> skipped(nt, 0);
+    std::vector<std::thread> pool;
+    const size_t np = P.pairs.size();
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&, t]() {
+            int64_t n = 0;
+            for (size_t i = t; i < np; i += nt)
+                for (size_t j = 0; j < np; ++j) n += P.key(P.pairs[i], P.pairs[j]) < P.tau;
+            skipped[t] = n;
+        });
+    for (auto &th : pool) th.join();
+    int64_t sk = 0;
+    for (int64_t x : skipped) sk += x;
+    counts[0] = (int64_t)np;
+    counts[1] = (int64_t)P.batches.size();
+    counts[2] = (int64_t)P.launches.size();
+    counts[3] = n_cls;
+    counts[4] = (int64_t)np * (int64_t)np;
+    counts[5] = sk;
+    return FJB_OK;
+}
+
+int fjb_hjk_export(const fjb_handle *hc, int32_t *pairs, double *pair_G, int32_t *batches, int32_t *launches) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h) return fail(h, FJB_E_ARG, "null handle");
+    if (!h->hjk_planned) return fail(h, FJB_E_STATE, "no split stream: call fjb_hjk_plan first");
+    const HjkPlan &P = h->hjk;
+    if (pairs)
+        for (size_t i = 0; i < P.pairs.size(); ++i) {
+            const HjkPair &p = P.pairs[i];
+            const int32_t v[5] = {p.a, p.b, p.la, p.lb, p.degree};
+            std::copy(v, v + 5, pairs + 5 * i);
+        }
+    if (pair_G)
+        for (size_t i = 0; i < P.pairs.size(); ++i) pair_G[i] = P.pairs[i].G;
+    if (batches)
+        for (size_t i = 0; i < P.batches.size(); ++i) {
+            const HjkBatch &b = P.batches[i];
+            const int32_t v[5] = {b.la, b.lb, b.degree, b.p0, b.n};
+            std::copy(v, v + 5, batches + 5 * i);
+        }
+    if (launches)
+        for (size_t l = 0; l < P.launches.size(); ++l) {
+            std::array<int, 4> g;
+            const std::array<int, 4> o = P.ordered((int)l), k = P.kernel_class((int)l, &g);
+            int32_t *w = launches + 14 * l;
+            w[0] = P.launches[l].first;
+            w[1] = P.launches[l].second;
+            for (int j = 0; j < 4; ++j) {
+                w[2 + j] = o[j];
+                w[6 + j] = k[j];
+                w[10 + j] = g[j];
+            }
+        }
+    return FJB_OK;
+}
+
+int fjb_hjk_keys(const fjb_handle *hc, int launch, double *keys, uint8_t *skipped) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h) return fail(h, FJB_E_ARG, "null handle");
+    if (!h->hjk_planned) return fail(h, FJB_E_STATE, "no split stream: call fjb_hjk_plan first");
+    const HjkPlan &P = h->hjk;
+    if (launch < 0 || launch >= (int)P.launches.size()) return fail(h, FJB_E_ARG, "launch index out of range");
+    const HjkBatch &br = P.batches[P.launches[launch].first], &kt = P.batches[P.launches[launch].second];
+    size_t at = 0;
+    for (int i = 0; i < br.n; ++i)
+        for (int j = 0; j < kt.n; ++j, ++at) {
+            const double k = P.key(P.pairs[br.p0 + i], P.pairs[kt.p0 + j]);
+            if (keys) keys[at] = k;
+            if (skipped) skipped[at] = k < P.tau;
+        }
+    return FJB_OK;
+}
+
+int fjb_hjk_computed(fjb_handle *h, int64_t *per_launch) {
+    if (!h || !per_launch) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->hjk_staged) return fail(h, FJB_E_STATE, "no split K build yet (fjb_hjk_k)");
+    CUDA_OK(h, cudaSetDevice(h->device));
+    CUDA_OK(h, cudaDeviceSynchronize());
+    std::vector<unsigned long long> c(h->hjk.launches.size());
+    if (!c.empty())
+        CUDA_OK(h, cudaMemcpy(c.data(), h->hk_computed.p, c.size() * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < c.size(); ++i) per_launch[i] = (int64_t)c[i];
+    return FJB_OK;
+}
+
+namespace {
+
+// The split K build's records, staged once per stream: each launch's pairs
+// in its kernel class's orientation (kernel position j holds the ordered
+// quartet's position shells[j]; a pair reversed keeps its ordered G), the
+// launch's axes (shells' inverse) packed into LaunchRec.pad0, units of up to
+// 32 kets, grouped by kernel class.
+int stage_hjk(fjb_handle *h) {
+    if (h->hjk_staged) return FJB_OK;
+    const HjkPlan &P = h->hjk;
+    const HostBasis &B = h->basis;
+    std::vector<PairRec> pr;
+    std::vector<PrimRec> pm;
+    std::vector<LaunchRec> lr;
+    std::map<std::tuple<int, int, int, int>, std::vector<Unit>> by_class;
+    std::map<std::tuple<int, int, int, int>, std::pair<int, int>> deg;
+    auto add_list = [&](const HjkBatch &bt, bool reversed) {
+        const int p0 = (int)pr.size();
+        for (int i = 0; i < bt.n; ++i) {
+            const HjkPair &p = P.pairs[bt.p0 + i];
+            const int x = reversed ? p.b : p.a, y = reversed ? p.a : p.b;
+            const HostShell &sx = B.shells[x], &sy = B.shells[y];
+            const int K = (int)(sx.exps.size() * sy.exps.size());
+            pr.push_back(pair_record(B, x, y, p.G, (int)pm.size(), K));
+            for (int k = 0; k < K; ++k) pm.push_back(prim_record(sx, sy, k));
+        }
+        return p0;
+    };
+    for (size_t l = 0; l < P.launches.size(); ++l) {
+        std::array<int, 4> g;
+        const std::array<int, 4> kc = P.kernel_class((int)l, &g);
+        const HjkBatch &bra = P.batches[P.launches[l].first], &ket = P.batches[P.launches[l].second];
+        const bool swap = g[0] >= 2;  // the kernel's bra is the ordered ket
+        const HjkBatch &kb = swap ? ket : bra, &kk = swap ? bra : ket;
+        LaunchRec r{};
+        r.bra_pair0 = add_list(kb, g[0] != (swap ? 2 : 0));
+        r.n_bra = kb.n;
+        r.ket_pair0 = add_list(kk, g[2] != (swap ? 0 : 2));
+        r.n_ket = kk.n;
+        int axes[4];
+        for (int j = 0; j < 4; ++j) axes[g[j]] = j;
+        r.pad0 = axes[0] | axes[1] << 2 | axes[2] << 4 | axes[3] << 6;
+        const int li = (int)lr.size();
+        lr.push_back(r);
+        auto key = std::make_tuple(kc[0], kc[1], kc[2], kc[3]);
+        auto &d = deg[key];
+        d.first = std::max(d.first, kb.degree);
+        d.second = std::max(d.second, kk.degree);
+        for (int ib = 0; ib < kb.n; ++ib)
+            for (int k0 = 0; k0 < kk.n; k0 += kKetChunk)
+                by_class[key].push_back(Unit{li, ib, k0, std::min(kk.n, k0 + kKetChunk)});
+    }
+    std::vector<Unit> units;
+    h->hk_runs.clear();
+    for (auto &kv : by_class) {
+        auto [la, lb, lc, ld] = kv.first;
+        h->hk_runs.push_back({la, lb, lc, ld, (int)units.size(), (int)kv.second.size(), deg[kv.first].first,
+                              deg[kv.first].second});
+        units.insert(units.end(), kv.second.begin(), kv.second.end());
+    }
+    try {
+        h->hk_pairs.upload(pr);
+        h->hk_prims.upload(pm);
+        h->hk_launches.upload(lr);
+        h->hk_units.upload(units);
+        h->hk_computed.alloc(std::max<size_t>(1, lr.size()));
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, e.what());
+    }
+    h->hjk_staged = true;
+    return FJB_OK;
+}
+
+}  // namespace
+
+int fjb_hjk_k(fjb_handle *h, const double *D_dev, double *K_dev, void *stream) {
+    if (!h || !D_dev || !K_dev) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->hjk_planned) return fail(h, FJB_E_STATE, "no split stream: call fjb_hjk_plan first");
+    if (h->hjk.screen != kHjkScreenK)
+        return fail(h, FJB_E_STATE, "the stream was planned with J's key, which does not bound K's deposits");
+    if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
+    CUDA_OK(h, cudaSetDevice(h->device));
+    if (int rc = stage_hjk(h)) return rc;
+    if (int rc = ensure_smem_attr(h)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nsh = (int)h->basis.shells.size(), nao = h->basis.n_ao;
+    try {
+        if (h->Dsh.n < (size_t)nsh * nsh) h->Dsh.alloc((size_t)nsh * nsh);
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, e.what());
+    }
+    density_blocks_kernel<<<(nsh * nsh + 255) / 256, 256, 0, st>>>(D_dev, nao, nsh, h->sh_off.p, h->sh_nc.p,
+                                                                 h->Dsh.p);
+    CUDA_OK(h, cudaMemsetAsync(K_dev, 0, (size_t)nao * nao * sizeof(double), st));
+    CUDA_OK(h, cudaMemsetAsync(h->hk_computed.p, 0, h->hk_computed.n * sizeof(unsigned long long), st));
+    for (const auto &r : h->hk_runs) {
+        ClassEntry *ce;
+        ClassDev dev;
+        try {
+            ce = &h->cls(r.la, r.lb, r.lc, r.ld);
+            dev = ce->dev(r.max_kab, r.max_kcd);
+        } catch (const std::length_error &e) {
+            return fail(h, FJB_E_LIMIT, e.what());
+        } catch (const std::exception &e) {
+            return fail(h, FJB_E_CUDA, e.what());
+        }
+        KArgs a{};
+        a.C = dev;
+        a.units = h->hk_units.p + r.unit0;
+        a.n_units = r.n_units;
+        a.launches = h->hk_launches.p;
+        a.pairs = h->hk_pairs.p;
+        a.prims = h->hk_prims.p;
+        a.D = D_dev;
+        a.Dsh = h->Dsh.p;
+        a.n_sh = nsh;
+        a.n_ao = nao;
+        a.tau = h->hjk.tau;
+        a.Kp = K_dev;
+        a.boys_tab = h->boys.p;
+        a.hk = 1;
+        a.computed = h->hk_computed.p;
+        CUDA_OK(h, launch_hgp<double>(dev, grid_for(dev, a.n_units), st, a));
+    }
+    CUDA_OK(h, cudaGetLastError());
     return FJB_OK;
 }
 

@@ -45,6 +45,11 @@ struct KArgs {
     double *Jp, *Kp;
     double *tap_out;        // ERI tap mode when non-null
     const int64_t *tap_off; // per unit
+    // the split K build (fjb_hjk_k; HGP interpreter only): every visited
+    // quartet deposits K[x_p][x_q] += D[x_r][x_s] (x_0 x_1|x_2 x_3) into Kp
+    // alone, (p, r, q, s) = the launch's axes (LaunchRec.pad0, two bits
+    // each), and is skipped when (G_bra G_ket) max|D_{x_r x_s}| < tau
+    int hk;
     const double *boys_tab;
     const uint8_t *route;   // per unit ket flags, routed mode (null: all FP64)
     double route_thresh;

@@ -19,11 +19,11 @@
 //   * batch pairs I <= J: screened when mag_I + mag_J >= n (refused unless
 //     max G_I * max G_J < tau), launched otherwise.
 // Every step is written to give the reference's floating-point results
-// operation for operation; the one deliberate difference is F_m(0), which
-// the bound takes as the exact 1/(2m+1) where the reference evaluates its
-// quadrature at T = 0 (within a few ulps of it).  The integer lists are held
+// operation for operation; F_m(0) is the reference's own quadrature value
+// (boys_zero.h), a few ulps from 1/(2m+1).  The lists and bounds are held
 // equal to the reference's own on the seeded workloads by tests/test_plan.py.
 #include "plan.h"
+#include "boys_zero.h"
 
 #include <algorithm>
 #include <array>
@@ -120,9 +120,9 @@ void hermite_bounds(double zeta, int L, const std::vector<Cart3> &hs, double *I)
     for (size_t k = 0; k < hs.size(); ++k) {
         const Cart3 &p = hs[k];
         int M = p[0] + p[1] + p[2];
-        // fundamental(M, 0, theta) with F_M(0) = 1/(2M+1)
-        double v = two_over_sqrt_pi * theta * std::pow(-2.0 * t2, (double)M) *
-                   (1.0 / (double)(2 * M + 1));
+        // fundamental(M, 0, theta) with F_M(0) the reference's own value
+        if (M > kBoysZeroMax) throw std::invalid_argument("Hermite order above the F_m(0) table");
+        double v = two_over_sqrt_pi * theta * std::pow(-2.0 * t2, (double)M) * kBoysZero[M];
         // the recursion's integer factors, innermost (z) first
         for (int q = 1; q <= p[2]; ++q) v = (double)(2 * q - 1) * v;
         for (int q = 1; q <= p[1]; ++q) v = (double)(2 * q - 1) * v;

@@ -59,7 +59,7 @@ std::vector<Cart3> carts(int l);
 // Gaussian-product factor exp(zeta pa pb) in E^{00}_0.
 void e_axis(int i, int j, double zeta, double pa, double pb, double *e);
 // I_p = sqrt((-1)^|p| [2p]^(0)(PQ = 0, theta = sqrt(zeta/2))) for every p of
-// hs (ao/pairs.py:270-287), with F_M(0) = 1/(2M+1).
+// hs (ao/pairs.py:270-287), with F_M(0) the reference's own (boys_zero.h).
 void hermite_bounds(double zeta, int L, const std::vector<Cart3> &hs, double *I);
 
 // G_[ab] of every primitive pair of the ordered shell pair (a, b), in
@@ -81,5 +81,39 @@ struct PairBounds {
 // densities (an SCF loop) compute them once.
 Plan f_launches(const HostBasis &basis, const double *D, double tau, int n, int threads,
                 std::vector<PairBounds> *bounds = nullptr);
+
+// The split build's ordered pair stream (eri/hjk/launch_hjk.py:280
+// hjk_launches): every ORDERED shell pair (a, b) with G = fsum of its
+// primitive bounds, nothing pruned; bins (la, lb, degree) in sorted order,
+// pairs descending by G, stably (a outer, b inner); every ordered batch pair
+// a launch; every ordered quartet of shell pairs a visit with the key
+// G_ab G_cd max|D_bd| (screen K) or G_ab G_cd max|D_cd| (screen J), skipped
+// when the key is below tau.  Visits are not stored (n_pairs^2 of them):
+// hjk_key gives any one, in the plan's order.
+struct HjkPair {
+    int a, b, la, lb, degree;
+    double G;
+};
+struct HjkBatch {
+    int la, lb, degree, p0, n;  // its pairs: pairs[p0, p0 + n)
+};
+struct HjkPlan {
+    double tau = 0.0;
+    int mode = 0;    // 0 ordered (each launch its own class), 1 canonical
+    int screen = 1;  // 0 J's key, 1 K's key
+    int n_sh = 0;
+    std::vector<HjkPair> pairs;  // batch by batch, in batch order
+    std::vector<HjkBatch> batches;
+    std::vector<std::pair<int, int>> launches;  // (bra batch, ket batch), bra outer
+    std::vector<double> dmax;                    // n_sh x n_sh: max |D| of each shell block
+    // a launch's kernel class and the shell positions that class reads:
+    // kernel position j holds the ordered quartet's position shells[j]
+    std::array<int, 4> ordered(int launch) const;
+    std::array<int, 4> kernel_class(int launch, std::array<int, 4> *shells) const;
+    double key(const HjkPair &p, const HjkPair &q) const;
+};
+constexpr int kHjkModeOrdered = 0, kHjkModeCanonical = 1, kHjkScreenJ = 0, kHjkScreenK = 1;
+
+HjkPlan hjk_launches(const HostBasis &basis, const double *D, double tau, int mode, int screen, int threads);
 
 }  // namespace fjb

@@ -448,6 +448,62 @@ class FockEngine:
         return [{k: getattr(arr[i], k) for k, _ in _lib.ClassStat_t._fields_}
                 for i in range(nc.value)]
 
+    # --- the split build's ordered pair stream (eri/hjk/launch_hjk.py) -----
+
+    HJK_MODES = {"ordered": 0, "canonical": 1}
+    HJK_SCREENS = {"j": 0, "k": 1}
+
+    def hjk_plan(self, D, tau: float = 1e-12, *, mode: str = "ordered", screen: str = "k") -> dict:
+        """The split build's stream (fjb_hjk_plan; `hjk_launches`): every
+        ordered shell pair, bins (la, lb, degree), every ordered batch pair
+        a launch.  Returns its lists as arrays: `pairs` (a, b, la, lb,
+        degree) in batch order, `pair_G`, `batches` (la, lb, degree, first
+        pair, pairs), `launches` (bra, ket, ordered class, kernel class,
+        shells), and `counts` (pairs, batches, launches, classes, quartets,
+        quartets_skipped)."""
+        if mode not in self.HJK_MODES:
+            raise ValueError(f"mode = {mode!r} is not one of {tuple(self.HJK_MODES)}")
+        if screen not in self.HJK_SCREENS:
+            raise ValueError(f"screen = {screen!r} is not one of {tuple(self.HJK_SCREENS)}")
+        Dh = _checked_density(self.basis, D)
+        _lib.check(self._L.fjb_hjk_plan(self._h, Dh.ctypes.data, float(tau), self.HJK_MODES[mode],
+                                        self.HJK_SCREENS[screen]), self._h)
+        cnt = np.zeros(6, np.int64)
+        _lib.check(self._L.fjb_hjk_counts(self._h, cnt.ctypes.data), self._h)
+        n_p, n_b, n_l = int(cnt[0]), int(cnt[1]), int(cnt[2])
+        pairs = np.zeros((n_p, 5), np.int32)
+        pair_G = np.zeros(n_p)
+        batches = np.zeros((n_b, 5), np.int32)
+        launches = np.zeros((n_l, 14), np.int32)
+        _lib.check(self._L.fjb_hjk_export(self._h, pairs.ctypes.data, pair_G.ctypes.data, batches.ctypes.data,
+                                          launches.ctypes.data), self._h)
+        names = ("pairs", "batches", "launches", "classes", "quartets", "quartets_skipped")
+        return {"pairs": pairs, "pair_G": pair_G, "batches": batches, "launches": launches,
+                "counts": dict(zip(names, map(int, cnt)))}
+
+    def hjk_keys(self, launch: int, n_visits: int) -> tuple[np.ndarray, np.ndarray]:
+        """One launch's visit keys and skip flags (bra pair outer)."""
+        keys = np.zeros(n_visits)
+        skipped = np.zeros(n_visits, np.uint8)
+        _lib.check(self._L.fjb_hjk_keys(self._h, int(launch), keys.ctypes.data, skipped.ctypes.data), self._h)
+        return keys, skipped.astype(bool)
+
+    def hjk_k(self, D, K=None, stream=None):
+        """K over the split stream (fjb_hjk_k): every ordered quartet not
+        skipped by K's key deposits K[a][c] += D[b][d] (ab|cd)."""
+        import torch
+        if K is None:
+            K = torch.empty_like(D)
+        st = stream if stream is not None else torch.cuda.current_stream(D.device)
+        _lib.check(self._L.fjb_hjk_k(self._h, D.data_ptr(), K.data_ptr(), C.c_void_p(st.cuda_stream)), self._h)
+        return K
+
+    def hjk_computed(self, n_launches: int) -> np.ndarray:
+        """Per launch, the quartets the last hjk_k computed on the device."""
+        out = np.zeros(n_launches, np.int64)
+        _lib.check(self._L.fjb_hjk_computed(self._h, out.ctypes.data), self._h)
+        return out
+
     def screen_mask(self, D, at=None) -> np.ndarray:
         """Per launched quartet (launch, bra pair, ket pair order), 1 when
         the six-block screen skips it (walk_f.py:344-380); only the entries

@@ -186,6 +186,46 @@ int fjb_eri_blocks(fjb_handle *h, const int32_t *quartets, int n, double *out_de
 int fjb_eri_blocks_fp32(fjb_handle *h, const int32_t *quartets, int n, double *out_dev,
                         int64_t *offsets);
 
+/* The split build's ordered pair stream and its K build
+ * (eri/hjk/launch_hjk.py:280 hjk_launches; eri/hjk/kernel_hk.py:324
+ * build_hk_kernel).  fjb_hjk_plan: every ORDERED shell pair (a, b) with G
+ * the fsum of its primitive Schwarz bounds (none pruned), bins (la, lb,
+ * degree) in sorted order, pairs descending by G stably, every ordered batch
+ * pair a launch, every ordered quartet of pairs a visit with the key
+ * (G_ab G_cd) max|D_bd| (screen FJB_HJK_SCREEN_K, k_key) or (G_ab G_cd)
+ * max|D_cd| (FJB_HJK_SCREEN_J, j_key), skipped when below tau.  mode
+ * FJB_HJK_ORDERED runs each launch on its own class; FJB_HJK_CANONICAL on
+ * the first member of its 8-fold orbit (the reference's GROUP order) with
+ * la <= lb, lc <= ld, (la, lb) <= (lc, ld), this library's compiled classes
+ * (the reference's canonical mode takes its cheapest generated recurrence
+ * instead; launches and visits are the same).  D_host is n_ao^2, exactly
+ * symmetric; refusals as the reference's (FJB_E_ARG; FJB_E_LIMIT for a
+ * degree above 128).
+ * fjb_hjk_counts: counts[6] = pairs, batches, launches, kernel classes,
+ * visits (pairs^2), skipped visits (a host sweep over every visit).
+ * fjb_hjk_export (HOST arrays, each may be NULL): pairs[5 n_pairs] = (a, b,
+ * la, lb, degree) in batch order, pair_G[n_pairs], batches[5 n_batches] =
+ * (la, lb, degree, first pair, pairs), launches[14 n_launches] = (bra
+ * batch, ket batch, ordered class[4], kernel class[4], shells[4]: kernel
+ * position j reads the ordered quartet's position shells[j]).
+ * fjb_hjk_keys: one launch's visit keys (bra pair outer) and skip flags.
+ * fjb_hjk_k: K (DEVICE, n_ao^2) = sum over every visit not skipped of
+ * K[a][c] += D[b][d] (ab|cd), no weights (each ordered quartet once), on
+ * the HGP interpreter, the key evaluated on the device in the plan's
+ * operation order; needs a stream planned with K's key.  Stream-ordered. */
+#define FJB_HJK_ORDERED 0
+#define FJB_HJK_CANONICAL 1
+#define FJB_HJK_SCREEN_J 0
+#define FJB_HJK_SCREEN_K 1
+int fjb_hjk_plan(fjb_handle *h, const double *D_host, double tau, int mode, int screen);
+int fjb_hjk_counts(const fjb_handle *h, int64_t *counts);
+int fjb_hjk_export(const fjb_handle *h, int32_t *pairs, double *pair_G, int32_t *batches, int32_t *launches);
+int fjb_hjk_keys(const fjb_handle *h, int launch, double *keys, uint8_t *skipped);
+int fjb_hjk_k(fjb_handle *h, const double *D_dev, double *K_dev, void *stream);
+/* Per launch (HOST, n_launches): the quartets the last fjb_hjk_k computed
+ * (visits not skipped by the device's key).  Synchronises the device. */
+int fjb_hjk_computed(fjb_handle *h, int64_t *per_launch);
+
 /* Density fitting (eri/density_fit/metric.py:228 metric_matrix,
  * eri3.py:226 eri3_tensor).  fjb_create_df makes a handle over the AO basis
  * (l <= 3) and an auxiliary basis (l <= FJB_MAX_L_AUX); an auxiliary

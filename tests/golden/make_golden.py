@@ -10,7 +10,7 @@ files this script writes.
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
 parts: libcint boys eri plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 scatter_c0 onee
-scf bse harmonics grad rys (default: all
+scf bse harmonics grad rys hjk_c0 boys_zero (default: all
 but plan_c1 and jk_small, which take minutes).
 """
 
@@ -734,6 +734,75 @@ def part_jplan_c0():
     print("jplan_c0", sum(len(v) for v in bras.values()), "records,", round(time.time() - t, 1), "s")
 
 
+# --- F_m(0) as the reference's Boys function returns it ---------------------
+
+
+def part_boys_zero():
+    """felizjueves_b200/csrc/boys_zero.h: the reference's F_m(0), m = 0..24
+    (its quadrature at T = 0 lands a few ulps from 1/(2m+1)), the table the
+    plans' pair bounds read so that they are the reference's to the bit."""
+    _ref_imports()
+    from felizjueves.reference.boys import boys
+    vals = [boys(m, 0.0) for m in range(25)]
+    lines = ["// boys_zero.h -- F_m(0), m = 0..24, as the reference's Boys function returns",
+             "// them (reference/boys.py:218 _boys: 112-node Gauss-Legendre quadrature at",
+             "// T = 0, a few ulps from 1/(2m+1)).  Written by tests/golden/make_golden.py",
+             "// part boys_zero.  The plans' primitive Schwarz bounds read these, so the",
+             "// bounds, and the orders they decide, are the reference's to the bit.",
+             "#pragma once", "", "namespace fjb {", "", "constexpr int kBoysZeroMax = 24;",
+             "constexpr double kBoysZero[kBoysZeroMax + 1] = {"]
+    lines += [f"    {v.hex()},  // m = {m}" for m, v in enumerate(vals)]
+    lines += ["};", "", "}  // namespace fjb", ""]
+    with open(os.path.join(REPO, "felizjueves_b200", "csrc", "boys_zero.h"), "w") as f:
+        f.write("\n".join(lines))
+
+
+# --- the split build's ordered pair stream (eri/hjk/launch_hjk.py) ----------
+
+
+def part_hjk_c0():
+    """hjk_launches on c0 in ordered mode, screens "k" and "j" at c0's tau and
+    at 1e-6: pairs, batches, launches in full; the visit keys (n_pairs^2
+    of them) as a SHA-256 of their float64 bytes in visit order and a
+    strided sample; the skipped mask as a SHA-256 of its packed bits and its
+    first 2,000 skipped indices."""
+    import hashlib
+    _ref_imports()
+    from felizjueves.ao.pairs import primitive_schwarz_bounds
+    from felizjueves.eri.hjk.launch_hjk import hjk_launches
+    from felizjueves.reference.pq import one_centre
+    from felizjueves_b200 import configs
+    w = configs.c0()
+    rb = ref_basis(w.basis)
+    bound = partial(primitive_schwarz_bounds, one_centre=one_centre)
+    out = {}
+    t = time.time()
+    for screen in ("k", "j"):
+        for tau in (w.tau, 1e-6):
+            P = hjk_launches(rb, w.D.tolist(), bound=bound, tau=tau, mode="ordered", screen=screen)
+            tag = f"{screen}_{'c0tau' if tau == w.tau else '1e-6'}"
+            keys = np.array([v.key for v in P.visits], np.float64)
+            out[f"{tag}_keys_sha256"] = hashlib.sha256(keys.tobytes()).hexdigest()
+            out[f"{tag}_keys_sample"] = keys[::997].copy()
+            mask = np.array([v.skipped for v in P.visits], bool)
+            out[f"{tag}_skipped_sha256"] = hashlib.sha256(np.packbits(mask).tobytes()).hexdigest()
+            out[f"{tag}_skipped_head"] = np.nonzero(mask)[0][:2000].astype(np.int64)
+            out[f"{tag}_counts"] = json.dumps(P.counts())
+            if screen == "k" and tau == w.tau:
+                pairs = P.pairs
+                out["pair_ab"] = np.array([(q.a, q.b) for q in pairs], np.int32)
+                out["pair_l_deg"] = np.array([(q.la, q.lb, q.degree) for q in pairs], np.int32)
+                out["pair_G"] = np.array([q.G for q in pairs], np.float64)
+                out["batch_key"] = np.array([(b.la, b.lb, b.degree) for b in P.batches], np.int32)
+                out["batch_npairs"] = np.array([len(b.pairs) for b in P.batches], np.int32)
+                out["launches"] = np.array([(L.bra, L.ket) for L in P.launches], np.int32)
+                out["launch_cls"] = np.array([L.ordered for L in P.launches], np.int32)
+            print("hjk", tag, P.counts(), round(time.time() - t, 1), "s", flush=True)
+            del P
+    out["tau"] = w.tau
+    np.savez_compressed(os.path.join(HERE, "hjk_c0.npz"), **out)
+
+
 # --- the reference's FLOP model (hgp/cost.py) for every class to L=3 ---------
 
 
@@ -771,7 +840,8 @@ PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_
          "cpu_c0": part_cpu_c0,
          "cost": part_cost, "jplan_c0": part_jplan_c0, "scatter_c0": part_scatter_c0,
          "onee": part_onee, "scf": part_scf, "bse": part_bse,
-         "harmonics": part_harmonics, "grad": part_grad, "rys": part_rys}
+         "harmonics": part_harmonics, "grad": part_grad, "rys": part_rys,
+         "hjk_c0": part_hjk_c0, "boys_zero": part_boys_zero}
 DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
 
 

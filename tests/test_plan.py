@@ -1,6 +1,6 @@
 """The pair stream built by libfjb (plan.cpp) against the reference's own
 f_launches (eri/fock/launch_f.py:390) on the seeded workloads: every integer
-list bit-exact, the bounds to the ulp.  Runs through the C ABI on a host-only
+list and bound bit-exact.  Runs through the C ABI on a host-only
 handle (device -1): no GPU."""
 
 import numpy as np
@@ -35,9 +35,9 @@ def test_plan_lists_bit_exact(lib_built, wname):
     assert P.magnitudes == tuple(g["magnitudes"])
     assert P.eps == float(g["eps"]) and P.g_max == float(g["g_max"])
     assert P.n_prim_total == int(g["n_prim_total"])
-    # bounds: the only deliberate difference is F_m(0) = 1/(2m+1) exactly
+    # bounds: to the bit (F_m(0) is the reference's own quadrature value)
     G = np.array([p.G for p in pairs])
-    assert np.max(np.abs(G - g["pair_G"]) / g["pair_G"]) < 1e-15
+    assert np.array_equal(G, g["pair_G"])
     assert np.array_equal(np.array([p.dmax for p in pairs]), g["pair_dmax"])
     import json
     assert P.counts() == json.loads(str(g["counts"]))
