@@ -489,8 +489,13 @@ def side_path(a, local):
         eng = FockEngine(w.basis, device=local)
         J = torch.empty_like(D)
         ms, _ = timed(lambda: eng.coulomb(D, tau=w.tau, J=J))
+        J64 = J.clone()
+        ms32, _ = timed(lambda: eng.coulomb(D, tau=w.tau, J=J, threshold=a.threshold))
         line.update(metric="J-engine J build ms/iter", value=round(ms, 3), unit="ms/iter",
-                    gpu_launches=eng.j_launches())
+                    gpu_launches=eng.j_launches(),
+                    fp32_tier={"threshold": a.threshold, "ms": round(ms32, 3),
+                               "speedup_vs_fp64": round(ms / ms32, 4),
+                               "max_abs_dJ_vs_fp64": float((J - J64).abs().max())})
     elif a.path == "onee":
         # S, T, V and H = T + V; one nucleus of charge 1 + (k mod 9) per atom
         from felizjueves_b200.fock import FockEngine

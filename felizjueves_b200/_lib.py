@@ -112,6 +112,7 @@ def load():
     L.fjb_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_float, C.c_int, vp]
     L.fjb_route_stats.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
     L.fjb_coulomb.argtypes = [vp, vp, vp, dbl, vp]
+    L.fjb_coulomb_mixed.argtypes = [vp, vp, vp, dbl, dbl, vp]
     L.fjb_j_last_launches.argtypes = [vp]
     L.fjb_j_plan_lists.argtypes = [vp, vp, C.POINTER(JLists_t), C.POINTER(i64)]
     L.fjb_scatter_map.argtypes = [vp, C.c_int, vp, vp, vp, C.POINTER(i64), C.POINTER(i64)]
@@ -131,7 +132,7 @@ EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_
            "fjb_batch_last_error", "fjb_batch_destroy",
            "fjb_fock_build_graph", "fjb_create_df", "fjb_df_blocks", "fjb_mlp_n_params",
            "fjb_router_set", "fjb_router_features", "fjb_mlp_forward", "fjb_mlp_gradient",
-           "fjb_mlp_adam", "fjb_route_stats", "fjb_coulomb", "fjb_j_last_launches",
+           "fjb_mlp_adam", "fjb_route_stats", "fjb_coulomb", "fjb_coulomb_mixed", "fjb_j_last_launches",
            "fjb_j_plan_lists", "fjb_scatter_map", "fjb_one_electron")
 
 

@@ -2683,10 +2683,15 @@ int fjb_scatter_map(const fjb_handle *hc, int launch, int32_t *el, int32_t *ptr,
 }
 
 int fjb_coulomb(fjb_handle *h, const double *D_dev, double *J_dev, double tau, void *stream) {
+    return fjb_coulomb_mixed(h, D_dev, J_dev, tau, 0.0, stream);
+}
+
+int fjb_coulomb_mixed(fjb_handle *h, const double *D_dev, double *J_dev, double tau, double threshold, void *stream) {
     if (!h || !D_dev || !J_dev) return fail(h, FJB_E_ARG, "null argument");
     if (h->device < 0) return fail(h, FJB_E_STATE, "host-only handle (device -1): no device work");
     if (h->df) return fail(h, FJB_E_STATE, "a density-fitting handle has no J-engine");
     if (!std::isfinite(tau) || tau < 0.0) return fail(h, FJB_E_ARG, "tau must be finite and >= 0");
+    if (!std::isfinite(threshold) || threshold < 0.0) return fail(h, FJB_E_ARG, "threshold must be finite and >= 0");
     CUDA_OK(h, cudaSetDevice(h->device));
     std::string err;
     if (!h->jeng) {
@@ -2694,7 +2699,7 @@ int fjb_coulomb(fjb_handle *h, const double *D_dev, double *J_dev, double tau, v
         if (!h->jeng) return fail(h, FJB_E_CUDA, err);
     }
     int nl = 0;
-    if (jengine_build(h->jeng, D_dev, J_dev, tau, h->boys.p, (cudaStream_t)stream, &err, &nl))
+    if (jengine_build(h->jeng, D_dev, J_dev, tau, threshold, h->boys.p, (cudaStream_t)stream, &err, &nl))
         return fail(h, FJB_E_CUDA, err);
     h->j_launches = nl;
     return FJB_OK;

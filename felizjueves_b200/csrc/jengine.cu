@@ -181,53 +181,53 @@ __host__ __device__ constexpr int hc_idx(int t, int u, int v) {
 // and the J_p partials stay in registers.
 // One entry I of the R recursion: [r]^(m) = PQ_d [r-1_d]^(m+1) + (r_d - 1)
 // [r-2_d]^(m+1), d the first nonzero axis.
-template <int I>
-__device__ __forceinline__ void r_entry(double *R, double X, double Y, double Z) {
+template <int I, typename T>
+__device__ __forceinline__ void r_entry(T *R, T X, T Y, T Z) {
     constexpr int t = hc_t(I), u = hc_u(I), v = hc_v(I);
     if constexpr (t > 0) {
-        double x = X * R[hc_idx(t - 1, u, v)];
-        if constexpr (t >= 2) x += (double)(t - 1) * R[hc_idx(t - 2, u, v)];
+        T x = X * R[hc_idx(t - 1, u, v)];
+        if constexpr (t >= 2) x += (T)(t - 1) * R[hc_idx(t - 2, u, v)];
         R[I] = x;
     } else if constexpr (u > 0) {
-        double x = Y * R[hc_idx(0, u - 1, v)];
-        if constexpr (u >= 2) x += (double)(u - 1) * R[hc_idx(0, u - 2, v)];
+        T x = Y * R[hc_idx(0, u - 1, v)];
+        if constexpr (u >= 2) x += (T)(u - 1) * R[hc_idx(0, u - 2, v)];
         R[I] = x;
     } else {
-        double x = Z * R[hc_idx(0, 0, v - 1)];
-        if constexpr (v >= 2) x += (double)(v - 1) * R[hc_idx(0, 0, v - 2)];
+        T x = Z * R[hc_idx(0, 0, v - 1)];
+        if constexpr (v >= 2) x += (T)(v - 1) * R[hc_idx(0, 0, v - 2)];
         R[I] = x;
     }
 }
-template <int I0, int... K>
-__device__ __forceinline__ void r_entries(double *R, double X, double Y, double Z, std::integer_sequence<int, K...>) {
-    (r_entry<I0 + K>(R, X, Y, Z), ...);
+template <int I0, typename T, int... K>
+__device__ __forceinline__ void r_entries(T *R, T X, T Y, T Z, std::integer_sequence<int, K...>) {
+    (r_entry<I0 + K, T>(R, X, Y, Z), ...);
 }
 // Totals S, S-1, .. 1 of one level (descending: each reads the level above
 // at totals S-1 and S-2 before they are rewritten).
-template <int S>
+template <int S, typename T>
 struct RTotals {
-    static __device__ __forceinline__ void run(double *R, double X, double Y, double Z) {
+    static __device__ __forceinline__ void run(T *R, T X, T Y, T Z) {
         if constexpr (S >= 1) {
-            r_entries<nh(S - 1)>(R, X, Y, Z, std::make_integer_sequence<int, nh(S) - nh(S - 1)>{});
-            RTotals<S - 1>::run(R, X, Y, Z);
+            r_entries<nh(S - 1), T>(R, X, Y, Z, std::make_integer_sequence<int, nh(S) - nh(S - 1)>{});
+            RTotals<S - 1, T>::run(R, X, Y, Z);
         }
     }
 };
 // Levels M, M-1, .. 0 of R_{tuv} at total order L.
-template <int L, int M>
+template <int L, int M, typename T>
 struct RLevels {
-    static __device__ __forceinline__ void run(double *R, const double *f, double X, double Y, double Z) {
+    static __device__ __forceinline__ void run(T *R, const T *f, T X, T Y, T Z) {
         if constexpr (M >= 0) {
-            RTotals<L - M>::run(R, X, Y, Z);
+            RTotals<L - M, T>::run(R, X, Y, Z);
             R[0] = f[M];
-            RLevels<L, M - 1>::run(R, f, X, Y, Z);
+            RLevels<L, M - 1, T>::run(R, f, X, Y, Z);
         }
     }
 };
 // d[q] = (-1)^|q| D_q.
-template <int... Q>
-__device__ __forceinline__ void signed_dq(double *d, const double *dq, std::integer_sequence<int, Q...>) {
-    ((d[Q] = ((hc_total(Q) & 1) ? -1.0 : 1.0) * __ldg(dq + Q)), ...);
+template <typename T, int... Q>
+__device__ __forceinline__ void signed_dq(T *d, const double *dq, std::integer_sequence<int, Q...>) {
+    ((d[Q] = (T)(((hc_total(Q) & 1) ? -1.0 : 1.0) * __ldg(dq + Q))), ...);
 }
 // jp[p] += R_{p+q} d[q] over I = p * NQ + q.
 template <int NQ, int I>
@@ -235,9 +235,8 @@ struct PQIndex {
     static constexpr int pi = I / NQ, qi = I % NQ;
     static constexpr int r = hc_idx(hc_t(pi) + hc_t(qi), hc_u(pi) + hc_u(qi), hc_v(pi) + hc_v(qi));
 };
-template <int NQ, int... I>
-__device__ __forceinline__ void contract(double *jp, const double *R, const double *d,
-                                         std::integer_sequence<int, I...>) {
+template <int NQ, typename T, int... I>
+__device__ __forceinline__ void contract(T *jp, const T *R, const T *d, std::integer_sequence<int, I...>) {
     ((jp[PQIndex<NQ, I>::pi] += R[PQIndex<NQ, I>::r] * d[PQIndex<NQ, I>::qi]), ...);
 }
 
@@ -245,12 +244,16 @@ __device__ __forceinline__ void contract(double *jp, const double *R, const doub
 // every index a compile-time constant.
 constexpr int kSmallL = 6;
 
+// thr32 > 0: a chunk of kets whose first (largest) bound I_bra key is below
+// it runs R, D_q and the contraction in FP32 (T, the Boys values and the
+// J_p sums stay FP64): the FP32 E/R tier.  The kets are sorted by key, so
+// every ket of such a chunk is under the bound too.
 template <int LP, int LQ>
 __global__ void __launch_bounds__(128) j_pq_small_kernel(const JRec *__restrict__ recs, int bra0, int nbra,
                                                          int ket0, int nket, const double4 *__restrict__ kst, const int *__restrict__ kdq,
                                                          const double *__restrict__ skey,
                                                          const double *__restrict__ Dq, double *__restrict__ Jp,
-                                                         double tau, const double *__restrict__ boys_tab) {
+                                                         double tau, double thr32, const double *__restrict__ boys_tab) {
     constexpr int L = LP + LQ, NP = nh(LP), NQ = nh(LQ), NR = nh(L);
     constexpr double kTwoOverSqrtPi = 1.1283791670955126;
     const int lane = threadIdx.x & 31;
@@ -263,6 +266,7 @@ __global__ void __launch_bounds__(128) j_pq_small_kernel(const JRec *__restrict_
         for (int k0 = 0; k0 < nket; k0 += 32) {
             const int k = k0 + lane;
             const bool on = k < nket && !(B.G * skey[ket0 + k] < tau);
+            const bool f32 = thr32 > 0.0 && B.G * skey[ket0 + k0] < thr32;  // uniform over the warp
             if (on) {
                 const double4 KP = kst[ket0 + k];  // (P, eta) of the k-th ket in key order
                 const int kdo = kdq[ket0 + k];
@@ -273,19 +277,39 @@ __global__ void __launch_bounds__(128) j_pq_small_kernel(const JRec *__restrict_
                 double F[L + 1];
                 boys_t<L>(T, F, boys_tab);
                 const double pref = kTwoOverSqrtPi * sqrt(rho), m2r = -2.0 * rho;
-                double f[L + 1];
-                double pw = pref;
+                if (f32) {
+                    float f[L + 1];
+                    double pw = pref;
 #pragma unroll
-                for (int m = 0; m <= L; ++m) {
-                    f[m] = pw * F[m];
-                    pw *= m2r;
+                    for (int m = 0; m <= L; ++m) {
+                        f[m] = (float)(pw * F[m]);
+                        pw *= m2r;
+                    }
+                    float R[NR];
+                    R[0] = f[L];
+                    RLevels<L, L - 1, float>::run(R, f, (float)X, (float)Y, (float)Z);
+                    float d[NQ], j32[NP];
+                    signed_dq<float>(d, Dq + kdo, std::make_integer_sequence<int, NQ>{});
+#pragma unroll
+                    for (int pi = 0; pi < NP; ++pi) j32[pi] = 0.f;
+                    contract<NQ, float>(j32, R, d, std::make_integer_sequence<int, NP * NQ>{});
+#pragma unroll
+                    for (int pi = 0; pi < NP; ++pi) jp[pi] += (double)j32[pi];
+                } else {
+                    double f[L + 1];
+                    double pw = pref;
+#pragma unroll
+                    for (int m = 0; m <= L; ++m) {
+                        f[m] = pw * F[m];
+                        pw *= m2r;
+                    }
+                    double R[NR];
+                    R[0] = f[L];
+                    RLevels<L, L - 1, double>::run(R, f, X, Y, Z);
+                    double d[NQ];
+                    signed_dq<double>(d, Dq + kdo, std::make_integer_sequence<int, NQ>{});
+                    contract<NQ, double>(jp, R, d, std::make_integer_sequence<int, NP * NQ>{});
                 }
-                double R[NR];
-                R[0] = f[L];
-                RLevels<L, L - 1>::run(R, f, X, Y, Z);
-                double d[NQ];
-                signed_dq(d, Dq + kdo, std::make_integer_sequence<int, NQ>{});
-                contract<NQ>(jp, R, d, std::make_integer_sequence<int, NP * NQ>{});
             }
             const unsigned bal = __ballot_sync(0xffffffffu, on);
             if (__popc(bal) < min(32, nket - k0)) break;  // the first ket under tau is in this chunk
@@ -300,12 +324,69 @@ __global__ void __launch_bounds__(128) j_pq_small_kernel(const JRec *__restrict_
     }
 }
 
+// One bra-ket record pair of the table-indexed walk in T (float: the FP32
+// E/R tier): R from the FP64 Boys values, then jp[p] += R_{p+q} (-1)^|q| D_q
+// summed in T over the ket and added to the FP64 partials.
+template <int L, typename T>
+__device__ __forceinline__ void pq_lane_general(const JRec &B, double4 KP, const double *dq, int lp, int lq,
+                                                const double *boys_tab, double *jp) {
+    constexpr int NR = nh(L);
+    constexpr double kTwoOverSqrtPi = 1.1283791670955126;
+    const int NP = nh(lp), NQ = nh(lq);
+    const double p = B.zeta, q = KP.w;
+    const double rho = p * q / (p + q);
+    const double Xd = B.P[0] - KP.x, Yd = B.P[1] - KP.y, Zd = B.P[2] - KP.z;
+    const double Tt = rho * (Xd * Xd + Yd * Yd + Zd * Zd);
+    double F[L + 1];
+    boys_t<L>(Tt, F, boys_tab);
+    const double pref = kTwoOverSqrtPi * sqrt(rho), m2r = -2.0 * rho;
+    T f[L + 1];
+    double pw = pref;
+#pragma unroll
+    for (int m = 0; m <= L; ++m) {
+        f[m] = (T)(pw * F[m]);
+        pw *= m2r;
+    }
+    const T X = (T)Xd, Y = (T)Yd, Z = (T)Zd;
+    T R[NR];
+    R[0] = f[L];
+    for (int m = L - 1; m >= 0; --m) {
+        for (int s = L - m; s >= 1; --s) {
+            for (int i = nh(s - 1); i < nh(s); ++i) {
+                const int t = kHermR[i][0], u = kHermR[i][1], v = kHermR[i][2];
+                T x;
+                if (t > 0) {
+                    x = X * R[h_index(t - 1, u, v)];
+                    if (t >= 2) x += (T)(t - 1) * R[h_index(t - 2, u, v)];
+                } else if (u > 0) {
+                    x = Y * R[h_index(0, u - 1, v)];
+                    if (u >= 2) x += (T)(u - 1) * R[h_index(0, u - 2, v)];
+                } else {
+                    x = Z * R[h_index(0, 0, v - 1)];
+                    if (v >= 2) x += (T)(v - 1) * R[h_index(0, 0, v - 2)];
+                }
+                R[i] = x;
+            }
+        }
+        R[0] = f[m];
+    }
+    for (int pi = 0; pi < NP; ++pi) {
+        T acc = (T)0;
+        for (int qi = 0; qi < NQ; ++qi) {
+            const int tq = kHermR[qi][0], uq = kHermR[qi][1], vq = kHermR[qi][2];
+            const T d = (T)((((tq + uq + vq) & 1) ? -1.0 : 1.0) * __ldg(dq + qi));
+            acc += R[h_index(kHermR[pi][0] + tq, kHermR[pi][1] + uq, kHermR[pi][2] + vq)] * d;
+        }
+        jp[pi] += (double)acc;
+    }
+}
+
 // One (bra L, ket L) class at total order L = lp + lq (runtime lp, lq).
 template <int L>
 __global__ void __launch_bounds__(128) j_pq_kernel(const JRec *__restrict__ recs, int lp, int lq, int bra0, int nbra,
                                                    int ket0, int nket, const double4 *__restrict__ kst, const int *__restrict__ kdq,
                                                    const double *__restrict__ skey, const double *__restrict__ Dq,
-                                                   double *__restrict__ Jp, double tau,
+                                                   double *__restrict__ Jp, double tau, double thr32,
                                                    const double *__restrict__ boys_tab) {
     constexpr int NR = nh(L), NPMAX = nh(L < kJMaxL ? L : kJMaxL);
     constexpr double kTwoOverSqrtPi = 1.1283791670955126;
@@ -319,7 +400,10 @@ __global__ void __launch_bounds__(128) j_pq_kernel(const JRec *__restrict__ recs
         for (int k0 = 0; k0 < nket; k0 += 32) {
             const int k = k0 + lane;
             const bool on = k < nket && !(B.G * skey[ket0 + k] < tau);
-            if (on) {
+            const bool f32 = thr32 > 0.0 && B.G * skey[ket0 + k0] < thr32;  // uniform over the warp
+            if (on && f32) {
+                pq_lane_general<L, float>(B, kst[ket0 + k], Dq + kdq[ket0 + k], lp, lq, boys_tab, jp);
+            } else if (on) {
                 const double4 KP = kst[ket0 + k];  // (P, eta) of the k-th ket in key order
                 const int kdo = kdq[ket0 + k];
                 const double p = B.zeta, q = KP.w;
@@ -438,13 +522,14 @@ __global__ void j_jab_kernel(const JRec *__restrict__ recs, const int *__restric
 }
 
 using PqLaunch = void (*)(int grid, cudaStream_t st, const JRec *, int, int, int, int, int, int, const double4 *,
-                          const int *, const double *, const double *, double *, double, const double *);
+                          const int *, const double *, const double *, double *, double, double, const double *);
 
 template <int L>
 void pq_launch(int grid, cudaStream_t st, const JRec *recs, int lp, int lq, int bra0, int nbra, int ket0, int nket,
                const double4 *kst, const int *kdq, const double *skey, const double *Dq, double *Jp, double tau,
-               const double *boys) {
-    j_pq_kernel<L><<<grid, 128, 0, st>>>(recs, lp, lq, bra0, nbra, ket0, nket, kst, kdq, skey, Dq, Jp, tau, boys);
+               double thr32, const double *boys) {
+    j_pq_kernel<L><<<grid, 128, 0, st>>>(recs, lp, lq, bra0, nbra, ket0, nket, kst, kdq, skey, Dq, Jp, tau, thr32,
+                                         boys);
 }
 
 template <int... L>
@@ -454,15 +539,16 @@ constexpr std::array<PqLaunch, sizeof...(L)> pq_table(std::integer_sequence<int,
 const auto kPqTable = pq_table(std::make_integer_sequence<int, 2 * kJMaxL + 1>{});
 
 using PqSmallLaunch = void (*)(int grid, cudaStream_t st, const JRec *, int, int, int, int, const double4 *,
-                               const int *, const double *, const double *, double *, double, const double *);
+                               const int *, const double *, const double *, double *, double, double,
+                               const double *);
 
 template <int LP, int LQ>
 void pq_small_launch(int grid, cudaStream_t st, const JRec *recs, int bra0, int nbra, int ket0, int nket,
                      const double4 *kst, const int *kdq, const double *skey, const double *Dq, double *Jp, double tau,
-                     const double *boys) {
+                     double thr32, const double *boys) {
     if constexpr (LP + LQ <= kSmallL)
         j_pq_small_kernel<LP, LQ><<<grid, 128, 0, st>>>(recs, bra0, nbra, ket0, nket, kst, kdq, skey, Dq, Jp,
-                                                        tau, boys);
+                                                        tau, thr32, boys);
 }
 
 template <int LP, int... LQ>
@@ -621,7 +707,7 @@ JEngine *jengine_create(const HostBasis &basis, int device, std::string *err) {
 
 void jengine_destroy(JEngine *e) { delete e; }
 
-int jengine_build(JEngine *e, const double *D_dev, double *J_dev, double tau, const double *boys_tab,
+int jengine_build(JEngine *e, const double *D_dev, double *J_dev, double tau, double thr32, const double *boys_tab,
                   cudaStream_t st, std::string *err, int *launches) {
     int nl = 0;
     auto check = [&](cudaError_t c, const char *what) {
@@ -657,10 +743,10 @@ int jengine_build(JEngine *e, const double *D_dev, double *J_dev, double tau, co
             if (nk == 0) continue;
             if (lp + lq <= kSmallL)
                 kPqSmall[lp][lq](grid, st, e->recs.p, b0, nb, k0, nk, e->kst.p, e->kdq.p, e->skey.p, e->Dqs.p, e->Jp.p, tau,
-                                 boys_tab);
+                                 thr32, boys_tab);
             else
                 kPqTable[lp + lq](grid, st, e->recs.p, lp, lq, b0, nb, k0, nk, e->kst.p, e->kdq.p, e->skey.p, e->Dqs.p,
-                                  e->Jp.p, tau, boys_tab);
+                                  e->Jp.p, tau, thr32, boys_tab);
             ++nl;
             if (!check(cudaGetLastError(), "j_pq_kernel")) return -2;
         }

@@ -32,9 +32,10 @@ JEngine *jengine_create(const HostBasis &basis, int device, std::string *err);
 void jengine_destroy(JEngine *e);
 
 // J (n_ao^2, DEVICE, row-major; every element written) from the symmetric
-// density D_dev at threshold tau.  boys_tab: the device Boys table.
+// density D_dev at threshold tau.  thr32 > 0: the record pairs under it run
+// their R and contraction in FP32.  boys_tab: the device Boys table.
 // *launches receives the kernel launches issued.
-int jengine_build(JEngine *e, const double *D_dev, double *J_dev, double tau, const double *boys_tab,
+int jengine_build(JEngine *e, const double *D_dev, double *J_dev, double tau, double thr32, const double *boys_tab,
                   cudaStream_t st, std::string *err, int *launches);
 
 // The host plan of the same sweep, for the bit-exact comparison with the

@@ -346,11 +346,12 @@ class FockEngine:
         return {"el": el.reshape(-1, 2), "ptr": ptr, "src": src}
 
     # -- the J-engine (eri/j_coulomb/j.py) ----------------------------------
-    def coulomb(self, D, *, tau: float = 0.0, J=None):
+    def coulomb(self, D, *, tau: float = 0.0, J=None, threshold: float = 0.0):
         """J of the symmetric density D by the McMurchie-Davidson J-engine
         (the reference's coulomb_matrix / coulomb_matrix_screened sweep,
         eri/j_coulomb/j.py:436-581): a device tensor D in, a device J out
-        (written in full).  Needs no plan."""
+        (written in full).  Needs no plan.  threshold > 0: the FP32 E/R tier
+        for record pairs whose bound is under it (fjb_coulomb_mixed)."""
         import torch
         tau = _checked_tau(tau)
         if not isinstance(D, torch.Tensor):
@@ -361,7 +362,8 @@ class FockEngine:
         if J is None:
             J = torch.empty_like(D)
         st = torch.cuda.current_stream(D.device).cuda_stream
-        _lib.check(self._L.fjb_coulomb(self._h, D.data_ptr(), J.data_ptr(), tau, C.c_void_p(st)), self._h)
+        _lib.check(self._L.fjb_coulomb_mixed(self._h, D.data_ptr(), J.data_ptr(), tau, float(threshold),
+                                             C.c_void_p(st)), self._h)
         return J
 
     # -- the one-electron matrices (one_electron/) ---------------------------

@@ -289,6 +289,13 @@ int fjb_boys(int m, const double *T_dev, int n, double *F_dev);
  * stages the records (allocates), later calls allocate nothing and can be
  * captured in a CUDA graph. */
 int fjb_coulomb(fjb_handle *h, const double *D_dev, double *J_dev, double tau, void *stream);
+/* The same with the FP32 E/R tier (eri/j_coulomb/levers/mixed.py:101 _f32,
+ * as magnitude routing): a chunk of 32 sorted kets whose largest bound
+ * I_bra I_ket max|D_q| is below `threshold` runs its R_{tuv} recursion, its
+ * signed D_q and the contraction in FP32; T, the Boys values and every J_p
+ * sum stay FP64.  threshold 0 is fjb_coulomb. */
+int fjb_coulomb_mixed(fjb_handle *h, const double *D_dev, double *J_dev, double tau, double threshold,
+                      void *stream);
 /* The atomics-free build's map of plan launch `launch` (plan order): n_el
  * distinct elements (row, col) of J'/K' ascending in el[2*n_el], CSR offsets
  * ptr[n_el + 1], and src[n_slot] each element's slots ascending, the slots

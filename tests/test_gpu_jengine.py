@@ -69,3 +69,25 @@ def test_j_engine_screened_and_fused_build(cuda, lib_built):
           f"{eng.j_launches()} launches")
     assert d_scr <= 1e-10
     assert d_fused <= 1e-10
+
+
+@pytest.mark.parametrize("atoms,seed", [(3, 5), (6, 11)])
+def test_j_engine_fp32_tier(cuda, lib_built, oracle_lib, atoms, seed):
+    """The FP32 E/R tier (fjb_coulomb_mixed) at the 1e-9 routing bound:
+    within the metric's 1e-8 budget of the FP64 J-engine and of the oracle;
+    a bound above every key runs every chunk in FP32, at FP32 accuracy."""
+    import torch
+    w = configs.cluster(atoms, seed)
+    eng = FockEngine(w.basis)
+    D = torch.tensor(w.D, device=cuda)
+    J64 = eng.coulomb(D, tau=0.0).clone()
+    J32 = eng.coulomb(D, tau=0.0, threshold=1e-9).clone()
+    Jall = eng.coulomb(D, tau=0.0, threshold=1e30).clone()
+    torch.cuda.synchronize()
+    Jo, _ = oracle_lib.jk(oracle_lib.OracleBasis.of(w.basis), w.D)
+    d64 = float((J32 - J64).abs().max())
+    dor = float(np.abs(J32.cpu().numpy() - Jo).max())
+    dall = float((Jall - J64).abs().max() / J64.abs().max())
+    print(f"{atoms} atoms: mixed vs FP64 {d64:.2e}, vs oracle {dor:.2e}; all-FP32 relative {dall:.2e}")
+    assert d64 <= 1e-8 and dor <= 1e-8
+    assert 0.0 < dall <= 1e-5
