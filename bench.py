@@ -53,12 +53,17 @@ def parse():
     ap.add_argument("--workload", default="c1")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--path", default="fock", choices=["fock", "coulomb", "df", "batch", "onee"],
+    ap.add_argument("--path", default="fock", choices=["fock", "coulomb", "df", "batch", "onee", "router"],
                     help="fock: the G build (the headline); coulomb: the MMD J-engine; "
                          "df: DF-J/K (FP64 and split-BF16 tensor-core GEMMs); batch: the "
                          "uneven molecule batch (c4) as one captured graph")
     ap.add_argument("--molecules", type=int, default=64, help="batch path: the first N c4 molecules")
     ap.add_argument("--atoms", type=int, default=16, help="df path: atoms of the c1-recipe cluster")
+    ap.add_argument("--clusters", type=int, default=200, help="router path: c3 training clusters (8-64 atoms)")
+    ap.add_argument("--router-samples", type=int, default=60000,
+                    help="router path: launched quartets sampled per training cluster")
+    ap.add_argument("--router-out", default="",
+                    help="router path: where to save the trained network (.npz)")
     ap.add_argument("--df-block", type=int, default=768,
                     help="streamed df path: aux functions per block of (mn|P) (n_ao^2 x block doubles)")
     ap.add_argument("--df-stream", action="store_true",
@@ -485,6 +490,8 @@ def side_path(a, local):
             "data": "synthetic", "dtype": "f64", "config": {"workload": a.workload, "n_ao": w.n_ao}}
     if a.path == "batch":
         return batch_path(a, local)
+    if a.path == "router":
+        return router_path(a, local)
     if a.path == "coulomb":
         from felizjueves_b200.fock import FockEngine
         eng = FockEngine(w.basis, device=local)
@@ -554,6 +561,81 @@ def side_path(a, local):
                     max_abs_dJ_bf16x3_vs_fp64=float((J16 - J64).abs().max()),
                     max_abs_dK_bf16x3_vs_fp64=float((K16 - K64).abs().max()),
                     max_abs_K_fp64=float(K64.abs().max()))
+    print(json.dumps(line))
+
+
+def router_path(a, local):
+    """Config c3: the learned router trained at scale -- `--clusters` seeded
+    clusters of 8-64 atoms with the c1 shells, `--router-samples` launched
+    quartets sampled from each, those the six-block screen computes labelled
+    by the FP64 HGP tap (log10 of the largest deposit into G), about 1e7 in
+    all -- on the GPU with the library's MLP kernels, calibrated on held-out
+    quartets; then on the c1 system (not in the training set) the routed
+    build at 1e-9 with the learned router against the bound alone, both with
+    the on-device budget check, against the FP64 build.  W warm-up and K
+    timed graph replays each."""
+    import time as _t
+    import torch
+    from felizjueves_b200 import _lib, configs, router
+    from felizjueves_b200.fock import FockEngine
+    torch.cuda.set_device(local)
+    t0 = _t.perf_counter()
+    X, y = router.training_set(router.c3_clusters(a.clusters), n_per=a.router_samples, seed=1)
+    t_data = _t.perf_counter() - t0
+    perm = np.random.default_rng(2).permutation(len(X))
+    ntr = int(0.9 * len(X))
+    tr, va = perm[:ntr], perm[ntr:]
+    mlp = router.MLP(router.init_params(X[tr], y[tr], seed=0), device=local)
+    t1 = _t.perf_counter()
+    losses = mlp.train(X[tr], y[tr], epochs=12, batch=8192)
+    torch.cuda.synchronize()
+    t_train = _t.perf_counter() - t1
+    margin = router.calibrate(mlp, X[va], y[va], 0.999)
+    rmse_va = float(np.sqrt(np.mean((y[va] - mlp.predict(X[va]).cpu().numpy()) ** 2)))
+    if a.router_out:
+        np.savez(a.router_out, params=mlp.params(), margin=margin, n_train=len(tr))
+    w = configs.c1()
+    eng = FockEngine(w.basis, device=local)
+    eng.plan(w.D, w.tau, w.n_mag)
+    D = torch.tensor(w.D, device=f"cuda:{local}")
+    J, K, G = (torch.empty_like(D) for _ in range(3))
+    st = torch.cuda.current_stream()
+
+    def timed(prec, thr):
+        for _ in range(max(1, a.warmup)):
+            eng.build(D, J=J, K=K, G=G, precision=prec, threshold=thr, graph=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(a.steps):
+            eng.build(D, J=J, K=K, G=G, precision=prec, threshold=thr, graph=True)
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / a.steps
+
+    ms64 = timed(_lib.FJB_FP64, 0.0)
+    G64 = G.clone()
+    res = {}
+    for kind in ("bound", "learned"):
+        if kind == "learned":
+            router.install(eng, mlp, threshold=1e-9, margin=margin)
+        ms = timed(_lib.FJB_ROUTED, 1e-9)
+        n32, n64 = router.route_stats(eng)
+        est, rr = eng.route_check()
+        res[kind] = {"ms_per_step": round(ms, 3), "speedup_vs_fp64": round(ms64 / ms, 4),
+                     "max_abs_dG_vs_fp64": float((G - G64).abs().max()), "fp32_units": n32,
+                     "fp64_units": n64, "budget_check": {"estimate": est, "rerouted_to_fp64": rr}}
+    line = {"metric": "learned router on c1: routed G build ms/iter at 1e-9 vs the bound alone",
+            "value": res["learned"]["ms_per_step"], "unit": "ms/iter", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "higher_is_better": False, "data": "synthetic", "dtype": "f64+f32",
+            "config": {"workload": "c3: train on seeded 8-64-atom clusters, evaluate on c1",
+                       "clusters": a.clusters, "samples_per_cluster": a.router_samples},
+            "training_quartets": int(len(tr)), "validation_quartets": int(len(va)),
+            "data_s": round(t_data, 1), "train_s": round(t_train, 1), "epochs": len(losses),
+            "final_train_mse_log10": round(losses[-1], 5), "validation_rmse_log10": round(rmse_va, 4),
+            "margin_log10": round(margin, 4), "fp64_ms_per_step": round(ms64, 3),
+            "bound": res["bound"], "learned": res["learned"],
+            "learned_gain_vs_bound": round(res["bound"]["ms_per_step"] / res["learned"]["ms_per_step"], 4)}
     print(json.dumps(line))
 
 

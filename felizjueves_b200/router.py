@@ -122,6 +122,37 @@ class MLP:
         return losses
 
 
+def plan_samples(eng: FockEngine, n: int, rng) -> tuple[np.ndarray, np.ndarray]:
+    """n random launched quartets as (launch, bra index, ket index) and their
+    shells (a, b, c, d), drawn like sample_launched but from the handle's
+    exported arrays, vectorised (no per-pair objects: 64-atom plans)."""
+    c = eng.counts_raw()
+    nb, nk, nl = c["batches"], c["kept_pairs"], c["launches"]
+    arr = {"batch_key": np.zeros(4 * nb, np.int32), "batch_npairs": np.zeros(nb, np.int32),
+           "pair_ab": np.zeros(2 * nk, np.int32), "pair_mag": np.zeros(nk, np.int32),
+           "prims": np.zeros(c["kept_prims"], np.int32), "pair_G": np.zeros(nk), "pair_dmax": np.zeros(nk),
+           "pair_key": np.zeros(nk), "prim_G": np.zeros(c["kept_prims"]),
+           "launches": np.zeros(2 * nl, np.int32),
+           "screened": np.zeros(2 * c["batch_pairs_screened"], np.int32),
+           "deleted": np.zeros(2 * c["pairs_deleted"], np.int32),
+           "magnitudes": np.zeros(eng._n_mag), "eps": np.zeros(1), "g_max": np.zeros(1)}
+    lists = _lib.PlanLists_t(**{k: v.ctypes.data for k, v in arr.items()})
+    _lib.check(eng._L.fjb_plan_export(eng._h, C.byref(lists)), eng._h)
+    npairs = arr["batch_npairs"].astype(np.int64)
+    p0 = np.concatenate([[0], np.cumsum(npairs)[:-1]])
+    L = arr["launches"].reshape(-1, 2)
+    sizes = (npairs[L[:, 0]] * npairs[L[:, 1]]).astype(np.float64)
+    li = rng.choice(nl, size=n, p=sizes / sizes.sum())
+    ib = (rng.random(n) * npairs[L[li, 0]]).astype(np.int64)
+    ik = (rng.random(n) * npairs[L[li, 1]]).astype(np.int64)
+    diag = (L[li, 0] == L[li, 1]) & (ik < ib)
+    ib[diag], ik[diag] = ik[diag], ib[diag].copy()
+    ab = arr["pair_ab"].reshape(-1, 2)
+    bra, ket = ab[p0[L[li, 0]] + ib], ab[p0[L[li, 1]] + ik]
+    samples = np.stack([li, ib, ik], axis=1).astype(np.int32)
+    return samples, np.concatenate([bra, ket], axis=1).astype(np.int32)
+
+
 def sample_launched(eng: FockEngine, n: int, rng) -> np.ndarray:
     """n random launched quartets (launch, bra index, ket index), launches
     drawn by the quartets they hold; the canonical half on the diagonal."""
@@ -167,24 +198,46 @@ def training_set(workloads, n_per: int = 20000, seed: int = 0, zero_gap: float =
     Xs, ys = [], []
     for w in workloads:
         eng = FockEngine(w.basis, tuned=False)
-        P = eng.plan(w.D, w.tau, w.n_mag)
-        s = sample_launched(eng, n_per, rng)
+        eng.plan(w.D, w.tau, w.n_mag, export=False)
+        s, q = plan_samples(eng, n_per, rng)
         X, b = features(eng, w.D, s)
         keep = b >= w.tau  # computed (not screened) quartets only
-        s, X = s[keep], X[keep]
-        quartets = []
-        for l, ib, ik in s:
-            L = P.launches[l]
-            pb, pk = P.batches[L.bra].pairs[ib], P.batches[L.ket].pairs[ik]
-            quartets.append((pb.a, pb.b, pk.a, pk.b))
-        blocks = eng.eri_blocks(quartets)
-        mx = np.array([np.abs(blk).max() for blk in blocks])
+        s, X, q = s[keep], X[keep], q[keep]
+        mx = block_max(eng, q)
         y = np.log10(np.maximum(mx, 1e-300)) + X[:, 11]  # + log10 dmax
         keep = y - bound_log10(X) > zero_gap
         Xs.append(X[keep])
         ys.append(y[keep].astype(np.float32))
         eng.close()
     return np.concatenate(Xs), np.concatenate(ys)
+
+
+def block_max(eng: FockEngine, quartets: np.ndarray) -> np.ndarray:
+    """max |(ab|cd)| of each quartet's block, from the FP64 HGP tap, on the
+    device (segment maxima: one pass over the tap's output)."""
+    import torch
+    q = np.ascontiguousarray(quartets, np.int32)
+    n = len(q)
+    off = np.zeros(n + 1, np.int64)
+    nc = np.array([s.n_cart for s in eng.basis.shells], np.int64)
+    off[1:] = np.cumsum(nc[q[:, 0]] * nc[q[:, 1]] * nc[q[:, 2]] * nc[q[:, 3]])
+    out = torch.empty(max(int(off[-1]), 1), dtype=torch.float64, device=f"cuda:{eng.device}")
+    _lib.check(eng._L.fjb_eri_blocks(eng._h, q.ctypes.data, n, out.data_ptr(), off.ctypes.data), eng._h)
+    seg = torch.repeat_interleave(torch.arange(n, device=out.device),
+                                  torch.as_tensor(np.diff(off), device=out.device))
+    mx = torch.zeros(n, dtype=torch.float64, device=out.device)
+    mx.scatter_reduce_(0, seg, out[: int(off[-1])].abs(), reduce="amax", include_self=True)
+    return mx.cpu().numpy()
+
+
+def c3_clusters(n: int = 200, lo: int = 8, hi: int = 64, seed: int = 3):
+    """Config c3's training systems: n seeded clusters of the c1 shell recipe
+    at c1's number density, lo..hi atoms (uniform draw)."""
+    from . import configs
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(lo, hi + 1, size=n)
+    for i, k in enumerate(sizes):
+        yield configs.cluster(int(k), 10_000 + i)
 
 
 def calibrate(mlp: MLP, X, y, quantile: float = 0.999) -> float:
