@@ -64,6 +64,9 @@ def parse():
                     help="router path: launched quartets sampled per training cluster")
     ap.add_argument("--router-out", default="",
                     help="router path: where to save the trained network (.npz)")
+    ap.add_argument("--router-in", default="",
+                    help="router path: evaluate this trained network (.npz) instead of training one "
+                         "(its reach from a fresh c3 sample)")
     ap.add_argument("--df-block", type=int, default=768,
                     help="streamed df path: aux functions per block of (mn|P) (n_ao^2 x block doubles)")
     ap.add_argument("--df-stream", action="store_true",
@@ -435,26 +438,16 @@ def ctypes_probe(_lib, fp32: int) -> float:
     return float(v.value)
 
 
-def train_router():
-    """The learned precision router: trained on the GPU with the library's
-    kernels on quartets the FP64 method computes for six seeded 4-10 atom
-    clusters (not a benchmarked system), calibrated on held-out quartets
-    (0.999 residual quantile).  Returns (network, margin, training size)."""
-    from felizjueves_b200 import configs, router
-    X, y = router.training_set([configs.cluster(n, 100 + n) for n in (4, 5, 6, 7, 8, 10)], n_per=12000, seed=1)
-    perm = np.random.default_rng(2).permutation(len(X))
-    tr, va = perm[: int(0.8 * len(X))], perm[int(0.8 * len(X)):]
-    mlp = router.MLP(router.init_params(X[tr], y[tr], seed=0))
-    mlp.train(X[tr], y[tr])
-    return mlp, router.calibrate(mlp, X[va], y[va], 0.999), int(len(tr))
-
-
 def install_learned_router(eng) -> dict:
-    """train_router(), installed on `eng` at the 1e-9 threshold."""
+    """The network trained for config c3 (router.load_default: 7.87 M FP64
+    quartets of 200 seeded 8-64-atom clusters; bench.py --path router
+    retrains it), installed on `eng` at the 1e-9 threshold with its
+    calibrated margin, reach and class gate."""
     from felizjueves_b200 import router
-    mlp, margin, n_tr = train_router()
-    router.install(eng, mlp, threshold=1e-9, margin=margin)
-    return {"kind": "learned", "training_quartets": n_tr, "margin_log10": round(margin, 3)}
+    mlp, margin, reach, min_l = router.load_default(device=eng.device)
+    router.install(eng, mlp, threshold=1e-9, margin=margin, reach=reach, min_total_l=min_l)
+    return {"kind": "learned", "training_quartets": 7867810, "margin_log10": round(margin, 3),
+            "reach_decades": reach, "min_total_l": min_l}
 
 
 def route_counts(eng):
@@ -580,20 +573,30 @@ def router_path(a, local):
     from felizjueves_b200.fock import FockEngine
     torch.cuda.set_device(local)
     t0 = _t.perf_counter()
-    X, y = router.training_set(router.c3_clusters(a.clusters), n_per=a.router_samples, seed=1)
-    t_data = _t.perf_counter() - t0
-    perm = np.random.default_rng(2).permutation(len(X))
-    ntr = int(0.9 * len(X))
-    tr, va = perm[:ntr], perm[ntr:]
-    mlp = router.MLP(router.init_params(X[tr], y[tr], seed=0), device=local)
-    t1 = _t.perf_counter()
-    losses = mlp.train(X[tr], y[tr], epochs=12, batch=8192)
-    torch.cuda.synchronize()
-    t_train = _t.perf_counter() - t1
-    margin = router.calibrate(mlp, X[va], y[va], 0.999)
+    if a.router_in:  # a trained network: a fresh sample of c3 systems for its reach and check
+        z = np.load(a.router_in)
+        X, y = router.training_set(router.c3_clusters(a.clusters, seed=7, first=20_000), n_per=a.router_samples,
+                                   seed=5)
+        va = np.arange(len(X))
+        tr = np.arange(int(z["n_train"]))
+        mlp = router.MLP(z["params"], device=local)
+        margin, losses, t_train = float(z["margin"]), [float("nan")], 0.0
+    else:
+        X, y = router.training_set(router.c3_clusters(a.clusters), n_per=a.router_samples, seed=1)
+        perm = np.random.default_rng(2).permutation(len(X))
+        ntr = int(0.9 * len(X))
+        tr, va = perm[:ntr], perm[ntr:]
+        mlp = router.MLP(router.init_params(X[tr], y[tr], seed=0), device=local)
+        t1 = _t.perf_counter()
+        losses = mlp.train(X[tr], y[tr], epochs=12, batch=8192)
+        torch.cuda.synchronize()
+        t_train = _t.perf_counter() - t1
+        margin = router.calibrate(mlp, X[va], y[va], 0.999)
+    t_data = _t.perf_counter() - t0 - t_train
     rmse_va = float(np.sqrt(np.mean((y[va] - mlp.predict(X[va]).cpu().numpy()) ** 2)))
+    reach = router.reach(mlp, X[va], margin)
     if a.router_out:
-        np.savez(a.router_out, params=mlp.params(), margin=margin, n_train=len(tr))
+        np.savez(a.router_out, params=mlp.params(), margin=margin, reach=reach, n_train=len(tr))
     w = configs.c1()
     eng = FockEngine(w.basis, device=local)
     eng.plan(w.D, w.tau, w.n_mag)
@@ -616,9 +619,11 @@ def router_path(a, local):
     ms64 = timed(_lib.FJB_FP64, 0.0)
     G64 = G.clone()
     res = {}
-    for kind in ("bound", "learned"):
+    for kind in ("bound", "learned", "learned_gated"):
         if kind == "learned":
-            router.install(eng, mlp, threshold=1e-9, margin=margin)
+            router.install(eng, mlp, threshold=1e-9, margin=margin, reach=reach)
+        if kind == "learned_gated":  # the reach and class gate measured best on c1
+            router.install(eng, mlp, threshold=1e-9, margin=margin, reach=0.5, min_total_l=7)
         ms = timed(_lib.FJB_ROUTED, 1e-9)
         n32, n64 = router.route_stats(eng)
         est, rr = eng.route_check()
@@ -633,9 +638,11 @@ def router_path(a, local):
             "training_quartets": int(len(tr)), "validation_quartets": int(len(va)),
             "data_s": round(t_data, 1), "train_s": round(t_train, 1), "epochs": len(losses),
             "final_train_mse_log10": round(losses[-1], 5), "validation_rmse_log10": round(rmse_va, 4),
-            "margin_log10": round(margin, 4), "fp64_ms_per_step": round(ms64, 3),
-            "bound": res["bound"], "learned": res["learned"],
-            "learned_gain_vs_bound": round(res["bound"]["ms_per_step"] / res["learned"]["ms_per_step"], 4)}
+            "margin_log10": round(margin, 4), "reach_decades": reach, "fp64_ms_per_step": round(ms64, 3),
+            "bound": res["bound"], "learned": res["learned"], "learned_gated": res["learned_gated"],
+            "learned_gain_vs_bound": round(res["bound"]["ms_per_step"] / res["learned"]["ms_per_step"], 4),
+            "learned_gated_gain_vs_bound": round(res["bound"]["ms_per_step"] /
+                                                 res["learned_gated"]["ms_per_step"], 4)}
     print(json.dumps(line))
 
 
@@ -743,11 +750,10 @@ def batch_path(a, local):
     bb.capture_merged("m32", _lib.FJB_ROUTED, 1e-9)
     m32_ms = timed(lambda: bb.replay("m32"))
     dG = max(float((g - h).abs().max()) for g, h in zip(bb.G(), G64))
-    # the learned router (trained here on seeded 4-10 atom clusters,
-    # calibrated, installed on the batch's first molecule: it routes them all)
-    from felizjueves_b200 import router
-    mlp, margin, n_tr = train_router()
-    router.install(bb.engines[0], mlp, threshold=1e-9, margin=margin)
+    # the learned router (config c3's trained network, installed on the
+    # batch's first molecule: it routes them all)
+    info = install_learned_router(bb.engines[0])
+    n_tr = info["training_quartets"]
     bb.capture_merged("mlp", _lib.FJB_ROUTED, 1e-9)
     mlp_ms = timed(lambda: bb.replay("mlp"))
     dG_mlp = max(float((g - h).abs().max()) for g, h in zip(bb.G(), G64))

@@ -285,20 +285,21 @@ __global__ void route_units_kernel(const Unit *units, int unit0, int n_units, co
 }
 
 // The largest gap (decades) below the Schwarz x density bound the router's
-// network may use: the range of gaps it is trained on (4.2 observed).
+// network is asked about by default: the range of gaps it is trained on (4.2
+// observed).  fjb_router_reach narrows it to what a trained network predicts.
 constexpr double kRouterMaxGap = 5.0;
-constexpr double kRouterReach = 1e5;  // 10^kRouterMaxGap
 
 // The learned router's unit split: as route_units_kernel, but a quartet the
 // rigorous bound calls high may still go to FP32 when the network predicts
-// its deposit under 10^log_thr -- provided its bound is within
-// kRouterMaxGap decades of the threshold; a unit with a quartet beyond that
-// stays FP64 without running the network.  Screening is untouched (the
+// its deposit under 10^log_thr -- provided its bound is within the reach
+// (reach_factor = 10^decades) of the threshold; a unit with a quartet beyond
+// that stays FP64 without running the network.  Screening is untouched (the
 // bound decides what is skipped).
 
 __global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units, const LaunchRec *launches,
                                        const PairRec *pairs, const PrimRec *prims, const double *Dsh, int n_sh,
-                                       double tau, double thresh, const float *params, float log_thr, int la,
+                                       double tau, double thresh, const float *params, float log_thr,
+                                       double reach_factor, int la,
                                        int lb, int lc, int ld, int *list32, int *list64, int *counts,
                                        int stride, int *list_s, const MolCtx *mols = nullptr,
                                        const int32_t *launch_mol = nullptr) {
@@ -326,7 +327,7 @@ __global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units
             need = active && !(b < thresh);
             // the network learned gaps below the bound of up to kRouterMaxGap
             // decades: a quartet further above the threshold cannot go FP32
-            reach = !need || b < thresh * kRouterReach;
+            reach = !need || b < thresh * reach_factor;
         }
         const bool any = __any_sync(0xffffffffu, active);
         bool low = true;
@@ -1007,6 +1008,8 @@ struct fjb_handle {
     // the learned router (fjb_router_set) and the per-launch class table it reads
     DevBuf<float> router_p;
     float router_log_thr = 0.f;
+    double router_reach = 1e5;  // 10^decades (fjb_router_reach)
+    int router_min_l = 0;       // classes below this total l route by the bound alone (fjb_router_classes)
     bool router_on = false;
     bool last_routed = false;
     DevBuf<int32_t> launch_cls;
@@ -1765,10 +1768,11 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
             int *cnt = h->route_counts.p + 4 * ri;
             const int stride = check ? h->check_stride : 0;
             const int rgrid = std::max(1, std::min((r.n_units + 3) / 4, 16 * sm_count()));
-            if (h->router_on)
+            if (h->router_on && r.dev.la + r.dev.lb + r.dev.lc + r.dev.ld >= h->router_min_l)
                 route_units_mlp_kernel<<<rgrid, 128, 0, st>>>(
                     h->units.p, r.unit0, r.n_units, h->launches.p, h->pairs.p, h->prims.p, h->Dsh.p, nsh,
-                    h->plan.tau, route, h->router_p.p, h->router_log_thr, r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld,
+                    h->plan.tau, route, h->router_p.p, h->router_log_thr, h->router_reach, r.dev.la, r.dev.lb,
+                    r.dev.lc, r.dev.ld,
                     l32, l64, cnt, stride, ls);
             else
                 route_units_kernel<<<rgrid, 128, 0, st>>>(h->units.p, r.unit0, r.n_units, h->launches.p,
@@ -2076,6 +2080,24 @@ int fjb_route_stats(const fjb_handle *hc, int64_t *n32, int64_t *n64) {
             *n64 += h->runs[ri].n_units;
         }
     }
+    return FJB_OK;
+}
+
+int fjb_router_reach(fjb_handle *h, double decades) {
+    if (!h) return fail(h, FJB_E_ARG, "null handle");
+    if (!(decades >= 0.0 && decades <= kRouterMaxGap))
+        return fail(h, FJB_E_ARG, "fjb_router_reach: decades must be in [0, 5]");
+    h->router_reach = std::pow(10.0, decades);
+    h->drop_graph();
+    return FJB_OK;
+}
+
+int fjb_router_classes(fjb_handle *h, int min_total_l) {
+    if (!h) return fail(h, FJB_E_ARG, "null handle");
+    if (min_total_l < 0 || min_total_l > 4 * FJB_MAX_L + 1)
+        return fail(h, FJB_E_ARG, "fjb_router_classes: min_total_l out of range");
+    h->router_min_l = min_total_l;
+    h->drop_graph();
     return FJB_OK;
 }
 
@@ -3288,10 +3310,12 @@ int fjb_batch_build(fjb_batch *b, int precision, double threshold, void *stream)
             int *l64 = b->route_list.p + b->n_units + r.unit0;
             int *cnt = b->route_counts.p + 4 * ri;
             const int rgrid = std::max(1, std::min((r.n_units + 3) / 4, 16 * sm_count()));
-            if (h0->router_on)  // the first molecule's learned router routes the whole batch
+            // the first molecule's learned router routes the whole batch
+            if (h0->router_on && r.dev.la + r.dev.lb + r.dev.lc + r.dev.ld >= h0->router_min_l)
                 route_units_mlp_kernel<<<rgrid, 128, 0, st>>>(
                     b->units.p, r.unit0, r.n_units, b->launches.p, b->pairs.p, b->prims.p, nullptr, 0, b->tau,
-                    route, h0->router_p.p, h0->router_log_thr, r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld, l32, l64,
+                    route, h0->router_p.p, h0->router_log_thr, h0->router_reach, r.dev.la, r.dev.lb, r.dev.lc,
+                    r.dev.ld, l32, l64,
                     cnt, 0, nullptr, b->ctx.p, b->launch_mol.p);
             else
                 route_units_kernel<<<rgrid, 128, 0, st>>>(b->units.p, r.unit0, r.n_units, b->launches.p,

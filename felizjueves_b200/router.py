@@ -230,14 +230,15 @@ def block_max(eng: FockEngine, quartets: np.ndarray) -> np.ndarray:
     return mx.cpu().numpy()
 
 
-def c3_clusters(n: int = 200, lo: int = 8, hi: int = 64, seed: int = 3):
+def c3_clusters(n: int = 200, lo: int = 8, hi: int = 64, seed: int = 3, first: int = 10_000):
     """Config c3's training systems: n seeded clusters of the c1 shell recipe
-    at c1's number density, lo..hi atoms (uniform draw)."""
+    at c1's number density, lo..hi atoms (uniform draw by `seed`), the i-th
+    from geometry seed first + i."""
     from . import configs
     rng = np.random.default_rng(seed)
     sizes = rng.integers(lo, hi + 1, size=n)
     for i, k in enumerate(sizes):
-        yield configs.cluster(int(k), 10_000 + i)
+        yield configs.cluster(int(k), first + i)
 
 
 def calibrate(mlp: MLP, X, y, quantile: float = 0.999) -> float:
@@ -246,10 +247,37 @@ def calibrate(mlp: MLP, X, y, quantile: float = 0.999) -> float:
     return float(np.quantile(r, quantile))
 
 
-def install(eng: FockEngine, mlp: MLP, *, threshold: float = 1e-9, margin: float = 0.0) -> None:
+def reach(mlp: MLP, X, margin: float, quantile: float = 0.9999) -> float:
+    """The router's reach (decades): the `quantile` of the gaps below the
+    Schwarz x density bound the network predicts on X, plus the margin,
+    rounded up to a quarter decade and capped at 5.  A quartet whose bound
+    is further above the threshold than that would need a larger gap than
+    the network gives: the routing pass does not ask it."""
+    gap = bound_log10(X) - mlp.predict(X).cpu().numpy()
+    r = float(np.quantile(gap, quantile)) + margin
+    return float(min(5.0, max(0.0, math.ceil(4.0 * r) / 4.0)))
+
+
+def install(eng: FockEngine, mlp: MLP, *, threshold: float = 1e-9, margin: float = 0.0,
+            reach: float | None = None, min_total_l: int = 0) -> None:
+    """Install the network on `eng`: units of classes with total angular
+    momentum >= min_total_l whose quartets are within `reach` decades of
+    the threshold ask it (fjb_router_reach, fjb_router_classes)."""
     p = np.ascontiguousarray(mlp.params(), np.float32)
     _lib.check(eng._L.fjb_router_set(eng._h, p.ctypes.data,
                                      C.c_float(math.log10(threshold) - margin)), eng._h)
+    _lib.check(eng._L.fjb_router_reach(eng._h, 5.0 if reach is None else float(reach)), eng._h)
+    _lib.check(eng._L.fjb_router_classes(eng._h, int(min_total_l)), eng._h)
+
+
+def load_default(device: int = 0) -> tuple[MLP, float, float, int]:
+    """The network trained for config c3 (data/router_c3.npz: 7.87 M FP64
+    quartets of 200 seeded 8-64-atom clusters, bench.py --path router) with
+    its calibrated margin and the reach and class gate measured best on c1
+    (0.5 decades, total l >= 7): (network, margin, reach, min_total_l)."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "data", "router_c3.npz"))
+    return MLP(z["params"], device=device), float(z["margin"]), float(z["reach"]), int(z["min_total_l"])
 
 
 def uninstall(eng: FockEngine) -> None:

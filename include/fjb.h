@@ -259,6 +259,19 @@ int fjb_df_blocks(fjb_handle *h, int kind, const int32_t *items, int n, double *
  * params_host NULL turns the learned router off. */
 int fjb_mlp_n_params(void);
 int fjb_router_set(fjb_handle *h, const float *params_host, float log10_threshold);
+/* How far above the threshold (decades, 0..5; default 5) a quartet's bound
+ * may be for the network to be asked: a unit with a quartet further above
+ * stays FP64 without running it.  Set it to the largest gap below the bound
+ * the trained network predicts (plus its margin) so the routing pass runs
+ * the network only where it can move a unit to FP32; a smaller reach only
+ * keeps more units FP64. */
+int fjb_router_reach(fjb_handle *h, double decades);
+/* Which classes ask the network: those with la + lb + lc + ld >=
+ * min_total_l (default 0, every class).  The network costs a few thousand
+ * flops a quartet, more than a small class's whole quartet, so below some
+ * total angular momentum asking it costs more than the FP32 units it adds
+ * save; those classes route by the bound alone. */
+int fjb_router_classes(fjb_handle *h, int min_total_l);
 /* Features (n x 12 floats) and six-block bounds (n doubles) of sampled
  * launched quartets, samples[3i..3i+2] = (launch, bra index, ket index) in
  * the plan's order (HOST); feat_dev, bound_dev DEVICE.  Synchronises. */
