@@ -16,7 +16,7 @@ bool layout_one(int max_kab, int max_kcd, int rsize, int budget, RysDev *o) {
     using S = rys::Shape<LA, LB, LC, LD>;
     const int minb = rsize == 8 ? S::template minb<double>() : S::template minb<float>();
     budget = std::min(budget, rys::rys_smem_budget(minb));
-    const int nt = S::nt();
+    const int nt = rsize == 8 ? S::template nt<double>() : S::template nt<float>();
     *o = RysDev{};
     o->threads = nt;
     o->kab = max_kab;

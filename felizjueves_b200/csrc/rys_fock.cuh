@@ -180,19 +180,35 @@ struct Shape {
     static constexpr int XS = NBF | 1;  // X row stride, odd: rows start in different banks
     static constexpr int YS = NCD | 1;
     static constexpr int N5 = NCD + NA * NC + NA * ND + NB * NC + NB * ND;
-    // CTA width: 128 threads (a thread per (ket, f) item, G = 128 / NBF kets
-    // a group), 256 for the ff kets (NBF = 74) so that a group holds more
-    // than one ket
-    __host__ __device__ static constexpr int nt() { return NBF > 64 ? 256 : 128; }
-    // CTAs an SM holds: 512 threads of 128 registers, unless the bra column
-    // the boundary phase keeps in registers is too long to fit in those
-    // (df and ff bras in FP64, the ff bra in FP32): then half as many; a bra
-    // column of at most 80 bytes (10 FP64 or 20 FP32 boundary values) fits
-    // six CTAs of 80 registers, with no more than a few dozen bytes of spill
+    // CTAs an SM at CTA width t: 512 threads an SM, halved when the bra
+    // column the boundary phase keeps in registers is too long for the
+    // registers that leaves (df and ff bras in FP64, the ff bra in FP32); a
+    // bra column of at most 80 bytes (10 FP64 or 20 FP32 boundary values)
+    // fits six CTAs of 128 threads at 80 registers, with no more than a few
+    // dozen bytes of spill
+    template <typename R>
+    __host__ __device__ static constexpr int minb_at(int t) {
+        if (t == 128 && NBE * (int)sizeof(R) <= 80) return 6;
+        const int m = (512 / t) / (NBE > (sizeof(R) == 8 ? 34 : 52) ? 2 : 1);
+        return m > 0 ? m : 1;
+    }
+    // CTA width: a thread per (ket, f) item, G = NT / NBF kets a group (at
+    // most kKetChunk).  128, but 160 for the 52-value kets (3 x 52 of 160
+    // threads busy, not 2 x 52 of 128) where that keeps more of them busy
+    // on an SM (not when the bra is short enough for six CTAs of 128, or so
+    // long that one of 160 fits), and 224 for the 74-value ff kets (3 x 74;
+    // 256 left 34 idle).  Measured on the 64-atom cluster: 256-wide CTAs on
+    // the 19- to 34-value kets, two an SM, ran 7-21 ms a class slower than
+    // four of 128.
+    template <typename R>
+    __host__ __device__ static constexpr int nt() {
+        if (NBF > 64) return 224;
+        const bool wide = NBF > 40 && minb_at<R>(160) * (160 / NBF) > minb_at<R>(128) * (128 / NBF);
+        return wide ? 160 : 128;
+    }
     template <typename R>
     __host__ __device__ static constexpr int minb() {
-        return nt() == 128 && NBE * (int)sizeof(R) <= 80 ? 6
-                                                          : (nt() == 256 ? 2 : 4) / (NBE > (sizeof(R) == 8 ? 34 : 52) ? 2 : 1);
+        return minb_at<R>(nt<R>());
     }
 };
 
@@ -654,7 +670,7 @@ __global__ void __launch_bounds__(NT, (rys::Shape<LA, LB, LC, LD>::template minb
 // (instantiated per precision in rys_fock64.cu and rys_fock32.cu).
 template <int LA, int LB, int LC, int LD, typename R>
 struct RysOne {
-    static constexpr int kRysThreads = rys::Shape<LA, LB, LC, LD>::nt();
+    static constexpr int kRysThreads = rys::Shape<LA, LB, LC, LD>::template nt<R>();
     static void attr() {
         static bool done = false;  // per kernel and process: the largest carve-up any layout takes
         if (done) return;

@@ -69,3 +69,27 @@ def test_trained_router_gains_within_budget(cuda, lib_built):
     assert d_mlp <= 1e-8
     v = router.validate(eng, D)
     assert v["within_budget"]
+
+
+def test_shipped_network_within_budget(cuda, lib_built):
+    """The network trained for config c3 (router.load_default), installed
+    with its margin, reach and class gate on a 6-atom cluster: the routed
+    build within the 1e-8 budget of the FP64 build, and at least the bound's
+    FP32 units."""
+    import torch
+    from felizjueves_b200 import _lib, router
+    from felizjueves_b200.fock import FockEngine
+    w = configs.cluster(6, 11)
+    eng = FockEngine(w.basis)
+    eng.plan(w.D, w.tau, w.n_mag)
+    D = torch.tensor(w.D, device=cuda)
+    G64 = eng.build(D)[2].clone()
+    eng.build(D, precision=_lib.FJB_ROUTED, threshold=1e-9)
+    n32_bound, _ = router.route_stats(eng)
+    mlp, margin, reach, min_l = router.load_default()
+    router.install(eng, mlp, threshold=1e-9, margin=margin, reach=reach, min_total_l=min_l)
+    G = eng.build(D, precision=_lib.FJB_ROUTED, threshold=1e-9)[2]
+    n32, _ = router.route_stats(eng)
+    d = float((G - G64).abs().max())
+    print(f"shipped network: {n32} FP32 units vs {n32_bound} by the bound, max|dG| {d:.2e}")
+    assert d <= 1e-8 and n32 >= n32_bound
