@@ -73,9 +73,14 @@ __global__ void density_blocks_kernel(const double *__restrict__ D, int n_ao, in
     Dsh[st] = m;
 }
 
+// With the budget check, the sampled FP32 units are in neither queue: their
+// contribution is the sample's own FP32 build (Js32, Ks32), or its FP64 one
+// (Js64, Ks64) when *flag says the FP32 queue was re-run in FP64.
 __global__ void close_kernel(const double *__restrict__ Jp, const double *__restrict__ Kp, int n,
                              double *J, double *K, double *G, const double *__restrict__ Jp2 = nullptr,
-                             const double *__restrict__ Kp2 = nullptr) {
+                             const double *__restrict__ Kp2 = nullptr, const double *__restrict__ Js32 = nullptr,
+                             const double *__restrict__ Ks32 = nullptr, const double *__restrict__ Js64 = nullptr,
+                             const double *__restrict__ Ks64 = nullptr, const int *flag = nullptr) {
     size_t ij = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (ij >= (size_t)n * n) return;
     size_t i = ij / n, j = ij % n, ji = j * n + i;
@@ -85,14 +90,22 @@ __global__ void close_kernel(const double *__restrict__ Jp, const double *__rest
         jv += Jp2[ij] + Jp2[ji];
         kv += Kp2[ij] + Kp2[ji];
     }
+    if (Js32) {  // the check's sample, in the precision the verdict kept
+        const bool over = *flag != 0;
+        const double *Js = over ? Js64 : Js32, *Ks = over ? Ks64 : Ks32;
+        jv += Js[ij] + Js[ji];
+        kv += Ks[ij] + Ks[ji];
+    }
     if (J) J[ij] = jv;
     if (K) K[ij] = kv;
     if (G) G[ij] = jv - 0.5 * kv;
 }
 
-// The routed build's budget check.  The sampled FP32 units were built twice
-// more, in FP64 into (EJ64, EK64) and in FP32 into (EJ32, EK32): their G
-// difference, closed as the build closes G, is the sample's own FP32 error.
+// The routed build's budget check.  The sampled FP32 units are left out of
+// the FP32 queue and built apart twice, in FP64 into (EJ64, EK64) and in
+// FP32 into (EJ32, EK32): their G difference, closed as the build closes G,
+// is the sample's own FP32 error (close_kernel adds the sample's FP32 build
+// when the verdict keeps FP32, its FP64 build when it re-routes).
 // Its largest element goes to *max_bits (a non-negative double's bits order
 // like the double, so an integer atomicMax takes the maximum).
 __global__ void route_check_kernel(const double *__restrict__ EJ64, const double *__restrict__ EK64,
@@ -274,12 +287,12 @@ __global__ void route_units_kernel(const Unit *units, int unit0, int n_units, co
         const bool any = __any_sync(0xffffffffu, active);
         const bool all_low = __all_sync(0xffffffffu, low);
         if (lane == 0 && any) {
-            if (all_low) {
+            if (all_low && stride > 0 && i % stride == 0)
+                list_s[atomicAdd(counts + 2, 1)] = i;  // the check's sample: built apart, twice
+            else if (all_low)
                 list32[atomicAdd(counts + 0, 1)] = i;
-                if (stride > 0 && i % stride == 0) list_s[atomicAdd(counts + 2, 1)] = i;
-            } else {
+            else
                 list64[atomicAdd(counts + 1, 1)] = i;
-            }
         }
     }
 }
@@ -342,12 +355,12 @@ __global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units
         }
         const bool all_low = __all_sync(0xffffffffu, low);
         if (lane == 0 && any) {
-            if (all_low) {
+            if (all_low && stride > 0 && i % stride == 0)
+                list_s[atomicAdd(counts + 2, 1)] = i;  // the check's sample: built apart, twice
+            else if (all_low)
                 list32[atomicAdd(counts + 0, 1)] = i;
-                if (stride > 0 && i % stride == 0) list_s[atomicAdd(counts + 2, 1)] = i;
-            } else {
+            else
                 list64[atomicAdd(counts + 1, 1)] = i;
-            }
         }
     }
 }
@@ -1859,9 +1872,10 @@ int fjb_fock_build(fjb_handle *h, const double *D_dev, double *J_dev, double *K_
     }
     h->built = true;
     CUDA_OK(h, cudaEventRecordWithFlags(h->ev1, st, ev_flags));
-    close_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(h->Jp.p, h->Kp.p, nao, J_dev, K_dev, G_dev,
-                                                               check ? h->Jp32.p : nullptr,
-                                                               check ? h->Kp32.p : nullptr);
+    close_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(
+        h->Jp.p, h->Kp.p, nao, J_dev, K_dev, G_dev, check ? h->Jp32.p : nullptr, check ? h->Kp32.p : nullptr,
+        check ? h->EJ32.p : nullptr, check ? h->EK32.p : nullptr, check ? h->EJ64.p : nullptr,
+        check ? h->EK64.p : nullptr, check ? h->check_flag.p : nullptr);
     ++launches;
     CUDA_OK(h, cudaGetLastError());
     h->last_launches = launches;
@@ -2074,7 +2088,7 @@ int fjb_route_stats(const fjb_handle *hc, int64_t *n32, int64_t *n64) {
     *n64 = 0;
     for (size_t ri = 0; ri < h->runs.size(); ++ri) {
         if (h->last_routed) {
-            *n32 += c[4 * ri];
+            *n32 += c[4 * ri] + (h->last_checked ? c[4 * ri + 2] : 0);  // the check's sample is FP32 too
             *n64 += c[4 * ri + 1];
         } else {
             *n64 += h->runs[ri].n_units;

@@ -466,14 +466,15 @@ int fjb_df_eri3(fjb_handle *h, int aux_shell0, int aux_shell1, double tau, doubl
 int fjb_df_syrk(fjb_handle *h, const double *Z_dev, int64_t rows, int64_t cols, double *K_dev, void *stream);
 
 /* The routed build's error-budget check (on by default: budget 1e-8,
- * stride 16).  Every stride-th unit the router puts on the FP32 queue is
- * built twice more, in FP32 and in FP64, into side accumulators; the
- * largest element of their G difference times sqrt(stride) estimates the
- * FP32 queue's error in G (independent rounding errors of stride times as
- * many units: a statistical estimate, not a bound).  If the estimate
- * exceeds `budget`, the same build re-runs
- * every FP32 unit in FP64 and uses those results: the build falls back to
- * plain FP64 by itself, on the device, inside a captured graph too.  The
+ * stride 16).  Every stride-th unit the router would put on the FP32 queue
+ * is built apart instead, twice, in FP32 and in FP64, into side
+ * accumulators; the largest element of their G difference times
+ * sqrt(stride) estimates the FP32 queue's error in G (independent rounding
+ * errors of stride times as many units: a statistical estimate, not a
+ * bound).  If the estimate is within `budget` the sample's FP32 build joins
+ * G; otherwise the same build re-runs every other FP32 unit in FP64 and
+ * takes the sample's FP64 build: the build falls back to plain FP64 by
+ * itself, on the device, inside a captured graph too.  The
  * first checked build of a handle allocates six n_ao^2 side buffers: make it
  * before any capture of your own (fjb_fock_build_graph does).  budget <= 0
  * turns the check off.  No counterpart in the reference; it is the
