@@ -337,7 +337,7 @@ def main():
         n32, n64 = route_counts(eng)
         est, rerouted = eng.route_check()
         router_info = dict(router_info or {"kind": "bound"}, fp32_units=n32, fp64_units=n64,
-                           budget_check={"budget": 1e-8, "sample_stride": 16, "estimate": est,
+                           budget_check={"budget": 1e-8, "sample_stride": 32, "estimate": est,
                                          "rerouted_to_fp64": rerouted})
         if a.budget_threshold > 0:
             msb, _, _, _, _, Gb = timed(_lib.FJB_ROUTED, a.budget_threshold)

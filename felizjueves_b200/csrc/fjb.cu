@@ -1009,7 +1009,7 @@ struct fjb_handle {
     // the routed build's budget check (fjb_set_route_check): the FP32 queue's
     // own accumulators, the sample's FP64 and FP32 twins, the verdict
     double check_budget = 1e-8;
-    int check_stride = 16;
+    int check_stride = 32;
     DevBuf<double> Jp32, Kp32, EJ64, EK64, EJ32, EK32;
     DevBuf<unsigned long long> check_max;
     DevBuf<int> check_flag;

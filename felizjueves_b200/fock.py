@@ -295,7 +295,7 @@ class FockEngine:
         2 every class it has."""
         _lib.check(self._L.fjb_set_rys(self._h, int(mode)), self._h)
 
-    def set_route_check(self, budget: float = 1e-8, stride: int = 16) -> None:
+    def set_route_check(self, budget: float = 1e-8, stride: int = 32) -> None:
         """The routed build's error-budget check (fjb_set_route_check): a
         sampled FP64 re-build of every stride-th FP32 unit estimates the
         FP32 error in G; over `budget` the build re-runs its FP32 units in

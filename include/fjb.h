@@ -466,7 +466,7 @@ int fjb_df_eri3(fjb_handle *h, int aux_shell0, int aux_shell1, double tau, doubl
 int fjb_df_syrk(fjb_handle *h, const double *Z_dev, int64_t rows, int64_t cols, double *K_dev, void *stream);
 
 /* The routed build's error-budget check (on by default: budget 1e-8,
- * stride 16).  Every stride-th unit the router would put on the FP32 queue
+ * stride 32).  Every stride-th unit the router would put on the FP32 queue
  * is built apart instead, twice, in FP32 and in FP64, into side
  * accumulators; the largest element of their G difference times
  * sqrt(stride) estimates the FP32 queue's error in G (independent rounding
