@@ -64,6 +64,8 @@ def parse():
                     help="router path: launched quartets sampled per training cluster")
     ap.add_argument("--router-out", default="",
                     help="router path: where to save the trained network (.npz)")
+    ap.add_argument("--router-threshold", type=float, default=1e-9,
+                    help="router path: the routed builds' threshold")
     ap.add_argument("--router-in", default="",
                     help="router path: evaluate this trained network (.npz) instead of training one "
                          "(its reach from a fresh c3 sample)")
@@ -330,7 +332,7 @@ def main():
     ms64, ck64, nl64, cs, ls, G64 = timed(_lib.FJB_FP64)
     router_info = None
     if a.precision == "routed" and a.router == "learned":
-        router_info = install_learned_router(eng)
+        router_info = install_learned_router(eng, a.threshold)
     budget = None
     if a.precision == "routed":
         ms, ck, nl, cs_r, ls_r, Gr = timed(_lib.FJB_ROUTED, a.threshold)
@@ -340,6 +342,8 @@ def main():
                            budget_check={"budget": 1e-8, "sample_stride": 32, "estimate": est,
                                          "rerouted_to_fp64": rerouted})
         if a.budget_threshold > 0:
+            if a.router == "learned":
+                install_learned_router(eng, a.budget_threshold)
             msb, _, _, _, _, Gb = timed(_lib.FJB_ROUTED, a.budget_threshold)
             estb, rrb = eng.route_check()
             budget = {"threshold": a.budget_threshold, "ms_per_step": round(msb, 3),
@@ -438,14 +442,14 @@ def ctypes_probe(_lib, fp32: int) -> float:
     return float(v.value)
 
 
-def install_learned_router(eng) -> dict:
+def install_learned_router(eng, threshold: float = 1e-9) -> dict:
     """The network trained for config c3 (router.load_default: 7.87 M FP64
     quartets of 200 seeded 8-64-atom clusters; bench.py --path router
-    retrains it), installed on `eng` at the 1e-9 threshold with its
-    calibrated margin, reach and class gate."""
+    retrains it), installed on `eng` at the routed build's threshold with
+    its calibrated margin, reach and class gate."""
     from felizjueves_b200 import router
     mlp, margin, reach, min_l = router.load_default(device=eng.device)
-    router.install(eng, mlp, threshold=1e-9, margin=margin, reach=reach, min_total_l=min_l)
+    router.install(eng, mlp, threshold=threshold, margin=margin, reach=reach, min_total_l=min_l)
     return {"kind": "learned", "training_quartets": 7867810, "margin_log10": round(margin, 3),
             "reach_decades": reach, "min_total_l": min_l}
 
@@ -564,7 +568,7 @@ def router_path(a, local):
     by the FP64 HGP tap (log10 of the largest deposit into G), about 1e7 in
     all -- on the GPU with the library's MLP kernels, calibrated on held-out
     quartets; then on the c1 system (not in the training set) the routed
-    build at 1e-9 with the learned router against the bound alone, both with
+    build at `--router-threshold` (1e-9) with the learned router against the bound alone, both with
     the on-device budget check, against the FP64 build.  W warm-up and K
     timed graph replays each."""
     import time as _t
@@ -580,7 +584,9 @@ def router_path(a, local):
         va = np.arange(len(X))
         tr = np.arange(int(z["n_train"]))
         mlp = router.MLP(z["params"], device=local)
-        margin, losses, t_train = float(z["margin"]), [float("nan")], 0.0
+        # the margin recalibrated on the fresh, held-out sample, through the
+        # routing pass's own arithmetic
+        margin, losses, t_train = router.calibrate(mlp, X, y, 0.999), [float("nan")], 0.0
     else:
         X, y = router.training_set(router.c3_clusters(a.clusters), n_per=a.router_samples, seed=1)
         perm = np.random.default_rng(2).permutation(len(X))
@@ -596,7 +602,8 @@ def router_path(a, local):
     rmse_va = float(np.sqrt(np.mean((y[va] - mlp.predict(X[va]).cpu().numpy()) ** 2)))
     reach = router.reach(mlp, X[va], margin)
     if a.router_out:
-        np.savez(a.router_out, params=mlp.params(), margin=margin, reach=reach, n_train=len(tr))
+        gate = {"min_total_l": int(z["min_total_l"])} if a.router_in and "min_total_l" in z else {}
+        np.savez(a.router_out, params=mlp.params(), margin=margin, reach=reach, n_train=len(tr), **gate)
     w = configs.c1()
     eng = FockEngine(w.basis, device=local)
     eng.plan(w.D, w.tau, w.n_mag)
@@ -618,19 +625,22 @@ def router_path(a, local):
 
     ms64 = timed(_lib.FJB_FP64, 0.0)
     G64 = G.clone()
+    thr = a.router_threshold
     res = {}
-    for kind in ("bound", "learned", "learned_gated"):
+    for kind in ("bound", "learned", "learned_r05", "learned_gated"):
         if kind == "learned":
-            router.install(eng, mlp, threshold=1e-9, margin=margin, reach=reach)
+            router.install(eng, mlp, threshold=thr, margin=margin, reach=reach)
+        if kind == "learned_r05":  # every class, reach 0.5 decades
+            router.install(eng, mlp, threshold=thr, margin=margin, reach=0.5)
         if kind == "learned_gated":  # the reach and class gate measured best on c1
-            router.install(eng, mlp, threshold=1e-9, margin=margin, reach=0.5, min_total_l=7)
-        ms = timed(_lib.FJB_ROUTED, 1e-9)
+            router.install(eng, mlp, threshold=thr, margin=margin, reach=0.5, min_total_l=7)
+        ms = timed(_lib.FJB_ROUTED, thr)
         n32, n64 = router.route_stats(eng)
         est, rr = eng.route_check()
         res[kind] = {"ms_per_step": round(ms, 3), "speedup_vs_fp64": round(ms64 / ms, 4),
                      "max_abs_dG_vs_fp64": float((G - G64).abs().max()), "fp32_units": n32,
                      "fp64_units": n64, "budget_check": {"estimate": est, "rerouted_to_fp64": rr}}
-    line = {"metric": "learned router on c1: routed G build ms/iter at 1e-9 vs the bound alone",
+    line = {"metric": f"learned router on c1: routed G build ms/iter at {thr:g} vs the bound alone",
             "value": res["learned"]["ms_per_step"], "unit": "ms/iter", "n_gpus": 1, "steps": a.steps,
             "warmup": a.warmup, "higher_is_better": False, "data": "synthetic", "dtype": "f64+f32",
             "config": {"workload": "c3: train on seeded 8-64-atom clusters, evaluate on c1",
@@ -639,7 +649,9 @@ def router_path(a, local):
             "data_s": round(t_data, 1), "train_s": round(t_train, 1), "epochs": len(losses),
             "final_train_mse_log10": round(losses[-1], 5), "validation_rmse_log10": round(rmse_va, 4),
             "margin_log10": round(margin, 4), "reach_decades": reach, "fp64_ms_per_step": round(ms64, 3),
-            "bound": res["bound"], "learned": res["learned"], "learned_gated": res["learned_gated"],
+            "bound": res["bound"], "learned": res["learned"], "learned_r05": res["learned_r05"],
+            "learned_gated": res["learned_gated"],
+            "learned_r05_gain_vs_bound": round(res["bound"]["ms_per_step"] / res["learned_r05"]["ms_per_step"], 4),
             "learned_gain_vs_bound": round(res["bound"]["ms_per_step"] / res["learned"]["ms_per_step"], 4),
             "learned_gated_gain_vs_bound": round(res["bound"]["ms_per_step"] /
                                                  res["learned_gated"]["ms_per_step"], 4)}

@@ -317,7 +317,10 @@ __global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units
                                        int stride, int *list_s, const MolCtx *mols = nullptr,
                                        const int32_t *launch_mol = nullptr) {
     __shared__ float sp[kNParams];
+    __shared__ __align__(16) __half wh[kTcSmemHalves];
+    __shared__ __align__(16) __half xs[4][32 * kXRow];  // 128 threads
     for (int i = threadIdx.x; i < kNParams; i += blockDim.x) sp[i] = params[i];
+    stage_mlp_half(params, wh, wh + kHid * kW1Row);
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -343,15 +346,18 @@ __global__ void route_units_mlp_kernel(const Unit *units, int unit0, int n_units
             reach = !need || b < thresh * reach_factor;
         }
         const bool any = __any_sync(0xffffffffu, active);
-        bool low = true;
+        bool low = !need;
         // a unit goes FP32 only if all its quartets do: if one is out of the
-        // network's reach the unit stays FP64 and the network is not run
-        if (__all_sync(0xffffffffu, reach) && need) {
+        // network's reach the unit stays FP64 and the network is not run; it
+        // runs on the whole warp (the tensor-core products take every lane)
+        if (__all_sync(0xffffffffu, reach) && __any_sync(0xffffffffu, need)) {
             float f[kFeat];
-            quartet_features(bra, ket, prims, la, lb, lc, ld, dmax, f);
-            low = mlp_forward(sp, f, nullptr, nullptr) < log_thr;
-        } else if (need) {
-            low = false;
+            if (need)
+                quartet_features(bra, ket, prims, la, lb, lc, ld, dmax, f);
+            else
+                for (int q = 0; q < kFeat; ++q) f[q] = sp[kOffMu + q];
+            const float y = mlp_forward_tc(sp, wh, wh + kHid * kW1Row, xs[threadIdx.x >> 5], f);
+            if (need) low = y < log_thr;
         }
         const bool all_low = __all_sync(0xffffffffu, low);
         if (lane == 0 && any) {

@@ -1,5 +1,7 @@
 // router.cu -- training and inference kernels of the learned precision router
-// (router.cuh has the network and the features).
+// (router.cuh has the network and the features).  Inference is
+// mlp_forward_tc_kernel, the arithmetic the routing pass runs (FP16 tensor-
+// core products); mlp_forward_kernel is the FP32 forward of training.
 //
 // Training is mini-batch Adam on the mean squared error of the predicted
 // log10 deposit.  A step is three kernels, all FP32 and deterministic:
@@ -31,6 +33,26 @@ __global__ void mlp_forward_kernel(const float *__restrict__ p, const float *__r
         float x[kFeat];
         for (int i = 0; i < kFeat; ++i) x[i] = X[(size_t)s * kFeat + i];
         Y[s] = mlp_forward(sp, x, nullptr, nullptr);
+    }
+}
+
+// The router's inference arithmetic (mlp_forward_tc), a warp per 32 samples.
+__global__ void mlp_forward_tc_kernel(const float *__restrict__ p, const float *__restrict__ X, int n,
+                                      float *__restrict__ Y) {
+    __shared__ float sp[kNParams];
+    __shared__ __align__(16) __half wh[kTcSmemHalves];
+    __shared__ __align__(16) __half xs[4][32 * kXRow];
+    for (int i = threadIdx.x; i < kNParams; i += blockDim.x) sp[i] = p[i];
+    stage_mlp_half(p, wh, wh + kHid * kW1Row);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int warp = blockIdx.x * (blockDim.x >> 5) + w, nwarps = gridDim.x * (blockDim.x >> 5);
+    for (int s0 = 32 * warp; s0 < n; s0 += 32 * nwarps) {  // warp-uniform
+        const int s = s0 + lane;
+        float x[kFeat];
+        for (int i = 0; i < kFeat; ++i) x[i] = s < n ? X[(size_t)s * kFeat + i] : sp[kOffMu + i];
+        const float y = mlp_forward_tc(sp, wh, wh + kHid * kW1Row, xs[w], x);
+        if (s < n) Y[s] = y;
     }
 }
 
@@ -126,6 +148,15 @@ int fjb_mlp_forward(const float *params_dev, const float *X_dev, int n, float *Y
     mlp_forward_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(params_dev, X_dev, n, Y_dev);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? FJB_OK : rfail("mlp_forward", e);
+}
+
+int fjb_mlp_forward_tc(const float *params_dev, const float *X_dev, int n, float *Y_dev, void *stream) {
+    if (!params_dev || !X_dev || !Y_dev || n < 0) return FJB_E_ARG;
+    if (n == 0) return FJB_OK;
+    const int grid = std::min((n + 127) / 128, 148 * 8);
+    mlp_forward_tc_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(params_dev, X_dev, n, Y_dev);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FJB_OK : rfail("mlp_forward_tc", e);
 }
 
 int fjb_mlp_gradient(const float *params_dev, const float *X_dev, const float *T_dev, int n, float *grad_dev,

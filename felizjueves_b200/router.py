@@ -74,12 +74,15 @@ class MLP:
     def params(self) -> np.ndarray:
         return self.p.cpu().numpy()
 
-    def predict(self, X):
+    def predict(self, X, *, exact: bool = False):
+        """The network's prediction in the routing pass's own arithmetic
+        (fjb_mlp_forward_tc: FP16 tensor-core products), or with `exact` in
+        the FP32 arithmetic of training (fjb_mlp_forward)."""
         import torch
         X = torch.as_tensor(X, dtype=torch.float32, device=self.dev).contiguous()
         Y = torch.empty(len(X), dtype=torch.float32, device=self.dev)
-        _lib.check(self._L.fjb_mlp_forward(self.p.data_ptr(), X.data_ptr(), len(X), Y.data_ptr(),
-                                           None))
+        f = self._L.fjb_mlp_forward if exact else self._L.fjb_mlp_forward_tc
+        _lib.check(f(self.p.data_ptr(), X.data_ptr(), len(X), Y.data_ptr(), None))
         return Y
 
     def gradient(self, X, T):

@@ -267,10 +267,10 @@ int fjb_router_set(fjb_handle *h, const float *params_host, float log10_threshol
  * keeps more units FP64. */
 int fjb_router_reach(fjb_handle *h, double decades);
 /* Which classes ask the network: those with la + lb + lc + ld >=
- * min_total_l (default 0, every class).  The network costs a few thousand
- * flops a quartet, more than a small class's whole quartet, so below some
- * total angular momentum asking it costs more than the FP32 units it adds
- * save; those classes route by the bound alone. */
+ * min_total_l (default 0, every class).  Asking the network costs a few
+ * hundred tensor-core cycles a warp of 32 quartets, so below some total
+ * angular momentum it can cost more than the FP32 units it adds save;
+ * those classes route by the bound alone. */
 int fjb_router_classes(fjb_handle *h, int min_total_l);
 /* Features (n x 12 floats) and six-block bounds (n doubles) of sampled
  * launched quartets, samples[3i..3i+2] = (launch, bra index, ket index) in
@@ -281,6 +281,11 @@ int fjb_router_features(fjb_handle *h, const double *D_dev, const int32_t *sampl
  * the mean-squared-error gradient of a batch (scratch_dev holds n x 257
  * floats, sq_err_dev n floats); one Adam step (step counts from 1). */
 int fjb_mlp_forward(const float *params_dev, const float *X_dev, int n, float *Y_dev, void *stream);
+/* The same network's forward in the routing pass's own arithmetic: both
+ * hidden layers as FP16 x FP16 -> FP32 tensor-core products (mma.sync
+ * m16n8k16), tanh by the hardware approximation.  The router's margin is
+ * calibrated through this call.  Same arguments as fjb_mlp_forward. */
+int fjb_mlp_forward_tc(const float *params_dev, const float *X_dev, int n, float *Y_dev, void *stream);
 int fjb_mlp_gradient(const float *params_dev, const float *X_dev, const float *T_dev, int n, float *grad_dev,
                      float *sq_err_dev, float *scratch_dev, void *stream);
 int fjb_mlp_adam(float *params_dev, const float *grad_dev, float *m_dev, float *v_dev, float lr, int step,
