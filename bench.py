@@ -64,6 +64,9 @@ def parse():
                     help="router path: launched quartets sampled per training cluster")
     ap.add_argument("--router-out", default="",
                     help="router path: where to save the trained network (.npz)")
+    ap.add_argument("--router-label", default="deposit", choices=["deposit", "fp32_error"],
+                    help="router path: train on each quartet's largest deposit (log10) or on its "
+                         "largest FP32 error into G (the FP32 tap against the FP64 one)")
     ap.add_argument("--router-threshold", type=float, default=1e-9,
                     help="router path: the routed builds' threshold")
     ap.add_argument("--router-in", default="",
@@ -588,7 +591,8 @@ def router_path(a, local):
         # routing pass's own arithmetic
         margin, losses, t_train = router.calibrate(mlp, X, y, 0.999), [float("nan")], 0.0
     else:
-        X, y = router.training_set(router.c3_clusters(a.clusters), n_per=a.router_samples, seed=1)
+        X, y = router.training_set(router.c3_clusters(a.clusters), n_per=a.router_samples, seed=1,
+                                   label=a.router_label)
         perm = np.random.default_rng(2).permutation(len(X))
         ntr = int(0.9 * len(X))
         tr, va = perm[:ntr], perm[ntr:]
@@ -627,7 +631,12 @@ def router_path(a, local):
     G64 = G.clone()
     thr = a.router_threshold
     res = {}
-    for kind in ("bound", "learned", "learned_r05", "learned_gated"):
+    kinds = ("bound", "learned", "learned_r05", "learned_gated")
+    if a.router_label == "fp32_error":  # the network routes by its predicted FP32 error
+        kinds = ("bound", "err_1e-15", "err_1e-14", "err_1e-13")
+    for kind in kinds:
+        if kind.startswith("err_"):  # a unit's quartets each under the bound or predicted under this error
+            router.install(eng, mlp, threshold=float(kind[4:]), margin=margin, reach=1.0)
         if kind == "learned":
             router.install(eng, mlp, threshold=thr, margin=margin, reach=reach)
         if kind == "learned_r05":  # every class, reach 0.5 decades
@@ -641,7 +650,7 @@ def router_path(a, local):
                      "max_abs_dG_vs_fp64": float((G - G64).abs().max()), "fp32_units": n32,
                      "fp64_units": n64, "budget_check": {"estimate": est, "rerouted_to_fp64": rr}}
     line = {"metric": f"learned router on c1: routed G build ms/iter at {thr:g} vs the bound alone",
-            "value": res["learned"]["ms_per_step"], "unit": "ms/iter", "n_gpus": 1, "steps": a.steps,
+            "value": res[kinds[1]]["ms_per_step"], "unit": "ms/iter", "n_gpus": 1, "steps": a.steps,
             "warmup": a.warmup, "higher_is_better": False, "data": "synthetic", "dtype": "f64+f32",
             "config": {"workload": "c3: train on seeded 8-64-atom clusters, evaluate on c1",
                        "clusters": a.clusters, "samples_per_cluster": a.router_samples},
@@ -649,12 +658,9 @@ def router_path(a, local):
             "data_s": round(t_data, 1), "train_s": round(t_train, 1), "epochs": len(losses),
             "final_train_mse_log10": round(losses[-1], 5), "validation_rmse_log10": round(rmse_va, 4),
             "margin_log10": round(margin, 4), "reach_decades": reach, "fp64_ms_per_step": round(ms64, 3),
-            "bound": res["bound"], "learned": res["learned"], "learned_r05": res["learned_r05"],
-            "learned_gated": res["learned_gated"],
-            "learned_r05_gain_vs_bound": round(res["bound"]["ms_per_step"] / res["learned_r05"]["ms_per_step"], 4),
-            "learned_gain_vs_bound": round(res["bound"]["ms_per_step"] / res["learned"]["ms_per_step"], 4),
-            "learned_gated_gain_vs_bound": round(res["bound"]["ms_per_step"] /
-                                                 res["learned_gated"]["ms_per_step"], 4)}
+            "label": a.router_label, **res,
+            **{f"{k}_gain_vs_bound": round(res["bound"]["ms_per_step"] / res[k]["ms_per_step"], 4)
+               for k in kinds if k != "bound"}}
     print(json.dumps(line))
 
 

@@ -187,9 +187,13 @@ def features(eng: FockEngine, D, samples: np.ndarray):
     return F[:n].cpu().numpy(), B[:n].cpu().numpy()
 
 
-def training_set(workloads, n_per: int = 20000, seed: int = 0, zero_gap: float = -6.0):
+def training_set(workloads, n_per: int = 20000, seed: int = 0, zero_gap: float = -6.0,
+                 label: str = "deposit"):
     """(X, y): features and log10(max|(ab|cd)| x dmax) of sampled computed
-    quartets of each workload, the targets from the FP64 HGP tap.
+    quartets of each workload, the targets from the FP64 HGP tap; with
+    label="fp32_error", log10 of the quartet's largest FP32 error into G,
+    max|(ab|cd)_FP32 - (ab|cd)_FP64| x dmax (block_err), floored at 10^-14
+    of its bound, every computed quartet kept.
 
     Quartets more than 10^-zero_gap below their Schwarz x density bound are
     left out: they vanish by symmetry (one-centre quartets of odd total
@@ -206,9 +210,13 @@ def training_set(workloads, n_per: int = 20000, seed: int = 0, zero_gap: float =
         X, b = features(eng, w.D, s)
         keep = b >= w.tau  # computed (not screened) quartets only
         s, X, q = s[keep], X[keep], q[keep]
-        mx = block_max(eng, q)
-        y = np.log10(np.maximum(mx, 1e-300)) + X[:, 11]  # + log10 dmax
-        keep = y - bound_log10(X) > zero_gap
+        if label == "fp32_error":
+            y = np.maximum(np.log10(np.maximum(block_err(eng, q), 1e-300)) + X[:, 11], bound_log10(X) - 14.0)
+            keep = np.ones(len(y), bool)
+        else:
+            mx = block_max(eng, q)
+            y = np.log10(np.maximum(mx, 1e-300)) + X[:, 11]  # + log10 dmax
+            keep = y - bound_log10(X) > zero_gap
         Xs.append(X[keep])
         ys.append(y[keep].astype(np.float32))
         eng.close()
@@ -230,6 +238,28 @@ def block_max(eng: FockEngine, quartets: np.ndarray) -> np.ndarray:
                                   torch.as_tensor(np.diff(off), device=out.device))
     mx = torch.zeros(n, dtype=torch.float64, device=out.device)
     mx.scatter_reduce_(0, seg, out[: int(off[-1])].abs(), reduce="amax", include_self=True)
+    return mx.cpu().numpy()
+
+
+def block_err(eng: FockEngine, quartets: np.ndarray) -> np.ndarray:
+    """max |(ab|cd)_FP32 - (ab|cd)_FP64| of each quartet's block: the FP32
+    tap (fjb_eri_blocks_fp32, the routed path's FP32 recurrences) against
+    the FP64 one, segment maxima on the device."""
+    import torch
+    q = np.ascontiguousarray(quartets, np.int32)
+    n = len(q)
+    off = np.zeros(n + 1, np.int64)
+    nc = np.array([s.n_cart for s in eng.basis.shells], np.int64)
+    off[1:] = np.cumsum(nc[q[:, 0]] * nc[q[:, 1]] * nc[q[:, 2]] * nc[q[:, 3]])
+    dev = f"cuda:{eng.device}"
+    o64 = torch.empty(max(int(off[-1]), 1), dtype=torch.float64, device=dev)
+    o32 = torch.empty_like(o64)
+    _lib.check(eng._L.fjb_eri_blocks(eng._h, q.ctypes.data, n, o64.data_ptr(), off.ctypes.data), eng._h)
+    _lib.check(eng._L.fjb_eri_blocks_fp32(eng._h, q.ctypes.data, n, o32.data_ptr(), off.ctypes.data), eng._h)
+    seg = torch.repeat_interleave(torch.arange(n, device=dev), torch.as_tensor(np.diff(off), device=dev))
+    mx = torch.zeros(n, dtype=torch.float64, device=dev)
+    m = int(off[-1])
+    mx.scatter_reduce_(0, seg, (o32[:m] - o64[:m]).abs(), reduce="amax", include_self=True)
     return mx.cpu().numpy()
 
 
