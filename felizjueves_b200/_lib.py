@@ -111,6 +111,7 @@ def load():
     L.fjb_router_features.argtypes = [vp, vp, vp, C.c_int, vp, vp]
     L.fjb_mlp_forward.argtypes = [vp, vp, C.c_int, vp, vp]
     L.fjb_mlp_forward_tc.argtypes = [vp, vp, C.c_int, vp, vp]
+    L.fjb_plan_units.argtypes = [vp, vp, i64, C.POINTER(i64)]
     L.fjb_mlp_gradient.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp, vp]
     L.fjb_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_float, C.c_int, vp]
     L.fjb_route_stats.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
@@ -135,7 +136,7 @@ EXPORTS = ("fjb_last_error", "fjb_version", "fjb_create", "fjb_destroy", "fjb_n_
            "fjb_batch_last_error", "fjb_batch_destroy",
            "fjb_fock_build_graph", "fjb_create_df", "fjb_df_blocks", "fjb_mlp_n_params",
            "fjb_router_set", "fjb_router_reach", "fjb_router_classes", "fjb_router_features", "fjb_mlp_forward", "fjb_mlp_forward_tc",
-           "fjb_mlp_gradient",
+           "fjb_mlp_gradient", "fjb_plan_units",
            "fjb_mlp_adam", "fjb_route_stats", "fjb_coulomb", "fjb_coulomb_mixed", "fjb_j_last_launches",
            "fjb_j_plan_lists", "fjb_scatter_map", "fjb_one_electron")
 

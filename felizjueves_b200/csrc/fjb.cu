@@ -58,6 +58,13 @@ namespace {
 
 constexpr double kTwoOverSqrtPi = 1.1283791670955126;
 
+// The plan's work units, one CTA a launch, a thread a bra pair
+// (write_span_units: the host's own fill of the same list).
+__global__ void make_units_kernel(const UnitSpan *__restrict__ spans, Unit *__restrict__ units) {
+    const UnitSpan S = spans[blockIdx.x];
+    for (int ib = threadIdx.x; ib < S.n_bra; ib += blockDim.x) write_span_units(S, ib, units);
+}
+
 __global__ void density_blocks_kernel(const double *__restrict__ D, int n_ao, int n_sh,
                                       const int *__restrict__ off, const int *__restrict__ nc,
                                       double *__restrict__ Dsh) {
@@ -989,7 +996,9 @@ struct fjb_handle {
     std::vector<ClassRun> runs;
     int64_t quartets_launched = 0;
     int n_units = 0;
-    // host copies the atomics-free build's maps are made from
+    // host copies the atomics-free build's maps are made from (units_host
+    // filled from the spans on first use: ensure_units_host)
+    std::vector<UnitSpan> spans_host;
     std::vector<Unit> units_host;
     std::vector<LaunchRec> lr_host;
     std::vector<PairRec> pr_host;
@@ -1182,8 +1191,21 @@ int run_grid32(const ClassRun &r) {
 // exceed kScatterMaxSlots (2 GiB of W).
 constexpr int64_t kScatterMaxSlots = int64_t(1) << 28;
 
+// The host copy of the plan's work units (the device list's twin).
+void ensure_units_host(fjb_handle *h) {
+    if ((int64_t)h->units_host.size() == (int64_t)h->n_units) return;
+    h->units_host.assign((size_t)h->n_units, Unit{});
+    for (const UnitSpan &S : h->spans_host)
+        for (int ib = 0; ib < S.n_bra; ++ib) write_span_units(S, ib, h->units_host.data());
+}
+
 int ensure_scatter(fjb_handle *h) {
     if (h->scatter_ready) return FJB_OK;
+    try {
+        ensure_units_host(h);
+    } catch (const std::exception &e) {
+        return fail(h, FJB_E_CUDA, std::string("work units: ") + e.what());
+    }
     std::vector<int32_t> el, ptr, src;
     std::vector<int64_t> w_base;
     h->lsc.clear();
@@ -1472,7 +1494,6 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     std::vector<LaunchRec> lr;
     std::map<std::tuple<int, int, int, int>, std::vector<int>> class_launches;  // launch indices, plan order
     std::map<std::tuple<int, int, int, int>, std::pair<int, int>> class_deg;
-    size_t n_units_total = 0;
     int64_t qbase = 0;
     for (auto &L : P.launches) {
         const PlanBatch &br = P.batches[L.first], &kt = P.batches[L.second];
@@ -1493,42 +1514,42 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
         cd.first = std::max(cd.first, br.degree);
         cd.second = std::max(cd.second, kt.degree);
         class_launches[key].push_back(li);
-        for (int ib = 0; ib < r.n_bra; ++ib) {
-            const int k_begin = r.diag ? ib : 0;
-            if (r.n_ket > k_begin) n_units_total += (size_t)((r.n_ket - k_begin + kKetChunk - 1) / kKetChunk);
-        }
     }
     // the work units, class by class (the map's order), each class's
-    // launches in plan order: written once into one array
-    std::vector<Unit> units;
+    // launches in plan order: one span a launch; the units themselves are
+    // written on the device (make_units_kernel), and on the host only where
+    // a host copy is needed (host-only handles, the atomics-free build's
+    // maps, batches), by the same write_span_units
+    std::vector<UnitSpan> spans;
     std::map<std::tuple<int, int, int, int>, std::pair<int, int>> class_units;  // (first unit, count)
-    if (n_units_total > (size_t)INT32_MAX)
-        return fail(h, FJB_E_LIMIT, "more than 2^31 work units: the unit indices are 32-bit");
-    try {
-        units.reserve(n_units_total);
-        for (auto &kv : class_launches) {
-            const int u0 = (int)units.size();
-            for (int li : kv.second) {
-                const LaunchRec &r = lr[li];
-                for (int ib = 0; ib < r.n_bra; ++ib) {
-                    const int k_begin = r.diag ? ib : 0;
-                    for (int k0 = k_begin; k0 < r.n_ket; k0 += kKetChunk)
-                        units.push_back(Unit{li, ib, k0, std::min(r.n_ket, k0 + kKetChunk)});
-                }
-            }
-            class_units[kv.first] = {u0, (int)units.size() - u0};
+    int64_t n_units_total = 0;
+    for (auto &kv : class_launches) {
+        const int64_t u0 = n_units_total;
+        for (int li : kv.second) {
+            const LaunchRec &r = lr[li];
+            UnitSpan S{n_units_total, 0, li, r.n_bra, r.n_ket, r.diag ? 1 : 0};
+            S.count = span_units(S);
+            n_units_total += S.count;
+            spans.push_back(S);
         }
-    } catch (const std::exception &e) {
-        return fail(h, FJB_E_LIMIT, std::string("work units: ") + e.what());
+        if (n_units_total > (int64_t)INT32_MAX)
+            return fail(h, FJB_E_LIMIT, "more than 2^31 work units: the unit indices are 32-bit");
+        class_units[kv.first] = {(int)u0, (int)(n_units_total - u0)};
     }
     h->runs.clear();
     h->scatter_ready = false;
     h->lr_host = lr;
     h->pr_host = pr;
+    h->spans_host = std::move(spans);
+    h->units_host.clear();
+    h->n_units = (int)n_units_total;
     if (h->device < 0) {  // host-only: the lists are complete, nothing is staged
-        h->units_host = std::move(units);
+        try {
+            ensure_units_host(h);
+        } catch (const std::exception &e) {
+            return fail(h, FJB_E_LIMIT, std::string("work units: ") + e.what());
+        }
         h->quartets_launched = qbase;
-        h->n_units = (int)h->units_host.size();
         h->planned = true;
         return FJB_OK;
     }
@@ -1561,8 +1582,15 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
         h->pairs.upload(pr);
         h->prims.upload(pm);
         h->launches.upload(lr);
-        h->units.upload(units);
-        h->units_host = std::move(units);
+        h->units.alloc(std::max<int64_t>(n_units_total, 1));
+        if (!h->spans_host.empty()) {
+            DevBuf<UnitSpan> dspans;
+            dspans.upload(h->spans_host);
+            make_units_kernel<<<(unsigned)h->spans_host.size(), 128>>>(dspans.p, h->units.p);
+            cudaError_t e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+            if (e != cudaSuccess) throw std::runtime_error(std::string("make_units_kernel: ") + cudaGetErrorString(e));
+        }
         const size_t nn = (size_t)h->basis.n_ao * h->basis.n_ao;
         const size_t ns = h->basis.shells.size();
         h->Dsh.alloc(ns * ns);
@@ -1596,7 +1624,7 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
             lc.push_back(s.ld);
         }
         h->launch_cls.upload(lc);
-        h->route_list.alloc(std::max<size_t>(1, 3 * h->units_host.size()));
+        h->route_list.alloc(std::max<size_t>(1, 3 * (size_t)h->n_units));
         h->route_counts.alloc(std::max<size_t>(1, 4 * h->runs.size()));
         if (h->Jp32.n) {  // the budget check's buffers follow the plan's size
             h->Jp32.reset();
@@ -1607,8 +1635,24 @@ int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag) {
     }
     h->built = false;
     h->quartets_launched = qbase;
-    h->n_units = (int)h->units_host.size();
     h->planned = true;
+    return FJB_OK;
+}
+
+int fjb_plan_units(const fjb_handle *hc, int32_t *units_host, int64_t cap, int64_t *n_units) {
+    fjb_handle *h = const_cast<fjb_handle *>(hc);
+    if (!h || !n_units || cap < 0) return fail(h, FJB_E_ARG, "null argument");
+    if (!h->planned) return fail(h, FJB_E_STATE, "no plan: call fjb_plan first");
+    *n_units = h->n_units;
+    if (!units_host) return FJB_OK;
+    if (cap < h->n_units) return fail(h, FJB_E_ARG, "units_host holds fewer than n_units units");
+    if (h->n_units == 0) return FJB_OK;
+    if (h->device < 0) {
+        std::memcpy(units_host, h->units_host.data(), (size_t)h->n_units * sizeof(Unit));
+        return FJB_OK;
+    }
+    CUDA_OK(h, cudaSetDevice(h->device));
+    CUDA_OK(h, cudaMemcpy(units_host, h->units.p, (size_t)h->n_units * sizeof(Unit), cudaMemcpyDeviceToHost));
     return FJB_OK;
 }
 
@@ -3168,6 +3212,7 @@ int fjb_batch_create(fjb_batch **out, fjb_handle *const *handles, int n) {
         for (int m = 0; m < n; ++m) {
             fjb_handle *h = b->mols[m];
             const int P0 = (int)pr.size(), Q0 = (int)pm.size(), L0 = (int)lr.size();
+            ensure_units_host(h);
             std::vector<PrimRec> hp(h->prims.n);
             if (!hp.empty() &&
                 cudaMemcpy(hp.data(), h->prims.p, hp.size() * sizeof(PrimRec), cudaMemcpyDeviceToHost) != cudaSuccess)

@@ -3,6 +3,12 @@
 #pragma once
 #include <cstdint>
 
+#ifdef __CUDACC__
+#define FJB_HD __host__ __device__
+#else
+#define FJB_HD
+#endif
+
 namespace fjb {
 
 constexpr int kMaxL = 3;          // per shell in the Fock build
@@ -70,6 +76,38 @@ struct LaunchRec {
 struct Unit {
     int32_t launch, ib, k0, k1;
 };
+
+// The work units of one launch: for each bra pair ib, its kets from k_begin
+// (ib on a diagonal launch, where the bra and ket batches are one; else 0)
+// in chunks of kKetChunk.  base is the launch's first unit in the plan's
+// unit order (class by class, each class's launches in plan order).
+struct UnitSpan {
+    int64_t base, count;
+    int32_t launch, n_bra, n_ket, diag;
+};
+
+// sum over m = 1..x of ceil(m / kKetChunk): the units of a diagonal launch's
+// last x bra pairs
+FJB_HD inline int64_t diag_chunk_sum(int64_t x) {
+    const int64_t q = x / kKetChunk, r = x % kKetChunk;
+    return kKetChunk * q * (q + 1) / 2 + r * (q + 1);
+}
+
+FJB_HD inline int64_t span_units(const UnitSpan &S) {
+    if (S.diag) return diag_chunk_sum(S.n_ket);
+    return (int64_t)S.n_bra * ((S.n_ket + kKetChunk - 1) / kKetChunk);
+}
+
+// Bra pair ib's units, written at their place in units[]: the host and the
+// device fill the plan's unit list with this same code.
+FJB_HD inline void write_span_units(const UnitSpan &S, int ib, Unit *units) {
+    const int k_begin = S.diag ? ib : 0;
+    int64_t at = S.base + (S.diag ? diag_chunk_sum(S.n_ket) - diag_chunk_sum(S.n_ket - ib)
+                                  : (int64_t)ib * ((S.n_ket + kKetChunk - 1) / kKetChunk));
+    const int64_t end = S.base + S.count;
+    for (int k0 = k_begin; k0 < S.n_ket && at < end; k0 += kKetChunk)
+        units[at++] = Unit{S.launch, ib, k0, k0 + kKetChunk < S.n_ket ? k0 + kKetChunk : S.n_ket};
+}
 
 // Device view of one class's tables (all pointers are device pointers).
 struct ClassDev {

@@ -432,6 +432,16 @@ class FockEngine:
         _lib.check(self._L.fjb_set_class_config32(self._h, *map(int, cls), int(threads),
                                                   int(slots)), self._h)
 
+    def plan_units(self) -> np.ndarray:
+        """The plan's work units, (n, 4) int32 rows (launch, bra pair
+        index, first ket, end ket), in the order the class kernels take
+        them (fjb_plan_units)."""
+        n = C.c_int64()
+        _lib.check(self._L.fjb_plan_units(self._h, None, 0, C.byref(n)), self._h)
+        out = np.zeros((max(n.value, 1), 4), np.int32)
+        _lib.check(self._L.fjb_plan_units(self._h, out.ctypes.data, n.value, C.byref(n)), self._h)
+        return out[: n.value]
+
     def launch_stats(self) -> list[dict]:
         """Per launch: class, degrees, quartets met and computed by the last
         build."""

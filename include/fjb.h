@@ -139,6 +139,13 @@ void fjb_destroy(fjb_handle *h);
 int fjb_plan(fjb_handle *h, const double *D_host, double tau, int n_mag);
 int fjb_plan_counts(const fjb_handle *h, fjb_plan_counts_t *out);
 int fjb_plan_export(const fjb_handle *h, fjb_plan_lists *out);
+/* The plan's work units, 4 int32 each (launch, bra pair index, first ket
+ * index, end ket index), in the order the build's class kernels take them
+ * (class by class, each class's launches in plan order, each bra pair's
+ * kets in chunks of 32).  The runtime writes them on the device from one
+ * span a launch; this copies them to units_host (HOST, room for cap units;
+ * NULL to ask only for n_units).  Synchronises. */
+int fjb_plan_units(const fjb_handle *h, int32_t *units_host, int64_t cap, int64_t *n_units);
 int fjb_n_ao(const fjb_handle *h);
 
 /* The six-block screen decision of every launched quartet, in (launch, bra
