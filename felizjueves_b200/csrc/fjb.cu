@@ -3203,7 +3203,7 @@ int fjb_batch_create(fjb_batch **out, fjb_handle *const *handles, int n) {
     std::vector<PrimRec> pm;
     std::vector<LaunchRec> lr;
     std::vector<int32_t> lmol;
-    std::map<std::tuple<int, int, int, int>, std::vector<Unit>> by_class;
+    std::map<std::tuple<int, int, int, int>, std::vector<UnitSpan>> by_class;  // the molecules' spans
     std::map<std::tuple<int, int, int, int>, std::pair<const ClassRun *, std::pair<int, int>>> first;
     std::vector<int> sh_off, sh_nc;
     std::vector<int64_t> dsh0, nn0;
@@ -3212,7 +3212,6 @@ int fjb_batch_create(fjb_batch **out, fjb_handle *const *handles, int n) {
         for (int m = 0; m < n; ++m) {
             fjb_handle *h = b->mols[m];
             const int P0 = (int)pr.size(), Q0 = (int)pm.size(), L0 = (int)lr.size();
-            ensure_units_host(h);
             std::vector<PrimRec> hp(h->prims.n);
             if (!hp.empty() &&
                 cudaMemcpy(hp.data(), h->prims.p, hp.size() * sizeof(PrimRec), cudaMemcpyDeviceToHost) != cudaSuccess)
@@ -3228,14 +3227,13 @@ int fjb_batch_create(fjb_batch **out, fjb_handle *const *handles, int n) {
                 lr.push_back(L);
                 lmol.push_back(m);
             }
+            for (UnitSpan S : h->spans_host) {
+                const fjb_launch_stat &ls = h->lstat[S.launch];
+                S.launch += L0;
+                by_class[std::make_tuple(ls.la, ls.lb, ls.lc, ls.ld)].push_back(S);
+            }
             for (const ClassRun &r : h->runs) {
                 const auto key = std::make_tuple(r.dev.la, r.dev.lb, r.dev.lc, r.dev.ld);
-                auto &v = by_class[key];
-                for (int u = r.unit0; u < r.unit0 + r.n_units; ++u) {
-                    Unit U = h->units_host[u];
-                    U.launch += L0;
-                    v.push_back(U);
-                }
                 auto it = first.find(key);
                 if (it == first.end())
                     first[key] = {&r, {r.max_kab, r.max_kcd}};
@@ -3257,22 +3255,40 @@ int fjb_batch_create(fjb_batch **out, fjb_handle *const *handles, int n) {
             b->max_nsh = std::max(b->max_nsh, nsh);
             b->max_nn = std::max(b->max_nn, (size_t)nao * nao);
         }
-        std::vector<Unit> units;
+        // the merged units, class by class, each class's molecules in order:
+        // the molecules' spans re-based, the units written on the device
+        std::vector<UnitSpan> spans;
+        int64_t total = 0;
         for (auto &kv : by_class) {
             const ClassRun *src = first[kv.first].first;
             ClassRun r = *src;
-            r.unit0 = (int)units.size();
-            r.n_units = (int)kv.second.size();
+            const int64_t u0 = total;
+            for (UnitSpan S : kv.second) {
+                S.base = total;
+                total += S.count;
+                spans.push_back(S);
+            }
+            if (total > (int64_t)INT32_MAX)
+                return bfail(nullptr, FJB_E_LIMIT, "fjb_batch_create: more than 2^31 work units");
+            r.unit0 = (int)u0;
+            r.n_units = (int)(total - u0);
             r.max_kab = first[kv.first].second.first;
             r.max_kcd = first[kv.first].second.second;
-            units.insert(units.end(), kv.second.begin(), kv.second.end());
             b->runs.push_back(r);
         }
-        b->n_units = (int)units.size();
+        b->n_units = (int)total;
         b->pairs.upload(pr);
         b->prims.upload(pm);
         b->launches.upload(lr);
-        b->units.upload(units);
+        b->units.alloc(std::max<int64_t>(total, 1));
+        if (!spans.empty()) {
+            DevBuf<UnitSpan> dspans;
+            dspans.upload(spans);
+            make_units_kernel<<<(unsigned)spans.size(), 128>>>(dspans.p, b->units.p);
+            cudaError_t e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+            if (e != cudaSuccess) throw std::runtime_error(std::string("make_units_kernel: ") + cudaGetErrorString(e));
+        }
         b->launch_mol.upload(lmol);
         b->sh_off.upload(sh_off);
         b->sh_nc.upload(sh_nc);
