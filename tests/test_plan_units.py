@@ -45,6 +45,13 @@ def test_host_units_follow_the_class_order(lib_built, n_atoms, seed):
     assert np.array_equal(got, exp)
 
 
+def test_everything_screened_gives_no_units(lib_built):
+    w = configs.cluster(2, 5)
+    eng = FockEngine(w.basis, device=-1)
+    P = eng.plan(w.D, 1e6, w.n_mag)
+    assert len(P.launches) == 0 and eng.plan_units().shape == (0, 4)
+
+
 def test_unit_buffer_too_small_is_refused(lib_built):
     import ctypes as C
     w = configs.cluster(2, 5)
