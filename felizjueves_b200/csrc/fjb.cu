@@ -809,6 +809,19 @@ __global__ void __launch_bounds__(NT) hgp_fock_kernel(const KArgs A) {
 namespace {
 
 
+// A class's recurrence programs, built once per process (every handle
+// uploads its own copy; the build is the costly part: about 0.2 s for all
+// 54 classes, which a batch of molecules would otherwise pay per molecule).
+const ClassHost &class_host_cached(int la, int lb, int lc, int ld) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int>, std::unique_ptr<ClassHost>> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_tuple(la, lb, lc, ld);
+    auto it = cache.find(key);
+    if (it == cache.end()) it = cache.emplace(key, std::make_unique<ClassHost>(build_class(la, lb, lc, ld))).first;
+    return *it->second;
+}
+
 template <typename T>
 struct DevBuf {
     T *p = nullptr;
@@ -1097,7 +1110,7 @@ struct fjb_handle {
         auto it = classes.find(key);
         if (it != classes.end()) return *it->second;
         auto e = std::make_unique<ClassEntry>();
-        e->host = build_class(la, lb, lc, ld);
+        e->host = class_host_cached(la, lb, lc, ld);
         e->upload();
         auto &ref = *e;
         classes[key] = std::move(e);
