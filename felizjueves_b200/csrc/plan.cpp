@@ -35,9 +35,32 @@
 
 namespace fjb {
 
+namespace {
+// fsum's partials: at most about 40 non-overlapping doubles ever (their
+// exponents are distinct and span the double range), so a fixed buffer on
+// the stack holds them; it grows onto the heap only if that bound is passed.
+struct Partials {
+    double fixed[64];
+    std::vector<double> spill;
+    double *d = fixed;
+    size_t n = 0, cap = 64;
+    size_t size() const { return n; }
+    double &operator[](size_t i) { return d[i]; }
+    void resize(size_t k) { n = k; }
+    void push_back(double v) {
+        if (n == cap) {
+            spill.assign(d, d + n);
+            spill.resize(2 * cap);
+            d = spill.data();
+            cap = spill.size();
+        }
+        d[n++] = v;
+    }
+};
+}  // namespace
+
 double fsum(const double *x, size_t n) {
-    std::vector<double> p;
-    p.reserve(32);
+    Partials p;
     for (size_t t = 0; t < n; ++t) {
         double v = x[t];
         if (!std::isfinite(v)) throw std::invalid_argument("fsum of a non-finite value");
@@ -136,6 +159,7 @@ void hermite_bounds(double zeta, int L, const std::vector<Cart3> &hs, double *I)
 std::vector<double> primitive_schwarz_bounds(const HostShell &sa, const HostShell &sb) {
     const double *A = sa.centre, *B = sb.centre;
     const int L = sa.l + sb.l;
+    if (sa.l > 6 || sb.l > 6) throw std::invalid_argument("a shell above l = 6 in the pair bounds");
     auto hs = herm_order(L);
     auto ca = carts(sa.l), cb = carts(sb.l);
     std::vector<double> out, I(hs.size()), terms(hs.size());
@@ -148,24 +172,34 @@ std::vector<double> primitive_schwarz_bounds(const HostShell &sa, const HostShel
             for (int d = 0; d < 3; ++d) P[d] = (alpha * A[d] + beta * B[d]) / zeta;
             double scale = ca_ * cb_ * std::pow(kPi / zeta, 1.5);
             hermite_bounds(zeta, L, hs, I.data());
+            // E^{ij}_t of each axis for every i <= la, j <= lb, once per
+            // primitive pair (the cartesian pairs below reuse them)
+            double ex[3][7][7][16];
+            for (int d = 0; d < 3; ++d)
+                for (int i2 = 0; i2 <= sa.l; ++i2)
+                    for (int j2 = 0; j2 <= sb.l; ++j2) e_axis(i2, j2, zeta, P[d] - A[d], P[d] - B[d], ex[d][i2][j2]);
             double best = 0.0;
             bool first = true;
             for (auto &a : ca)
                 for (auto &b : cb) {
-                    double ax[3][16];
+                    const double *ax[3];
                     int len[3];
                     for (int d = 0; d < 3; ++d) {
-                        e_axis(a[d], b[d], zeta, P[d] - A[d], P[d] - B[d], ax[d]);
+                        ax[d] = ex[d][a[d]][b[d]];
                         len[d] = a[d] + b[d] + 1;
                     }
+                    // the Hermite indices past an axis's E^{ij} give zero
+                    // terms; fsum is correctly rounded, so leaving them out
+                    // changes no bit of g
+                    size_t m = 0;
                     for (size_t t = 0; t < hs.size(); ++t) {
+                        if (hs[t][0] >= len[0] || hs[t][1] >= len[1] || hs[t][2] >= len[2]) continue;
                         double v = 1.0;
-                        for (int d = 0; d < 3; ++d)
-                            v = hs[t][d] < len[d] ? v * ax[d][hs[t][d]] : 0.0;
+                        for (int d = 0; d < 3; ++d) v = v * ax[d][hs[t][d]];
                         double e = scale * v;
-                        terms[t] = std::fabs(e) * I[t];
+                        terms[m++] = std::fabs(e) * I[t];
                     }
-                    double g = fsum(terms.data(), terms.size());
+                    double g = fsum(terms.data(), m);
                     if (first || g > best) best = g;
                     first = false;
                 }
