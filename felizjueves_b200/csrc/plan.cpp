@@ -49,7 +49,7 @@ struct Partials {
     void resize(size_t k) { n = k; }
     void push_back(double v) {
         if (n == cap) {
-            spill.assign(d, d + n);
+            if (d == fixed) spill.assign(fixed, fixed + n);
             spill.resize(2 * cap);
             d = spill.data();
             cap = spill.size();
