@@ -3213,7 +3213,8 @@ int fjb_batch_create(fjb_batch **out, fjb_handle *const *handles, int n) {
     }
     if (cudaSetDevice(b->device) != cudaSuccess) return bfail(nullptr, FJB_E_CUDA, "cudaSetDevice failed");
     std::vector<PairRec> pr;
-    std::vector<PrimRec> pm;
+    std::vector<std::pair<const PrimRec *, size_t>> prim_src;  // each molecule's device primitive pairs
+    int64_t n_prims = 0;
     std::vector<LaunchRec> lr;
     std::vector<int32_t> lmol;
     std::map<std::tuple<int, int, int, int>, std::vector<UnitSpan>> by_class;  // the molecules' spans
@@ -3224,12 +3225,11 @@ int fjb_batch_create(fjb_batch **out, fjb_handle *const *handles, int n) {
     try {
         for (int m = 0; m < n; ++m) {
             fjb_handle *h = b->mols[m];
-            const int P0 = (int)pr.size(), Q0 = (int)pm.size(), L0 = (int)lr.size();
-            std::vector<PrimRec> hp(h->prims.n);
-            if (!hp.empty() &&
-                cudaMemcpy(hp.data(), h->prims.p, hp.size() * sizeof(PrimRec), cudaMemcpyDeviceToHost) != cudaSuccess)
-                return bfail(nullptr, FJB_E_CUDA, "fjb_batch_create: reading a handle's primitive pairs");
-            pm.insert(pm.end(), hp.begin(), hp.end());
+            const int P0 = (int)pr.size(), Q0 = (int)n_prims, L0 = (int)lr.size();
+            prim_src.emplace_back(h->prims.p, h->prims.n);
+            n_prims += (int64_t)h->prims.n;
+            if (n_prims > (int64_t)INT32_MAX)
+                return bfail(nullptr, FJB_E_LIMIT, "fjb_batch_create: more than 2^31 primitive pairs");
             for (PairRec p : h->pr_host) {
                 p.prim0 += Q0;
                 pr.push_back(p);
@@ -3291,7 +3291,14 @@ int fjb_batch_create(fjb_batch **out, fjb_handle *const *handles, int n) {
         }
         b->n_units = (int)total;
         b->pairs.upload(pr);
-        b->prims.upload(pm);
+        b->prims.alloc(std::max<int64_t>(n_prims, 1));  // the molecules' records, device to device
+        int64_t q = 0;
+        for (auto &src : prim_src) {
+            if (src.second && cudaMemcpy(b->prims.p + q, src.first, src.second * sizeof(PrimRec),
+                                         cudaMemcpyDeviceToDevice) != cudaSuccess)
+                throw std::runtime_error("copying a molecule's primitive pairs");
+            q += (int64_t)src.second;
+        }
         b->launches.upload(lr);
         b->units.alloc(std::max<int64_t>(total, 1));
         if (!spans.empty()) {
