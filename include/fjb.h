@@ -274,10 +274,10 @@ int fjb_router_set(fjb_handle *h, const float *params_host, float log10_threshol
  * keeps more units FP64. */
 int fjb_router_reach(fjb_handle *h, double decades);
 /* Which classes ask the network: those with la + lb + lc + ld >=
- * min_total_l (default 0, every class).  Asking the network costs a few
- * hundred tensor-core cycles a warp of 32 quartets, so below some total
- * angular momentum it can cost more than the FP32 units it adds save;
- * those classes route by the bound alone. */
+ * min_total_l (default 0, every class).  Asking the network costs a warp
+ * of 32 quartets 80 tensor-core products (mma.sync m16n8k16) and 4,096
+ * tanh, so below some total angular momentum it can cost more than the
+ * FP32 units it adds save; those classes route by the bound alone. */
 int fjb_router_classes(fjb_handle *h, int min_total_l);
 /* Features (n x 12 floats) and six-block bounds (n doubles) of sampled
  * launched quartets, samples[3i..3i+2] = (launch, bra index, ket index) in
