@@ -45,6 +45,36 @@ def test_host_units_follow_the_class_order(lib_built, n_atoms, seed):
     assert np.array_equal(got, exp)
 
 
+def _expected_units_np(P) -> np.ndarray:
+    """The same order, vectorised per launch (batches of ~1,000 pairs)."""
+    keys = [(P.batches[L.bra].la, P.batches[L.bra].lb, P.batches[L.ket].la, P.batches[L.ket].lb)
+            for L in P.launches]
+    parts = []
+    for li in sorted(range(len(P.launches)), key=lambda i: (keys[i], i)):
+        L = P.launches[li]
+        nb, nk = len(P.batches[L.bra].pairs), len(P.batches[L.ket].pairs)
+        if L.bra == L.ket:
+            ib, k0 = np.triu_indices(nb)
+            keep = (k0 - ib) % CHUNK == 0  # chunk starts from the bra pair itself
+            ib, k0 = ib[keep], k0[keep]
+        else:
+            ib, k0 = np.meshgrid(np.arange(nb), np.arange(0, nk, CHUNK), indexing="ij")
+            ib, k0 = ib.ravel(), k0.ravel()
+        parts.append(np.stack([np.full(len(ib), li), ib, k0, np.minimum(nk, k0 + CHUNK)], axis=1))
+    return np.concatenate(parts).astype(np.int32) if parts else np.zeros((0, 4), np.int32)
+
+
+def test_host_units_at_4_6_million(lib_built):
+    """A 32-atom cluster (4.6 M units, batches of up to 956 pairs): the
+    closed forms of the diagonal launches' unit offsets at size."""
+    w = configs.cluster(32, 5)
+    eng = FockEngine(w.basis, device=-1)
+    P = eng.plan(w.D, w.tau, w.n_mag)
+    got = eng.plan_units()
+    assert len(got) > 4_000_000
+    assert np.array_equal(got, _expected_units_np(P))
+
+
 def test_everything_screened_gives_no_units(lib_built):
     w = configs.cluster(2, 5)
     eng = FockEngine(w.basis, device=-1)
