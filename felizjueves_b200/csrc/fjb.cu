@@ -1208,8 +1208,19 @@ constexpr int64_t kScatterMaxSlots = int64_t(1) << 28;
 void ensure_units_host(fjb_handle *h) {
     if ((int64_t)h->units_host.size() == (int64_t)h->n_units) return;
     h->units_host.assign((size_t)h->n_units, Unit{});
-    for (const UnitSpan &S : h->spans_host)
-        for (int ib = 0; ib < S.n_bra; ++ib) write_span_units(S, ib, h->units_host.data());
+    // the spans write disjoint ranges: one stride of them a host thread
+    const int nt = (int)std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()),
+                                         std::max<size_t>(1, h->spans_host.size() / 64));
+    auto fill = [h, nt](int t) {
+        for (size_t i = (size_t)t; i < h->spans_host.size(); i += (size_t)nt) {
+            const UnitSpan &S = h->spans_host[i];
+            for (int ib = 0; ib < S.n_bra; ++ib) write_span_units(S, ib, h->units_host.data());
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(fill, t);
+    fill(0);
+    for (auto &th : pool) th.join();
 }
 
 int ensure_scatter(fjb_handle *h) {

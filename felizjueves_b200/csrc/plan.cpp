@@ -331,12 +331,15 @@ Plan f_launches(const HostBasis &basis, const double *D, double tau, int n, int 
         kept.push_back(std::move(p));
     }
     std::map<std::tuple<int, int, int, int>, std::vector<PlanPair>> bins;
-    for (auto &p : kept) bins[{p.la, p.lb, (int)p.prims.size(), p.mag}].push_back(p);
+    for (auto &p : kept) {
+        const auto key = std::make_tuple(p.la, p.lb, (int)p.prims.size(), p.mag);
+        bins[key].push_back(std::move(p));
+    }
     for (auto &kv : bins) {
         PlanBatch b;
         std::tie(b.la, b.lb, b.degree, b.mag) = kv.first;
         b.magnitude = plan.mags[b.mag];
-        b.pairs = kv.second;
+        b.pairs = std::move(kv.second);
         std::stable_sort(b.pairs.begin(), b.pairs.end(),
                          [](const PlanPair &x, const PlanPair &y) { return x.key > y.key; });
         plan.batches.push_back(std::move(b));
