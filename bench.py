@@ -568,12 +568,18 @@ def router_path(a, local):
     """Config c3: the learned router trained at scale -- `--clusters` seeded
     clusters of 8-64 atoms with the c1 shells, `--router-samples` launched
     quartets sampled from each, those the six-block screen computes labelled
-    by the FP64 HGP tap (log10 of the largest deposit into G), about 1e7 in
-    all -- on the GPU with the library's MLP kernels, calibrated on held-out
-    quartets; then on the c1 system (not in the training set) the routed
-    build at `--router-threshold` (1e-9) with the learned router against the bound alone, both with
-    the on-device budget check, against the FP64 build.  W warm-up and K
-    timed graph replays each."""
+    by the FP64 HGP tap (log10 of the largest deposit into G; with
+    `--router-label fp32_error`, of the largest FP32 error into G), about 1e7
+    in all -- on the GPU with the library's MLP kernels, calibrated on
+    held-out quartets through the routing pass's tensor-core inference; then
+    on the c1 system (not in the training set) the routed build at
+    `--router-threshold` (1e-9) with the learned router (every class with
+    its measured reach, every class with a 0.5-decade reach, and the shipped
+    gate; or, for the error labels, three predicted-error thresholds)
+    against the bound alone, all with the on-device budget check, against
+    the FP64 build.  `--router-in` evaluates a trained network instead,
+    its margin recalibrated on a fresh sample.  W warm-up and K timed graph
+    replays each."""
     import time as _t
     import torch
     from felizjueves_b200 import _lib, configs, router
