@@ -40,3 +40,34 @@ def test_cpu_estimate_on_the_reference_plan(oracle_lib):
     ms, desc, spent = b.cpu_estimate(w, plan, w.D, cores=2, budget_s=0.5, seed=1)
     assert np.isfinite(ms) and ms > 0 and spent > 0
     assert "reference's own plan" in desc
+
+
+def test_reference_arm_line_without_this_library(oracle_lib):
+    """`bench.py --impl reference` on c0 prints one JSON line with the
+    contract's keys, its cpu_baseline and zero-copy e2e describing the same
+    run, and never maps libfjb.so into its process."""
+    import json
+    import subprocess
+    import sys
+    code = (
+        "import runpy, sys\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'c0', '--steps', '1', '--warmup', '0']\n"
+        "try:\n"
+        "    runpy.run_path('bench.py', run_name='__main__')\n"
+        "finally:\n"
+        "    maps = open('/proc/self/maps').read()\n"
+        "    print('LIBFJB_MAPPED' if 'libfjb' in maps else 'LIBFJB_ABSENT')\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=HERE, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = r.stdout.strip().splitlines()
+    assert lines[-1] == "LIBFJB_ABSENT"
+    rec = json.loads([ln for ln in lines if ln.startswith("{")][-1])
+    assert rec["impl"] == "reference" and rec["higher_is_better"] is False
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "config"):
+        assert k in rec, k
+    assert rec["value"] > 0 and rec["unit"] == "ms/iter"
+    cb = rec["cpu_baseline"]
+    assert cb["value"] == rec["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
+    e = rec["e2e"]
+    assert e["value"] == rec["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
