@@ -427,6 +427,11 @@ def main():
                                                           "rys_fock_kernel")[top.get("engine", 0)], *tcls),
                      "achieved": round(ach, 3), "peak": round(peak64, 3), "unit": "TFLOP/s",
                      "frac": round(ach / peak64, 4) if peak64 else None, "traffic": None,
+                     "traffic_note": "not captured at this size; the kernel is FP64-issue and "
+                                     "latency bound, its pair records and D read from L2: ncu "
+                                     "measured 1.6 MB read + 23 MB written per launch of the "
+                                     "(pp|pf) Rys class on a 16-atom cluster "
+                                     "(profiles/rys_fock_kernel_pppf_cluster16.md)",
                      "peak_source": "measured: fjb_fma_probe FP64 FMA chains on this GPU "
                                     "(MEASURED_PEAKS.json has no FP64 figure)",
                      "build_tflops": round(build_tf, 3), "kernel_ms": round(top["ms"], 3),
