@@ -29,6 +29,7 @@
 #include <array>
 #include <cmath>
 #include <map>
+#include <mutex>
 #include <stdexcept>
 #include <thread>
 #include <tuple>
@@ -135,17 +136,83 @@ void e_axis(int i, int j, double zeta, double pa, double pb, double *e) {
     for (int t = 0; t < n; ++t) e[t] = prev[t];
 }
 
+namespace {
+// One recurrence step of e_axis: E of length n -> length n + 1 along an
+// axis whose distance is x (the loop body of e_axis, operation for
+// operation).
+inline void e_step(const double *prev, int n, double x, double h, double *out) {
+    for (int t = 0; t <= n; ++t) {
+        double v = 0.0;
+        if (t >= 1) v += h * prev[t - 1];
+        if (t < n) v += x * prev[t];
+        if (t + 1 < n) v += (double)(t + 1) * prev[t + 1];
+        out[t] = v;
+    }
+}
+
+// e_axis(i, j, ...) for every i <= la, j <= lb at once: E^{ij} is i steps
+// along pa then j along pb from the same exp(zeta pa pb), so E^{i0} is
+// carried from i to i + 1 and each E^{ij} extends its E^{i,j-1}.  Every
+// value is the one e_axis computes, with the exponential taken once.
+void e_axis_all(int la, int lb, double zeta, double pa, double pb, double (*ex)[7][16]) {
+    const double h = 0.5 / zeta;
+    double ei0[16];
+    ei0[0] = std::exp(zeta * pa * pb);
+    for (int i = 0; i <= la; ++i) {
+        if (i > 0) {
+            double nxt[16];
+            e_step(ei0, i, pa, h, nxt);
+            for (int t = 0; t <= i; ++t) ei0[t] = nxt[t];
+        }
+        for (int t = 0; t <= i; ++t) ex[i][0][t] = ei0[t];
+        for (int j = 1; j <= lb; ++j) e_step(ex[i][j - 1], i + j, pb, h, ex[i][j]);
+    }
+}
+
+// Per (la, lb): for each Cartesian pair (a, b), in carts(la) x carts(lb)
+// order, the Hermite indices t of hermite_order(la + lb) whose every axis
+// stays within that pair's E^{a_d b_d} (the others give zero terms), and
+// the three axes' E rows.  Built once per process.
+struct PairTerms {
+    std::vector<int> idx, start;   // start[ab] .. start[ab + 1] into idx
+    std::vector<Cart3> ca, cb, hs;
+};
+const PairTerms &pair_terms(int la, int lb) {
+    static std::once_flag once[7][7];
+    static PairTerms tab[7][7];
+    std::call_once(once[la][lb], [la, lb]() {
+        PairTerms &P = tab[la][lb];
+        P.hs = herm_order(la + lb);
+        P.ca = carts(la);
+        P.cb = carts(lb);
+        P.start.push_back(0);
+        for (auto &a : P.ca)
+            for (auto &b : P.cb) {
+                for (size_t t = 0; t < P.hs.size(); ++t)
+                    if (P.hs[t][0] <= a[0] + b[0] && P.hs[t][1] <= a[1] + b[1] && P.hs[t][2] <= a[2] + b[2])
+                        P.idx.push_back((int)t);
+                P.start.push_back((int)P.idx.size());
+            }
+    });
+    return tab[la][lb];
+}
+}  // namespace
+
 // I_p for every p of hermite_order(L) at exponent sum zeta (ao/pairs.py:270).
 void hermite_bounds(double zeta, int L, const std::vector<Cart3> &hs, double *I) {
     const double two_over_sqrt_pi = 2.0 / std::sqrt(kPi);
     double theta = std::sqrt(zeta / 2.0);
     double t2 = theta * theta;
+    // the order-M factor, once per M (the same left-to-right product)
+    if (L > kBoysZeroMax) throw std::invalid_argument("Hermite order above the F_m(0) table");
+    double base[kBoysZeroMax + 1];
+    for (int M = 0; M <= L; ++M)
+        base[M] = two_over_sqrt_pi * theta * std::pow(-2.0 * t2, (double)M) * kBoysZero[M];
     for (size_t k = 0; k < hs.size(); ++k) {
         const Cart3 &p = hs[k];
         int M = p[0] + p[1] + p[2];
         // fundamental(M, 0, theta) with F_M(0) the reference's own value
-        if (M > kBoysZeroMax) throw std::invalid_argument("Hermite order above the F_m(0) table");
-        double v = two_over_sqrt_pi * theta * std::pow(-2.0 * t2, (double)M) * kBoysZero[M];
+        double v = base[M];
         // the recursion's integer factors, innermost (z) first
         for (int q = 1; q <= p[2]; ++q) v = (double)(2 * q - 1) * v;
         for (int q = 1; q <= p[1]; ++q) v = (double)(2 * q - 1) * v;
@@ -160,9 +227,10 @@ std::vector<double> primitive_schwarz_bounds(const HostShell &sa, const HostShel
     const double *A = sa.centre, *B = sb.centre;
     const int L = sa.l + sb.l;
     if (sa.l > 6 || sb.l > 6) throw std::invalid_argument("a shell above l = 6 in the pair bounds");
-    auto hs = herm_order(L);
-    auto ca = carts(sa.l), cb = carts(sb.l);
+    const PairTerms &PT = pair_terms(sa.l, sb.l);
+    const std::vector<Cart3> &hs = PT.hs;
     std::vector<double> out, I(hs.size()), terms(hs.size());
+    out.reserve(sa.exps.size() * sb.exps.size());
     for (size_t i = 0; i < sa.exps.size(); ++i)
         for (size_t j = 0; j < sb.exps.size(); ++j) {
             double alpha = sa.exps[i], beta = sb.exps[j];
@@ -175,30 +243,26 @@ std::vector<double> primitive_schwarz_bounds(const HostShell &sa, const HostShel
             // E^{ij}_t of each axis for every i <= la, j <= lb, once per
             // primitive pair (the cartesian pairs below reuse them)
             double ex[3][7][7][16];
-            for (int d = 0; d < 3; ++d)
-                for (int i2 = 0; i2 <= sa.l; ++i2)
-                    for (int j2 = 0; j2 <= sb.l; ++j2) e_axis(i2, j2, zeta, P[d] - A[d], P[d] - B[d], ex[d][i2][j2]);
+            for (int d = 0; d < 3; ++d) e_axis_all(sa.l, sb.l, zeta, P[d] - A[d], P[d] - B[d], ex[d]);
             double best = 0.0;
             bool first = true;
-            for (auto &a : ca)
-                for (auto &b : cb) {
+            int ab = 0;
+            for (auto &a : PT.ca)
+                for (auto &b : PT.cb) {
                     const double *ax[3];
-                    int len[3];
-                    for (int d = 0; d < 3; ++d) {
-                        ax[d] = ex[d][a[d]][b[d]];
-                        len[d] = a[d] + b[d] + 1;
-                    }
-                    // the Hermite indices past an axis's E^{ij} give zero
-                    // terms; fsum is correctly rounded, so leaving them out
-                    // changes no bit of g
+                    for (int d = 0; d < 3; ++d) ax[d] = ex[d][a[d]][b[d]];
+                    // only the Hermite indices within every axis's E^{ij}:
+                    // the others give zero terms, and fsum is correctly
+                    // rounded, so leaving them out changes no bit of g
                     size_t m = 0;
-                    for (size_t t = 0; t < hs.size(); ++t) {
-                        if (hs[t][0] >= len[0] || hs[t][1] >= len[1] || hs[t][2] >= len[2]) continue;
+                    for (int k = PT.start[ab]; k < PT.start[ab + 1]; ++k) {
+                        const int t = PT.idx[k];
                         double v = 1.0;
                         for (int d = 0; d < 3; ++d) v = v * ax[d][hs[t][d]];
                         double e = scale * v;
                         terms[m++] = std::fabs(e) * I[t];
                     }
+                    ++ab;
                     double g = fsum(terms.data(), m);
                     if (first || g > best) best = g;
                     first = false;
