@@ -9,9 +9,9 @@ files this script writes.
 
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
-parts: libcint boys eri plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 scatter_c0 onee
+parts: libcint boys eri eri_c1_sample plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 scatter_c0 onee
 scf bse harmonics grad rys hjk_c0 boys_zero (default: all
-but plan_c1 and jk_small, which take minutes).
+but plan_c1, jk_small and eri_c1_sample, which take minutes).
 """
 
 from __future__ import annotations
@@ -413,6 +413,46 @@ def part_eri():
                             quartets=np.asarray(qs, np.int32), values=vals,
                             scale=scl, offsets=offs)
         print("eri", wname, len(qs), "quartets", round(time.time() - t, 1), "s")
+
+
+def _eri_pick(args):
+    """One quartet's reference block, reduced to a few elements: the one of
+    largest |value|, the one of largest scale, and up to `k` more drawn at
+    random (seeded by the quartet's position), with the block's largest
+    scale."""
+    shells, q, k, seed = args
+    v, s = _eri_one((shells, q))
+    rng = np.random.default_rng(seed)
+    pick = [int(np.argmax(np.abs(v))), int(np.argmax(s))]
+    if len(v) > 2:
+        pick += [int(x) for x in rng.choice(len(v), size=min(k, len(v)), replace=False)]
+    pick = sorted(set(pick))
+    return pick, v[pick], s[pick], float(s.max())
+
+
+def part_eri_c1_sample():
+    """c1: 40 ordered quartets per class (10,240 in all), each reduced to a
+    few elements of the reference's eri_block_and_scale, so the fixture
+    stays small."""
+    _ref_imports()
+    from felizjueves_b200 import configs
+    w = configs.c1()
+    rb = ref_basis(w.basis)
+    rng = np.random.default_rng(12)
+    qs = sample_quartets(w.basis, rng, 40)
+    t = time.time()
+    with mp.get_context("spawn").Pool(8) as pool:
+        res = pool.map(_eri_pick, [(rb.shells, q, 6, 1000 + i) for i, q in enumerate(qs)],
+                       chunksize=8)
+    idx = np.concatenate([np.asarray(r[0], np.int32) for r in res])
+    offs = np.cumsum([0] + [len(r[0]) for r in res]).astype(np.int64)
+    np.savez_compressed(os.path.join(HERE, "eri_c1_sample.npz"),
+                        quartets=np.asarray(qs, np.int32), offsets=offs, element=idx,
+                        values=np.concatenate([r[1] for r in res]),
+                        scale=np.concatenate([r[2] for r in res]),
+                        block_scale=np.asarray([r[3] for r in res], np.float64))
+    print("eri c1 sample", len(qs), "quartets", len(idx), "elements",
+          round(time.time() - t, 1), "s")
 
 
 # --- f_launches plan lists --------------------------------------------------
@@ -835,6 +875,7 @@ def part_cost():
 
 
 PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_eri,
+         "eri_c1_sample": part_eri_c1_sample,
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "screen_c1": part_screen_c1, "jk_small": part_jk_small,
          "cpu_c0": part_cpu_c0,

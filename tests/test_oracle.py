@@ -28,6 +28,35 @@ def test_eri_blocks_match_reference(oracle_lib, wname):
         assert np.all(err <= 1e-14 * z["scale"][lo:hi] + 1e-300), (q, err.max())
 
 
+def test_eri_blocks_match_reference_c1_sample(oracle_lib):
+    """c1: 40 quartets per class (10,240), each checked at the reference's
+    largest-|value| element, its largest-scale element and six drawn at
+    random, to 1e-14 of the element's own scale.  The blocks are computed on
+    every host thread (the oracle's ctypes calls release the GIL; the first
+    call, which fills its quadrature table, runs alone)."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    w = configs.c1()
+    z = golden("eri_c1_sample.npz")
+    ob = oracle_lib.OracleBasis.of(w.basis)
+    Q, off, el = z["quartets"], z["offsets"], z["element"]
+    val, sc = z["values"], z["scale"]  # read once: the npz is not thread-safe
+
+    def ratio(i):
+        lo, hi = off[i], off[i + 1]
+        got = oracle_lib.eri_block(ob, *map(int, Q[i]))[el[lo:hi]]
+        err = np.abs(got - val[lo:hi])
+        return float((err / (1e-14 * sc[lo:hi] + 1e-300)).max())
+
+    r = [ratio(0)]
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        r += list(ex.map(ratio, range(1, len(Q)), chunksize=64))
+    r = np.asarray(r)
+    bad = np.flatnonzero(r > 1.0)
+    assert bad.size == 0, [(tuple(Q[i]), r[i]) for i in bad[:5]]
+    print(f"worst err/tol = {r.max():.3f}")
+
+
 LIBCINT = ["h2_sto3g", "h2o_sto3g", "h2o_631g", "h2o_ccpvdz", "h10_chain_ccpvdz", "co_ccpvtz"]
 
 
