@@ -21,11 +21,12 @@ def test_eri_blocks_match_reference(oracle_lib, wname):
     w = getattr(configs, wname)()
     z = golden(f"eri_{wname}.npz")
     ob = oracle_lib.OracleBasis.of(w.basis)
+    off, val, sc = z["offsets"], z["values"], z["scale"]  # each npz read decompresses
     for i, q in enumerate(z["quartets"]):
-        lo, hi = z["offsets"][i], z["offsets"][i + 1]
+        lo, hi = off[i], off[i + 1]
         got = oracle_lib.eri_block(ob, *map(int, q))
-        err = np.abs(got - z["values"][lo:hi])
-        assert np.all(err <= 1e-14 * z["scale"][lo:hi] + 1e-300), (q, err.max())
+        err = np.abs(got - val[lo:hi])
+        assert np.all(err <= 1e-14 * sc[lo:hi] + 1e-300), (q, err.max())
 
 
 def test_eri_blocks_match_reference_c1_sample(oracle_lib):
