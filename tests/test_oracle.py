@@ -153,3 +153,23 @@ def test_fock_quartets_equals_unique_sweep(oracle_lib):
     assert np.abs(J + J.T - Jo).max() <= 1e-12
     assert np.abs(K + K.T - Ko).max() <= 1e-12
     assert sec.shape == (len(qs),) and np.all(sec > 0)
+
+
+@pytest.mark.parametrize("name", ["h2_sto3g", "h2o_sto3g", "h2o_631g"])
+def test_schwarz_diagonal_matches_libcint(oracle_lib, name):
+    """(mn|mn) of every AO pair by the oracle's eri_block over each shell
+    pair's (ab|ab) (the diagonal of eri/schwarz.py:86-102) against libcint's
+    int2e diagonal the reference tracks."""
+    g = golden(f"libcint_{name}_schwarz.npz")
+    ob = oracle_lib.OracleBasis.from_npz(g)
+    nc = [int(x) for x in ob.ncart]
+    off = np.concatenate([[0], np.cumsum(nc)])
+    M = np.zeros((off[-1], off[-1]))
+    for a in range(len(nc)):
+        for b in range(len(nc)):
+            blk = oracle_lib.eri_block(ob, a, b, a, b).reshape(nc[a], nc[b], nc[a], nc[b])
+            for i in range(nc[a]):
+                for j in range(nc[b]):
+                    M[off[a] + i, off[b] + j] = blk[i, j, i, j]
+    ref = g["int2e_diag"]
+    assert np.abs(M - ref).max() <= 1e-12 * np.abs(ref).max()
