@@ -9,7 +9,7 @@ files this script writes.
 
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
-parts: libcint boys eri eri_c1_sample plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 scatter_c0 onee
+parts: libcint eri_libcint boys eri eri_c1_sample plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 scatter_c0 onee
 scf bse harmonics grad rys hjk_c0 boys_zero (default: all
 but plan_c1, jk_small and eri_c1_sample, which take minutes).
 """
@@ -106,6 +106,42 @@ def part_libcint():
                             int2e_diag=diag, **sh,
                             source=np.asarray(f"test/oracle/fixtures/{name}_schwarz.json"))
         print("libcint schwarz", name, n)
+
+
+ERI_LIBCINT = ["h2o_631g_eri", "hf_ccpvtz_eri", "hf_ccpvtz_eri_l9", "hf_ccpvtz_eri_l10",
+               "hf_ccpvtz_eri_l11", "hf_ccpvtz_eri_l12"]
+
+
+def part_eri_libcint():
+    """libcint's Cartesian (ij|kl) blocks the reference tracks
+    (`int2e:i,j,k,l` arrays, one shell quartet per class: every class to
+    (ff|ff) over the hf_ccpvtz files), with the converted shells they
+    index."""
+    fx = os.path.join(REF, "test", "oracle", "fixtures")
+    for name in ERI_LIBCINT:
+        d = json.load(open(os.path.join(fx, name + ".json")))
+        assert d["provenance"]["cart"] is True
+        conv = d["converted"]["shells"]
+        qs, vals, offs = [], [], [0]
+        for key, arr in d["arrays"].items():
+            if not key.startswith("int2e:"):
+                continue
+            q = tuple(int(x) for x in key[len("int2e:"):].split(","))
+            v = np.asarray(arr["values"], np.float64)
+            assert tuple(arr["shape"]) == tuple((conv[s]["l"] + 1) * (conv[s]["l"] + 2) // 2
+                                                for s in q)
+            qs.append(q)
+            vals.append(v)
+            offs.append(offs[-1] + len(v))
+        sh = flat_shells([s["l"] for s in conv], [s["centre"] for s in conv],
+                         [s["exponents"] for s in conv], [s["coefficients"] for s in conv])
+        np.savez_compressed(os.path.join(HERE, f"libcint_{name}.npz"),
+                            quartets=np.asarray(qs, np.int32), values=np.concatenate(vals),
+                            offsets=np.asarray(offs, np.int64), **sh,
+                            source=np.asarray(f"test/oracle/fixtures/{name}.json (PySCF "
+                                              f"{d['provenance']['pyscf']}, libcint "
+                                              f"{d['provenance']['libcint']})"))
+        print("libcint eri", name, len(qs), "blocks")
 
 
 # --- one-electron matrices: libcint int1e_* and the reference's own S, T, V ---
@@ -874,7 +910,7 @@ def part_cost():
     print("cost", len(rows), "classes")
 
 
-PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_eri,
+PARTS = {"libcint": part_libcint, "eri_libcint": part_eri_libcint, "df": part_df, "boys": part_boys, "eri": part_eri,
          "eri_c1_sample": part_eri_c1_sample,
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "screen_c1": part_screen_c1, "jk_small": part_jk_small,
@@ -883,7 +919,7 @@ PARTS = {"libcint": part_libcint, "df": part_df, "boys": part_boys, "eri": part_
          "onee": part_onee, "scf": part_scf, "bse": part_bse,
          "harmonics": part_harmonics, "grad": part_grad, "rys": part_rys,
          "hjk_c0": part_hjk_c0, "boys_zero": part_boys_zero}
-DEFAULT = ["libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
+DEFAULT = ["libcint", "eri_libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
 
 
 def main():

@@ -173,3 +173,29 @@ def test_schwarz_diagonal_matches_libcint(oracle_lib, name):
                     M[off[a] + i, off[b] + j] = blk[i, j, i, j]
     ref = g["int2e_diag"]
     assert np.abs(M - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+ERI_LIBCINT = ["h2o_631g_eri", "hf_ccpvtz_eri", "hf_ccpvtz_eri_l9", "hf_ccpvtz_eri_l10",
+               "hf_ccpvtz_eri_l11", "hf_ccpvtz_eri_l12"]
+
+
+@pytest.mark.parametrize("name", ERI_LIBCINT)
+def test_eri_blocks_match_libcint(oracle_lib, name):
+    """libcint's Cartesian (ij|kl) blocks the reference tracks, one shell
+    quartet per class (all 55 classes to (ff|ff) over the hf_ccpvtz files,
+    a general contraction with H off every axis), against the oracle's
+    eri_block, at the reference's own bar: 1e-12 of each element's scale
+    (test/test_ao_eri.py test_block_matches_libcint)."""
+    g = golden(f"libcint_{name}.npz")
+    ob = oracle_lib.OracleBasis.from_npz(g)
+    off, val = g["offsets"], g["values"]
+    classes = set()
+    for i, q in enumerate(g["quartets"]):
+        got, sc = oracle_lib.eri_block(ob, *map(int, q), want_scale=True)
+        ref = val[off[i]:off[i + 1]]
+        err = np.abs(got - ref)
+        assert np.all(err <= 1e-12 * sc), (tuple(q), float(err.max()))
+        ls = [int(g["l"][s]) for s in q]
+        classes.add(tuple(sorted((tuple(sorted(ls[:2])), tuple(sorted(ls[2:]))))))
+    # one quartet per class under the ERI's 8-fold symmetry
+    assert len(classes) == len(g["quartets"]) or name == "h2o_631g_eri"
