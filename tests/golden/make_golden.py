@@ -9,7 +9,7 @@ files this script writes.
 
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
-parts: libcint eri_libcint boys eri eri_c1_sample plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 scatter_c0 onee
+parts: libcint eri_libcint numeric_j boys eri eri_c1_sample plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 scatter_c0 onee
 scf bse harmonics grad rys hjk_c0 boys_zero (default: all
 but plan_c1, jk_small and eri_c1_sample, which take minutes).
 """
@@ -332,6 +332,37 @@ def part_bse():
                              "JSON, via FreeBreakfast data/basis), elements " + " ".join(BSE_ELEMENTS),
                    "sets": out}, fh, indent=0)
     print("bse", len(out))
+
+
+NUMERIC_J = [("j_h2o_sto3g_bse", "h2o_sto3g_j"), ("j_h2o_631g_bse", "h2o_631g_j"),
+             ("j_h2o_ccpvdz_bse", "h2o_ccpvdz_j")]
+
+
+def part_numeric_j():
+    """The reference's numerical golden store (test/golden/numeric/): PySCF's
+    J over a basis read exactly as the BSE document states it (no
+    free-primitive reduction), for the density of the fixture its manifest
+    names (checked by that manifest's sha256 of the density)."""
+    import hashlib
+    nd = os.path.join(REF, "test", "golden", "numeric")
+    man = json.load(open(os.path.join(nd, "manifest.json")))["entries"]
+    fx = os.path.join(REF, "test", "oracle", "fixtures")
+    for entry, case in NUMERIC_J:
+        m = man[entry]
+        assert m["density"]["fixture"] == case and m["provenance"]["cart"] is True
+        J = np.load(os.path.join(nd, m["file"]))
+        d = json.load(open(os.path.join(fx, case + ".json")))
+        n = d["nao"]
+        D = np.asarray(d["arrays"]["density"]["values"], np.float64).reshape(n, n)
+        assert J.shape == D.shape
+        assert hashlib.sha256(D.tobytes()).hexdigest() == m["density"]["sha256"]
+        np.savez_compressed(os.path.join(HERE, f"numeric_{entry}.npz"), J=J, D=D,
+                            basis_file=np.asarray(m["basis"]["file"]),
+                            source=np.asarray(f"test/golden/numeric/{m['file']} (PySCF "
+                                              f"{m['provenance']['pyscf']}, libcint "
+                                              f"{m['provenance']['libcint']}); density of "
+                                              f"test/oracle/fixtures/{case}.json"))
+        print("numeric", entry, n, hashlib.sha256(D.tobytes()).hexdigest()[:12])
 
 
 # --- density fitting: libcint (P|Q) rows and (mn|P) columns -------------------
@@ -910,7 +941,7 @@ def part_cost():
     print("cost", len(rows), "classes")
 
 
-PARTS = {"libcint": part_libcint, "eri_libcint": part_eri_libcint, "df": part_df, "boys": part_boys, "eri": part_eri,
+PARTS = {"libcint": part_libcint, "eri_libcint": part_eri_libcint, "numeric_j": part_numeric_j, "df": part_df, "boys": part_boys, "eri": part_eri,
          "eri_c1_sample": part_eri_c1_sample,
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "screen_c1": part_screen_c1, "jk_small": part_jk_small,
@@ -919,7 +950,7 @@ PARTS = {"libcint": part_libcint, "eri_libcint": part_eri_libcint, "df": part_df
          "onee": part_onee, "scf": part_scf, "bse": part_bse,
          "harmonics": part_harmonics, "grad": part_grad, "rys": part_rys,
          "hjk_c0": part_hjk_c0, "boys_zero": part_boys_zero}
-DEFAULT = ["libcint", "eri_libcint", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
+DEFAULT = ["libcint", "eri_libcint", "numeric_j", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
 
 
 def main():

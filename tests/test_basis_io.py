@@ -85,3 +85,21 @@ def test_parse_layout_and_refusals():
     bad["elements"]["1"]["electron_shells"][0].update(angular_momentum=[0, 1], coefficients=[["1.0"]])
     with pytest.raises(ValueError, match="one coefficient row per"):
         basis_io.parse(bad)
+
+
+NUMERIC_J = [("j_h2o_sto3g_bse", "h2o_sto3g_j", "sto-3g.json"),
+             ("j_h2o_631g_bse", "h2o_631g_j", "6-31g.json"),
+             ("j_h2o_ccpvdz_bse", "h2o_ccpvdz_j", "cc-pVDZ.json")]
+
+
+@pytest.mark.parametrize("entry,case,bse", NUMERIC_J)
+def test_bse_document_j_matches_pyscf(oracle_lib, entry, case, bse):
+    """A BSE document read as it stands (no free-primitive reduction) and
+    mapped by from_bse, then J by the oracle, against PySCF's J over the same
+    document (the reference's numerical golden store, test/golden/numeric/
+    j_*_bse.npy) for the fixture's density: 1e-12 of max|J|."""
+    g = golden(f"numeric_{entry}.npz")
+    B = basis_io.from_bse(_sets()[bse], _atoms(case), reduce=False)
+    assert B.n_ao == g["J"].shape[0]
+    J, _ = oracle_lib.jk(oracle_lib.OracleBasis.of(B), g["D"])
+    assert np.abs(J - g["J"]).max() <= 1e-12 * np.abs(g["J"]).max()
