@@ -9,7 +9,7 @@ files this script writes.
 
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
-parts: libcint eri_libcint numeric_j boys eri eri_c1_sample plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 scatter_c0 onee
+parts: libcint eri_libcint numeric_j numeric_metric boys eri eri_c1_sample plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 scatter_c0 onee
 scf bse harmonics grad rys hjk_c0 boys_zero (default: all
 but plan_c1, jk_small and eri_c1_sample, which take minutes).
 """
@@ -363,6 +363,38 @@ def part_numeric_j():
                                               f"{m['provenance']['libcint']}); density of "
                                               f"test/oracle/fixtures/{case}.json"))
         print("numeric", entry, n, hashlib.sha256(D.tobytes()).hexdigest()[:12])
+
+
+NUMERIC_METRIC = ["metric_h2o_ccpvdz_jkfit_bse", "metric_h2o_def2_universal_jkfit_bse"]
+
+
+def part_numeric_metric():
+    """The numerical golden store's Cartesian (P|Q) over auxiliary BSE
+    documents (data/aux_basis/, read as they stand) on the fixtures' H2O,
+    with those documents cut to H and O."""
+    nd = os.path.join(REF, "test", "golden", "numeric")
+    man = json.load(open(os.path.join(nd, "manifest.json")))["entries"]
+    fx = os.path.join(REF, "test", "oracle", "fixtures")
+    for entry in NUMERIC_METRIC:
+        m = man[entry]
+        assert m["provenance"]["cart"] is True
+        V = np.load(os.path.join(nd, m["file"]))
+        d = json.load(open(os.path.join(REF, m["basis"]["file"])))
+        doc = {"molssi_bse_schema": d["molssi_bse_schema"], "name": d["name"],
+               "function_types": d["function_types"],
+               "elements": {z: {"electron_shells": d["elements"][z]["electron_shells"]}
+                            for z in ("1", "8")}}
+        case = m["molecule"]["fixture"]
+        atoms = json.load(open(os.path.join(fx, case + ".json")))["atoms"]
+        np.savez_compressed(os.path.join(HERE, f"numeric_{entry}.npz"), metric=V,
+                            document=np.asarray(json.dumps(doc)),
+                            charges=np.asarray([a["charge"] for a in atoms], np.float64),
+                            coords=np.asarray([a["coord"] for a in atoms], np.float64),
+                            source=np.asarray(f"test/golden/numeric/{m['file']} (PySCF "
+                                              f"{m['provenance']['pyscf']}, libcint "
+                                              f"{m['provenance']['libcint']}); {m['basis']['file']} "
+                                              f"cut to H and O; atoms of test/oracle/fixtures/{case}.json"))
+        print("numeric", entry, V.shape)
 
 
 # --- density fitting: libcint (P|Q) rows and (mn|P) columns -------------------
@@ -941,7 +973,8 @@ def part_cost():
     print("cost", len(rows), "classes")
 
 
-PARTS = {"libcint": part_libcint, "eri_libcint": part_eri_libcint, "numeric_j": part_numeric_j, "df": part_df, "boys": part_boys, "eri": part_eri,
+PARTS = {"libcint": part_libcint, "eri_libcint": part_eri_libcint, "numeric_j": part_numeric_j,
+         "numeric_metric": part_numeric_metric, "df": part_df, "boys": part_boys, "eri": part_eri,
          "eri_c1_sample": part_eri_c1_sample,
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "screen_c1": part_screen_c1, "jk_small": part_jk_small,
@@ -950,7 +983,7 @@ PARTS = {"libcint": part_libcint, "eri_libcint": part_eri_libcint, "numeric_j": 
          "onee": part_onee, "scf": part_scf, "bse": part_bse,
          "harmonics": part_harmonics, "grad": part_grad, "rys": part_rys,
          "hjk_c0": part_hjk_c0, "boys_zero": part_boys_zero}
-DEFAULT = ["libcint", "eri_libcint", "numeric_j", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
+DEFAULT = ["libcint", "eri_libcint", "numeric_j", "numeric_metric", "boys", "cost", "plan_c0", "screen_c0", "eri", "jplan_c0", "scatter_c0"]
 
 
 def main():

@@ -103,3 +103,19 @@ def test_bse_document_j_matches_pyscf(oracle_lib, entry, case, bse):
     assert B.n_ao == g["J"].shape[0]
     J, _ = oracle_lib.jk(oracle_lib.OracleBasis.of(B), g["D"])
     assert np.abs(J - g["J"]).max() <= 1e-12 * np.abs(g["J"]).max()
+
+
+@pytest.mark.parametrize("entry", ["metric_h2o_ccpvdz_jkfit_bse", "metric_h2o_def2_universal_jkfit_bse"])
+def test_bse_aux_document_metric_matches_libcint(oracle_lib, entry):
+    """An auxiliary BSE document (cc-pVDZ-JKFIT, def2-universal-JKFIT) read
+    as it stands and mapped by from_bse onto H2O, then the Cartesian (P|Q)
+    by the oracle, against libcint's int2c2e_cart over the same document
+    (the reference's numerical golden store): 1e-12 of max|(P|Q)|."""
+    from oracle import df as odf
+    g = golden(f"numeric_{entry}.npz")
+    aux_set = basis_io.parse(json.loads(str(g["document"])))
+    atoms = [(z, tuple(c)) for z, c in zip(g["charges"], g["coords"])]
+    aux = basis_io.from_bse(aux_set, atoms, reduce=False)
+    assert aux.n_ao == g["metric"].shape[0]
+    V = odf.metric(aux)
+    assert np.abs(V - g["metric"]).max() <= 1e-12 * np.abs(g["metric"]).max()
