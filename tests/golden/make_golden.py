@@ -335,7 +335,9 @@ def part_bse():
 
 
 NUMERIC_J = [("j_h2o_sto3g_bse", "h2o_sto3g_j"), ("j_h2o_631g_bse", "h2o_631g_j"),
-             ("j_h2o_ccpvdz_bse", "h2o_ccpvdz_j")]
+             ("j_h2o_ccpvdz_bse", "h2o_ccpvdz_j"),
+             # grad.rhf.get_jk's vj, 3 x n x n
+             ("jx1_h2o_sto3g_bse", "h2o_sto3g_j"), ("jx1_h2o_ccpvdz_bse", "h2o_ccpvdz_j")]
 
 
 def part_numeric_j():
@@ -354,7 +356,7 @@ def part_numeric_j():
         d = json.load(open(os.path.join(fx, case + ".json")))
         n = d["nao"]
         D = np.asarray(d["arrays"]["density"]["values"], np.float64).reshape(n, n)
-        assert J.shape == D.shape
+        assert J.shape[-2:] == D.shape
         assert hashlib.sha256(D.tobytes()).hexdigest() == m["density"]["sha256"]
         np.savez_compressed(os.path.join(HERE, f"numeric_{entry}.npz"), J=J, D=D,
                             basis_file=np.asarray(m["basis"]["file"]),

@@ -104,3 +104,25 @@ def test_scf_then_gradient_with_oracle(oracle_lib):
                                 jk=lambda Bx, Dx: oracle.jk(oracle.OracleBasis.of(Bx), Dx),
                                 onee=lambda Bx, n: one_electron.matrices(Bx, n))
     assert np.abs(out["total"] - g["grad_total"]).max() <= 1e-7
+
+
+@pytest.mark.parametrize("entry,case,bse", [("jx1_h2o_sto3g_bse", "h2o_sto3g_j", "sto-3g.json"),
+                                            ("jx1_h2o_ccpvdz_bse", "h2o_ccpvdz_j", "cc-pVDZ.json")])
+def test_vj1_of_bse_documents_matches_pyscf(oracle_lib, entry, case, bse):
+    """vj1 (grad.rhf.get_jk's Coulomb derivative matrices) over a BSE
+    document read as it stands (no free-primitive reduction), against
+    PySCF's over the same document (the reference's numerical golden store,
+    test/golden/numeric/jx1_*_bse.npy): 1e-12 of max|vj1|."""
+    import json
+    import os
+    from conftest import GOLDEN
+    from felizjueves_b200 import basis_io
+    from oracle import gradient
+    with open(os.path.join(GOLDEN, "bse_subset.json")) as fh:
+        doc = json.load(fh)["sets"][bse]
+    g1 = golden(f"onee_{case}.npz")
+    atoms = [(z, tuple(c)) for z, c in zip(g1["charges"], g1["coords"])]
+    B = basis_io.from_bse(basis_io.parse(doc), atoms, reduce=False)
+    g = golden(f"numeric_{entry}.npz")
+    vj1, _ = gradient.jk_derivatives(B, g["D"])
+    assert np.abs(vj1 - g["J"]).max() <= 1e-12 * np.abs(g["J"]).max()
