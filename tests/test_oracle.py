@@ -121,7 +121,8 @@ def _df_bases(z):
     return mk("ao_"), mk("aux_")
 
 
-@pytest.mark.parametrize("name", ["h2o_ccpvtz_jkfit_metric", "h2o_sto3g_jkfit_3c"])
+@pytest.mark.parametrize("name", ["h2o_ccpvtz_jkfit_metric", "h2o_sto3g_jkfit_3c",
+                                  "prim_spd_f_auxi_metric", "prim_spd_f_auxi_3c"])
 def test_df_integrals_match_libcint(oracle_lib, name):
     """(P|Q) and (mn|P) by the oracle's eri_block with every aux primitive
     paired with a unit s function, against libcint's (the fixtures the
