@@ -9,9 +9,9 @@ files this script writes.
 
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
-parts: libcint eri_libcint numeric_j numeric_metric boys eri eri_c1_sample plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 scatter_c0 onee
+parts: libcint eri_libcint numeric_j numeric_metric boys eri eri_c1_sample plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 jplan_c1 scatter_c0 onee
 scf bse harmonics grad rys hjk_c0 boys_zero (default: all
-but plan_c1, jk_small and eri_c1_sample, which take minutes).
+but plan_c1, jk_small, eri_c1_sample and jplan_c1, which take minutes).
 """
 
 from __future__ import annotations
@@ -875,6 +875,47 @@ def part_jplan_c0():
     print("jplan_c0", sum(len(v) for v in bras.values()), "records,", round(time.time() - t, 1), "s")
 
 
+def part_jplan_c1():
+    """The reference's J-engine launches() on the 64-atom c1 (its bound is a
+    function of (zeta, L) alone, so it is memoised; the values are the
+    function's own).  The lists are large, so per Hermite order L the file
+    keeps the record count, the sha256 of the bra records (i, j, prim) in
+    sweep order and of the ket records in sorted order (int32), and every
+    64th record's G and key."""
+    import functools
+    import hashlib
+    _ref_imports()
+    from felizjueves.eri.j_coulomb import j as JJ
+    from felizjueves.eri.j_coulomb import launch as JL
+    from felizjueves.reference.pq import pq
+    from felizjueves_b200 import configs
+    w = configs.c1()
+    rb = ref_basis(w.basis)
+
+    @functools.lru_cache(maxsize=None)
+    def bound(z, L):
+        return JJ.pair_bound_pq(z, L, pq=pq)
+
+    t = time.time()
+    plan = JL.launches(rb, w.D.tolist(), bound=bound, n_batches=1, tau=w.tau)
+    bras, kets = {}, {}
+    for c in plan:
+        bras[c.lp] = c.bras
+        kets[c.lq] = c.kets
+    out = {"tau": w.tau, "stride": 64}
+    for L, recs in bras.items():
+        ijp = np.array([(r.i, r.j, r.prim) for r in recs], np.int32)
+        out[f"bra{L}_n"] = len(recs)
+        out[f"bra{L}_sha"] = hashlib.sha256(ijp.tobytes()).hexdigest()
+        out[f"bra{L}_G"] = np.array([r.G for r in recs])[::64]
+    for L, recs in kets.items():
+        ijp = np.array([(r.i, r.j, r.prim) for r in recs], np.int32)
+        out[f"ket{L}_sha"] = hashlib.sha256(ijp.tobytes()).hexdigest()
+        out[f"ket{L}_key"] = np.array([r.key for r in recs])[::64]
+    np.savez_compressed(os.path.join(HERE, "jplan_c1.npz"), **out)
+    print("jplan_c1", sum(len(v) for v in bras.values()), "records,", round(time.time() - t, 1), "s")
+
+
 # --- F_m(0) as the reference's Boys function returns it ---------------------
 
 
@@ -981,7 +1022,7 @@ PARTS = {"libcint": part_libcint, "eri_libcint": part_eri_libcint, "numeric_j": 
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "screen_c1": part_screen_c1, "jk_small": part_jk_small,
          "cpu_c0": part_cpu_c0,
-         "cost": part_cost, "jplan_c0": part_jplan_c0, "scatter_c0": part_scatter_c0,
+         "cost": part_cost, "jplan_c0": part_jplan_c0, "jplan_c1": part_jplan_c1, "scatter_c0": part_scatter_c0,
          "onee": part_onee, "scf": part_scf, "bse": part_bse,
          "harmonics": part_harmonics, "grad": part_grad, "rys": part_rys,
          "hjk_c0": part_hjk_c0, "boys_zero": part_boys_zero}
