@@ -9,7 +9,7 @@ files this script writes.
 
     python tests/golden/make_golden.py --ref /path/to/reference [parts...]
 
-parts: libcint eri_libcint numeric_j numeric_metric boys eri eri_c1_sample plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 jplan_c1 scatter_c0 onee
+parts: libcint eri_libcint numeric_j numeric_metric boys eri eri_c1_sample plan_c0 plan_c1 jk_small cpu_c0 screen_c0 screen_c1 cost jplan_c0 jplan_c1 scatter_c0 scatter_c1 onee
 scf bse harmonics grad rys hjk_c0 boys_zero (default: all
 but plan_c1, jk_small, eri_c1_sample and jplan_c1, which take minutes).
 """
@@ -846,6 +846,51 @@ def part_scatter_c0():
     print("scatter_c0", len(pick), "launches,", len(src), "slots")
 
 
+def part_scatter_c1():
+    """The reference's scatter_map on c1 launches, taken from its own c1 plan
+    (plan_c1.npz): per (class, diagonal) key the launch with the fewest
+    slots, where that is small enough for the reference's pure-Python map.
+    Kept as counts and the sha256 of each map's int32 arrays."""
+    import hashlib
+    _ref_imports()
+    from felizjueves.eri.fock import kernel_f_scatter as FS
+    from felizjueves_b200 import configs
+    w = configs.c1()
+    g = np.load(os.path.join(HERE, "plan_c1.npz"))
+    off = ref_basis(w.basis).offsets
+    key, npairs, ab = g["batch_key"], g["batch_npairs"], g["pair_ab"]
+    first = np.concatenate([[0], np.cumsum(npairs)])
+    lau = g["launches"]
+
+    def slots(li):
+        bi, ki = lau[li]
+        la, lb, lc, ld = int(key[bi][0]), int(key[bi][1]), int(key[ki][0]), int(key[ki][1])
+        nab = (la + 1) * (la + 2) // 2 * ((lb + 1) * (lb + 2) // 2)
+        ncd = (lc + 1) * (lc + 2) // 2 * ((ld + 1) * (ld + 2) // 2)
+        return int(npairs[bi]) * int(npairs[ki]) * (nab + ncd)  # a size order, not the layout
+
+    best = {}
+    for li, (bi, ki) in enumerate(lau):
+        k = (*map(int, key[bi][:2]), *map(int, key[ki][:2]), int(bi == ki))
+        if k not in best or slots(li) < slots(best[k]):
+            best[k] = li
+    pick = sorted(li for li in best.values() if slots(li) < (1 << 16))
+    meta, shas = [], []
+    for li in pick:
+        bi, ki = lau[li]
+        la, lb, lc, ld = int(key[bi][0]), int(key[bi][1]), int(key[ki][0]), int(key[ki][1])
+        bra_ao = [off[int(x)] for p in ab[first[bi]:first[bi + 1]] for x in p]
+        ket_ao = [off[int(x)] for p in ab[first[ki]:first[ki + 1]] for x in p]
+        m = FS.scatter_map((la, lb, lc, ld), int(npairs[ki]), bra_ao, ket_ao)
+        h = [hashlib.sha256(np.asarray(a, np.int32).tobytes()).hexdigest() for a in (m.el, m.ptr, m.src)]
+        meta.append((li, m.n_el, m.n_slot))
+        shas.append(h)
+        print("  launch", li, m.n_slot, "slots", flush=True)
+    np.savez_compressed(os.path.join(HERE, "scatter_c1.npz"), meta=np.asarray(meta, np.int64),
+                        sha=np.asarray(shas))
+    print("scatter_c1", len(pick), "launches,", sum(x[2] for x in meta), "slots")
+
+
 # --- the J-engine's launch plan (eri/j_coulomb/launch.py:274-327) on c0 -----
 
 
@@ -1022,7 +1067,7 @@ PARTS = {"libcint": part_libcint, "eri_libcint": part_eri_libcint, "numeric_j": 
          "plan_c0": part_plan_c0, "plan_c1": part_plan_c1,
          "screen_c0": part_screen_c0, "screen_c1": part_screen_c1, "jk_small": part_jk_small,
          "cpu_c0": part_cpu_c0,
-         "cost": part_cost, "jplan_c0": part_jplan_c0, "jplan_c1": part_jplan_c1, "scatter_c0": part_scatter_c0,
+         "cost": part_cost, "jplan_c0": part_jplan_c0, "jplan_c1": part_jplan_c1, "scatter_c0": part_scatter_c0, "scatter_c1": part_scatter_c1,
          "onee": part_onee, "scf": part_scf, "bse": part_bse,
          "harmonics": part_harmonics, "grad": part_grad, "rys": part_rys,
          "hjk_c0": part_hjk_c0, "boys_zero": part_boys_zero}
